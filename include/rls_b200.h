@@ -1,0 +1,171 @@
+/*
+ * rls_b200.h — C ABI of the B200 σ_min(C − zI) grid engine.
+ *
+ * Drop-in boundary for kuandeng/rls's per-grid-point engine.  Every entry
+ * point names the reference interface it replaces (file:line in the reference
+ * project).  Conventions, shared by all calls:
+ *   - complex values are rls_c64 {re, im} (layout of Julia ComplexF64 and of
+ *     C99 double complex); matrices are column-major with a leading dimension;
+ *   - grid indices and permutations are 1-based, as in the Julia API;
+ *   - calls are synchronous; no exceptions cross the ABI; a negative return is
+ *     an rls_status and rls_last_error() gives the message;
+ *   - the library never frees or retains caller memory.
+ */
+#ifndef RLS_B200_H
+#define RLS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } rls_c64;
+typedef struct rls_ctx rls_ctx;
+
+typedef enum {
+  RLS_OK = 0,
+  RLS_ERR_ARG = -1,        /* ArgumentError in the reference            */
+  RLS_ERR_DIM = -2,        /* DimensionMismatch in the reference        */
+  RLS_ERR_CUDA = -3,       /* CUDA runtime failure                      */
+  RLS_ERR_NOMEM = -4,      /* device allocation failed                  */
+  RLS_ERR_TIMEOUT = -5,    /* a bounded device wait gave up             */
+  RLS_ERR_BREAKDOWN = -6,  /* numerical breakdown (LAPACK info != 0)    */
+  RLS_ERR_STATE = -7       /* call order (e.g. no operator uploaded)    */
+} rls_status;
+
+/* Grid description; mirrors the fields of `Recursion` (src/core/recuGrid.jl:1-12). */
+typedef struct {
+  double x_st, x_ed, y_st, y_ed;
+  int64_t n_x, n_y, k;
+} rls_grid;
+
+/* Mirrors `PsTriRecyControl` (src/core/psTriRecy.jl:350-370), fields in order.
+ * lobpcg_side is a Julia Char (UTF-32 code point: 'L' or 'S').  The default
+ * of `shift` depends on normC at construction time, so callers pass it
+ * explicitly.  inner_verbose_override < 0 stands for `nothing`. */
+typedef struct {
+  double tol;
+  double normC;
+  double shift;
+  double gap_tau;
+  double gap_tau_scale;
+  double recy_tau;
+  double recycle_fail_dist_thresh;   /* NaN or Inf = default (one grid step × 1.01) */
+  int64_t r;
+  int64_t p;
+  int64_t p_min;
+  double lobpcg_tol_scale;
+  uint32_t lobpcg_side;
+  uint8_t implict_update;
+  uint8_t implict_recycle;
+  uint8_t collect_timing;
+  uint8_t _pad0;
+  int64_t inner_verbose_override;
+} rls_pstrirecy_control;
+
+/* Mirrors `PsTriRecyStats` (src/core/psTriRecy.jl:257-272).  Array members are
+ * caller-allocated with length nZ and may be NULL; refine_it is an addition
+ * (LOBPCG iterations per point, 0 when the point was recycled). */
+typedef struct {
+  int64_t* p_count;
+  int64_t* r_recy;
+  rls_c64* pts;
+  int64_t* M_vec_apps;
+  int64_t* M_vec_apps_no_recycle;
+  int64_t* R_vec_apps;
+  int64_t* refine_it;
+  uint64_t preprocess_time_ns;
+  uint64_t recycle_time_ns;
+  uint64_t qr_time_ns;
+  uint64_t refine_time_ns;
+  uint64_t update_time_ns;
+  uint8_t mv_stats_available;
+  uint8_t _pad0[7];
+  int64_t n_it;
+  int64_t n_pts;
+} rls_pstrirecy_stats;
+
+/* Mirrors `LobpcgSvdControl` (src/core/lobpcgSvd.jl:1-13).  orth_type: 0 =
+ * :lapack, 1 = :shiftchol.  conv_first/conv_last is the 1-based UnitRange
+ * conv_range. */
+typedef struct {
+  int64_t m, n, r, maxit;
+  double tol;
+  uint32_t side;
+  int32_t verbose;
+  double normC;
+  int32_t orth_type;
+  int32_t conv_thresh_type;
+  int64_t conv_first, conv_last;
+} rls_lobpcg_control;
+
+/* Optional per-point log sink (the reference prints the same lines to `io`). */
+typedef void (*rls_log_fn)(const char* line, void* user);
+
+/* ---- context ---------------------------------------------------------------- */
+
+/* One context per host thread: owns a CUDA stream, the device workspaces and
+ * the uploaded operator.  No reference counterpart (Julia keeps this state in
+ * PsTriRecyKeep, src/core/psTriRecy.jl:395-417). */
+int rls_ctx_create(rls_ctx** out, int device);
+void rls_ctx_destroy(rls_ctx* ctx);
+const char* rls_last_error(const rls_ctx* ctx);
+const char* rls_status_string(int status);
+int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verbose);
+
+/* ---- recursion grid (bit-exact) ------------------------------------------- */
+
+/* recursion_grid / recursion_grid_zigzag (src/core/recuGrid.jl:68-73, :157-176).
+ * Z has n_x*n_y entries. */
+int rls_grid_zigzag(const rls_grid* g, rls_c64* Z);
+/* recursion_grid_linear (src/core/recuGrid.jl:82-102). */
+int rls_grid_linear(const rls_grid* g, rls_c64* Z);
+/* recursion_grid_spiral (src/core/recuGrid.jl:109-148). */
+int rls_grid_spiral(const rls_grid* g, rls_c64* Z);
+/* recursion_natural_permutation (src/core/recuGrid.jl:196-208): perm is 1-based,
+ * length n_x*n_y, and Z[perm] is in natural order. */
+int rls_natural_perm(const rls_grid* g, const rls_c64* Z, int64_t nZ, int64_t* perm);
+/* reorder_to_natural (src/core/recuGrid.jl:216-221) for Float64 vectors. */
+int rls_reorder_to_natural(const rls_grid* g, const rls_c64* Z, int64_t nZ,
+                           const double* v, double* out);
+/* reorder_to_natural_grid (src/core/recuGrid.jl:229-232): out is the n_y × n_x
+ * column-major matrix A with A[iy, ix] at grid point (x[ix], y[iy]). */
+int rls_reorder_to_natural_grid(const rls_grid* g, const rls_c64* Z, int64_t nZ,
+                                const double* v, double* out);
+
+/* ---- operator upload ---------------------------------------------------------- */
+
+/* Uploads the upper-triangular complex Schur factor T of C (C = Q T Qᴴ), i.e.
+ * the M of `pre_process(C::Matrix)` (src/core/psTriRecy.jl:6-14; S = I).  Only
+ * the upper triangle of T (n × n, column-major, leading dimension ldt) is read.
+ * Host memory. */
+int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
+
+/* ---- solvers ------------------------------------------------------------------ */
+
+/* psTriRecy on the uploaded Schur factor (src/core/psTriRecy.jl:708-881,
+ * dense branch :580-650).  Z (nZ points, traversal order of `rec.Z`) and the
+ * grid g (used for the recycle-failure distance, recySpace.jl:22-37, and the
+ * forced-add gap budget, psTriRecy.jl:388-393) come from rls_grid_*.  X0 is
+ * the n × r initial block the reference draws with rand!(X)
+ * (psTriRecy.jl:607); NULL draws it on the device.  sigma_min receives nZ
+ * values in Z order. */
+int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                        const rls_pstrirecy_control* control, const rls_c64* X0,
+                        double* sigma_min, rls_pstrirecy_stats* stats);
+
+/* lobpcgSvd (src/core/lobpcgSvd.jl:365-477) on C = InvMat(adjoint(T − zI)) with
+ * K = I, as psTriRecy calls it at psTriRecy.jl:797-808.  X0 (n × r) may be
+ * NULL.  X_out (n × r, may be NULL) receives keep.S[:, 1:r]; sigma_r (r
+ * values, may be NULL) receives keep.σ[1:r].  *sigma gets the returned σ and
+ * *it the iteration count. */
+int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
+                          const rls_lobpcg_control* control, rls_c64* X_out,
+                          double* sigma_r, double* sigma, int64_t* it);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RLS_B200_H */

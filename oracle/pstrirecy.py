@@ -1,0 +1,209 @@
+"""Restatement of src/core/psTriRecy.jl (dense Schur-triangular path).
+
+Test infrastructure only (see oracle/__init__.py).
+
+``pre_process`` (psTriRecy.jl:6-14) reduces a square dense C to its complex
+Schur factor T (C = Q T Qᴴ, LAPACK zgees through scipy); M = T and S = I.
+Because the similarity is unitary, σ_min(C − zI) = σ_min(T − zI).
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field, fields
+
+import numpy as np
+import scipy.linalg as sla
+
+from .linalg import EPS
+from .lobpcg import LobpcgSvdControl, LobpcgSvdKeep, lobpcg_svd
+from .recycle import (RecycledSpace, fast_svd_rayl_ritz_implicit, update_recycled_space,
+                      resolve_recycle_fail_dist_thresh)
+
+
+@dataclass
+class PsTriRecyControl:
+    """psTriRecy.jl:350-370.  ``shift`` defaults to normC²·eps·100 (:353)."""
+    tol: float = 1e-3
+    normC: float = 1.0
+    shift: float = None
+    gap_tau: float = 1e-10
+    gap_tau_scale: float = 0.01
+    recy_tau: float = 1.5
+    recycle_fail_dist_thresh: float = float("nan")
+    r: int = 6
+    p: int = 50
+    p_min: int = 1
+    lobpcg_tol_scale: float = 0.1
+    lobpcg_side: str = "L"
+    implict_update: bool = False
+    implict_recycle: bool = True
+    collect_timing: bool = True
+    inner_verbose_override: int = None
+
+    def __post_init__(self):
+        if self.shift is None:
+            self.shift = self.normC ** 2 * EPS * 100
+
+
+@dataclass
+class PsTriRecyStats:
+    """psTriRecy.jl:257-292."""
+    p_count: np.ndarray
+    r_recy: np.ndarray
+    pts: np.ndarray
+    M_vec_apps: np.ndarray
+    M_vec_apps_no_recycle: np.ndarray
+    R_vec_apps: np.ndarray
+    preprocess_time_ns: int = 0
+    recycle_time_ns: int = 0
+    qr_time_ns: int = 0
+    refine_time_ns: int = 0
+    update_time_ns: int = 0
+    mv_stats_available: bool = True
+    n_it: int = 0
+    n_pts: int = 0
+    refine_it: np.ndarray = None
+
+    @classmethod
+    def alloc(cls, nZ):
+        z = lambda: np.zeros(nZ, dtype=np.int64)
+        return cls(z(), z(), np.zeros(nZ, dtype=np.complex128), z(), z(), z(), refine_it=z())
+
+
+class TriOp:
+    """Upper-triangular operator M = T (dense Schur factor)."""
+
+    def __init__(self, T):
+        self.T = T
+
+    def mul(self, X):
+        return self.T @ X
+
+    def mul_adj(self, Y):
+        return self.T.conj().T @ Y
+
+
+class IdentityOp:
+    """S = Diagonal(ones) (psTriRecy.jl:13)."""
+
+    def mul(self, X):
+        return X.copy()
+
+    def mul_adj(self, Y):
+        return Y.copy()
+
+
+class InvAdjR:
+    """InvMat(adjoint(Rz)) (psTriRecy.jl:797; RLSMatrices.jl:390-425).
+    mul: R⁻ᴴ X (forward solve with Rᴴ); mul_adj: R⁻¹ Y (back solve with R)."""
+
+    def __init__(self, R):
+        self.R = R
+
+    def mul(self, X):
+        return sla.solve_triangular(self.R, X, lower=False, trans="C", check_finite=False)
+
+    def mul_adj(self, Y):
+        return sla.solve_triangular(self.R, Y, lower=False, trans="N", check_finite=False)
+
+
+def pre_process_dense(C):
+    """psTriRecy.jl:6-14 (square branch): complex Schur T of C."""
+    T, _ = sla.schur(np.asarray(C, dtype=np.complex128), output="complex")
+    return np.triu(T)
+
+
+def _gap_tau(ctl, remaining):
+    """psTriRecy.jl:373-378."""
+    return ctl.gap_tau * ctl.gap_tau_scale if remaining > 0 else ctl.gap_tau
+
+
+def residual_norm_ok(W, sigma, tol, normC):
+    """_residual_norm_ok (psTriRecy.jl:237-245)."""
+    return np.linalg.norm(W[:, 0]) < normC * max(sigma * tol, normC * np.sqrt(2) * EPS)
+
+
+def ps_tri_recy_schur(T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None):
+    """_psTriRecy_impl (psTriRecy.jl:708-881) on a precomputed Schur factor T.
+
+    ``X0`` (n×r) replaces the reference's ``rand!(X)`` (psTriRecy.jl:607): the
+    Julia RNG stream is not reproducible here, so the caller supplies it.
+    Returns (σ_min, stats).
+    """
+    n = T.shape[0]
+    r = ctl.r
+    M, S = TriOp(T), IdentityOp()
+    rs = RecycledSpace(n, n, ctl.p, r, p_min=ctl.p_min)
+    keep = LobpcgSvdKeep(n, n, r)
+    X = keep.S[:, :r]
+    W = keep.S[:, r:2 * r]
+    if X0 is None:
+        rng = np.random.default_rng(seed)
+        X0 = rng.random((n, r)) + 1j * rng.random((n, r))
+    X[:, :] = X0
+    sigma_recy = np.zeros(r)
+    ctl_main = LobpcgSvdControl(m=n, n=n, r=r, conv_range=(1, 1),
+                                tol=float(ctl.lobpcg_tol_scale * ctl.tol),
+                                side=ctl.lobpcg_side, normC=ctl.normC)
+    shift = complex(ctl.shift)
+    thresh = resolve_recycle_fail_dist_thresh(ctl.recycle_fail_dist_thresh, rec)
+    remaining = 0
+    nZ = len(rec.Z)
+    sigma_min = np.full(nZ, np.nan)
+    st = PsTriRecyStats.alloc(nZ)
+    last_failed = None
+    Rz = T.copy()
+    diagT = np.diag(T).copy()
+    for i in range(nZ):
+        z = complex(rec.Z[i])
+        st.p_count[i] = rs.p
+        r_svdrr = 0
+        m_apps = 0
+        r_apps = 0
+        recycled = False
+        if rs.p > 0:
+            t0 = time.perf_counter_ns()
+            r_svdrr = fast_svd_rayl_ritz_implicit(rs, z, X, W, sigma_recy, shift,
+                                                  _gap_tau(ctl, remaining))
+            remaining = remaining - 1 if remaining > 0 else 0
+            st.recycle_time_ns += time.perf_counter_ns() - t0
+            st.r_recy[i] = r_svdrr
+            recycled = residual_norm_ok(W, sigma_recy[0], ctl.tol, ctl.normC)
+            if recycled:
+                sigma_min[i] = sigma_recy[0]
+                if log is not None:
+                    log(i, z, "recycled", rs.p, r_svdrr, sigma_min[i], 0)
+                continue
+        t0 = time.perf_counter_ns()
+        np.fill_diagonal(Rz, diagT - z)                       # get_R_factor! (psTriRecy.jl:87-99)
+        _, it = lobpcg_svd(InvAdjR(Rz), X, None, keep, ctl_main)
+        sigma_min[i] = keep.sigma[0]
+        st.refine_it[i] = it
+        if it > 0:
+            r_apps += 2 * r + it * r + (it - 1) * r
+        st.refine_time_ns += time.perf_counter_ns() - t0
+        st.n_it += it
+        st.pts[st.n_pts] = z
+        st.n_pts += 1
+        if i < nZ - 1 and it > 0:
+            t0 = time.perf_counter_ns()
+            force_add = last_failed is not None and abs(z - last_failed) <= thresh
+            update_recycled_space(M, S, z, rs, keep.S[:, :r], tau=ctl.recy_tau, r_sub=1,
+                                  force_add=force_add)
+            remaining = max(rec.k, 0) if force_add else 0
+            m_apps += 3 * r if ctl.implict_recycle else r
+            st.update_time_ns += time.perf_counter_ns() - t0
+        last_failed = z
+        st.M_vec_apps[i] = m_apps
+        st.M_vec_apps_no_recycle[i] = m_apps
+        st.R_vec_apps[i] = r_apps
+        if log is not None:
+            log(i, z, "refine", rs.p, r_svdrr, sigma_min[i], it)
+    return sigma_min, st
+
+
+def dense_sigma_min(C, z):
+    """Independent FP64 oracle: smallest singular value of C − zI by dense SVD."""
+    A = np.asarray(C, dtype=np.complex128).copy()
+    A[np.diag_indices_from(A)] -= z
+    return sla.svdvals(A)[-1]

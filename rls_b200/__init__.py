@@ -1,0 +1,19 @@
+"""B200 σ_min(C − zI) grid engine — the psTriRecy hot path of kuandeng/rls on sm_100a.
+
+Public names mirror the reference (src/core/recuGrid.jl, src/core/psTriRecy.jl,
+src/core/lobpcgSvd.jl).  All per-grid-point work runs in librls_b200.so; there is
+no CPU fallback.
+"""
+from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_grid_linear,
+                   recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
+                   reorder_to_natural_grid)
+from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, SchurFactor, pre_process,
+                      psTriRecy)
+from ._lib import RLSError, ArgumentError, DimensionMismatch
+
+__all__ = [
+    "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
+    "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
+    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "SchurFactor", "pre_process", "psTriRecy", "RLSError",
+    "ArgumentError", "DimensionMismatch",
+]

@@ -1,0 +1,415 @@
+// Streaming kernels over tall n-row blocks and the tiled Schur factor.
+//
+// Layout (shared by every kernel here):
+//   * tall blocks (V, J1, J2, J5, LOBPCG S/CS, ...) are column-major with
+//     leading dimension ld = n_pad (a multiple of TILE); rows n..n_pad-1 are
+//     kept at zero so every kernel may run over n_pad rows;
+//   * the upper-triangular Schur factor T is stored by TILE×TILE tiles, tile
+//     (I, J) (J >= I) at tile index J*(J+1)/2 + I, each tile column-major with
+//     leading dimension TILE.  Rows/columns beyond n are zero.
+#pragma once
+#include "common.cuh"
+
+#define TILE 64
+
+__host__ __device__ __forceinline__ int64_t tile_index(int I, int J) {
+  return (int64_t)J * (J + 1) / 2 + I;
+}
+
+// ------------------------------------------------------------------------------------
+// Gram: C (k1×k2) = alpha·AᴴB + beta·C.  Phase 1: grid (chunks, ceil(k1/8)); warp w
+// owns column (blockIdx.y*8+w) of A and sums over the chunk's rows; k2 <= 32.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gram_partial(int64_t nrows, int64_t chunk,
+                                                      const cplx* __restrict__ A, int64_t lda, int k1,
+                                                      const cplx* __restrict__ B, int64_t ldb, int k2,
+                                                      cplx* __restrict__ part) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int col = blockIdx.y * 8 + w;
+  const int64_t r0 = (int64_t)blockIdx.x * chunk;
+  const int64_t r1 = min(nrows, r0 + chunk);
+  cplx acc[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) acc[j] = czero();
+  if (col < k1) {
+    const cplx* a = A + (int64_t)col * lda;
+    for (int64_t row = r0 + lane; row < r1; row += 32) {
+      const cplx av = a[row];
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < k2) acc[j] = cfmac(av, __ldg(&B[(int64_t)j * ldb + row]), acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < k2) {
+      cplx s = warp_sum(acc[j]);
+      if (lane == 0 && col < k1) part[((int64_t)blockIdx.x * k1 + col) * k2 + j] = s;
+    }
+  }
+}
+
+__global__ void k_gram_reduce(int nchunks, int k1, int k2, const cplx* __restrict__ part, cplx alpha,
+                              cplx beta, cplx* C, int64_t ldc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= k1 * k2) return;
+  const int i = t / k2, j = t % k2;
+  cplx s = czero();
+  for (int c = 0; c < nchunks; ++c) s = cadd(s, part[((int64_t)c * k1 + i) * k2 + j]);
+  cplx out = cmul(alpha, s);
+  if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + i], out);
+  C[(int64_t)j * ldc + i] = out;
+}
+
+// ------------------------------------------------------------------------------------
+// Row-streaming GEMM with an affine combination of up to 4 sources:
+//   Y = sum_q coef_q * A_q           (row by row, never materialised)
+//   C = alpha * Y * B + beta * C     (B: k1 × k2 small, k2 <= 32)
+// Optional second product X = A_xsrc * B (same B) and epilogue C -= X * diag(s2),
+// plus per-CTA partial |C[:,0]|^2 sums.  One thread per row; a row of C is written
+// only after all reads of that row, so C may alias A_q when k1 == k2.
+// ------------------------------------------------------------------------------------
+struct CombSrc {
+  const cplx* a[4];
+  cplx coef[4];
+  int nsrc;
+};
+
+template <int K2MAX>
+__global__ void __launch_bounds__(128) k_gemm_rows(int64_t nrows, CombSrc src, int64_t lda, int k1,
+                                                   const cplx* __restrict__ B, int64_t ldb, int k2,
+                                                   cplx alpha, cplx beta, cplx* C, int64_t ldc,
+                                                   int xsrc, cplx* X, int64_t ldx,
+                                                   const double* __restrict__ s2,
+                                                   double* __restrict__ col0_part) {
+  extern __shared__ cplx sB[];  // KC × k2 chunk of B
+  const int KC = 32;
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  cplx acc[K2MAX], accx[K2MAX];
+#pragma unroll
+  for (int j = 0; j < K2MAX; ++j) { acc[j] = czero(); accx[j] = czero(); }
+  for (int kc = 0; kc < k1; kc += KC) {
+    const int kn = min(KC, k1 - kc);
+    __syncthreads();
+    for (int t = threadIdx.x; t < kn * k2; t += blockDim.x) {
+      const int kk = t % kn, j = t / kn;
+      sB[j * KC + kk] = B[(int64_t)j * ldb + kc + kk];
+    }
+    __syncthreads();
+    if (row < nrows) {
+      for (int kk = 0; kk < kn; ++kk) {
+        const int64_t off = (int64_t)(kc + kk) * lda + row;
+        cplx y = czero(), xv = czero();
+        for (int q = 0; q < src.nsrc; ++q) {
+          const cplx v = src.a[q][off];
+          y = cfma(src.coef[q], v, y);
+          if (q == xsrc) xv = v;
+        }
+#pragma unroll
+        for (int j = 0; j < K2MAX; ++j) {
+          if (j < k2) {
+            const cplx b = sB[j * KC + kk];
+            acc[j] = cfma(y, b, acc[j]);
+            if (xsrc >= 0) accx[j] = cfma(xv, b, accx[j]);
+          }
+        }
+      }
+    }
+  }
+  double c0 = 0.0;
+  if (row < nrows) {
+#pragma unroll
+    for (int j = 0; j < K2MAX; ++j) {
+      if (j < k2) {
+        cplx out = cmul(alpha, acc[j]);
+        if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + row], out);
+        if (xsrc >= 0) {
+          if (s2) out = csub(out, cscale(accx[j], s2[j]));
+          X[(int64_t)j * ldx + row] = accx[j];
+        }
+        C[(int64_t)j * ldc + row] = out;
+        if (j == 0) c0 = cabs2(out);
+      }
+    }
+  }
+  if (col0_part) {
+    __shared__ double red[32];
+    const double s = block_sum(c0, red);
+    if (threadIdx.x == 0) col0_part[blockIdx.x] = s;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Tiled TRMM: Y = T X (adj=0) or Y = Tᴴ X (adj=1), X/Y n_pad × k (k <= 16).
+// Work unit u = (output tile row/col O, chunk of up to UT source tiles); partials
+// land in part[u] and k_trmm_reduce sums the units of each O in a fixed order.
+// ------------------------------------------------------------------------------------
+#define TRMM_UT 8
+
+// Loads tile `tp` (TILE×TILE, column-major) into shared memory with row stride
+// TILE_LDS.  For adj the tile is stored transposed so that both T·x and Tᴴ·x read
+// consecutive addresses across threads (the odd stride keeps the 16-byte slots of
+// eight consecutive threads in distinct banks).
+#define TILE_LDS (TILE + 1)
+__device__ __forceinline__ void load_tile(cplx* sT, const cplx* __restrict__ tp, int adj) {
+  for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
+    const int rr = t % TILE, cc = t / TILE;
+    const cplx v = tp[t];
+    if (!adj) sT[cc * TILE_LDS + rr] = v;   // element (rr, cc) at column cc
+    else sT[rr * TILE_LDS + cc] = v;        // element (rr, cc) at "column" rr
+  }
+}
+
+// acc[c] += (adj ? Tᴴ : T)[row, inner-range] · sX[inner-range, c], inner range of group grp.
+template <int KMAX>
+__device__ __forceinline__ void tile_apply(const cplx* sT, const cplx* sX, int k, int adj, int row, int grp,
+                                           cplx* acc) {
+  if (!adj) {
+    for (int jj = grp * 16; jj < grp * 16 + 16; ++jj) {
+      const cplx tv = sT[jj * TILE_LDS + row];
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c)
+        if (c < k) acc[c] = cfma(tv, sX[c * TILE + jj], acc[c]);
+    }
+  } else {
+    for (int ii = grp * 16; ii < grp * 16 + 16; ++ii) {
+      const cplx tv = sT[ii * TILE_LDS + row];   // T[ii, row]
+#pragma unroll
+      for (int c = 0; c < KMAX; ++c)
+        if (c < k) acc[c] = cfmac(tv, sX[c * TILE + ii], acc[c]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_trmm_partial(int nb, const cplx* __restrict__ T,
+                                                      const cplx* __restrict__ X, int64_t ldx, int k,
+                                                      int adj, const int* __restrict__ unit_O,
+                                                      const int* __restrict__ unit_s,
+                                                      cplx* __restrict__ part) {
+  extern __shared__ cplx sm[];
+  cplx* sT = sm;                       // TILE*TILE_LDS
+  cplx* sX = sm + TILE * TILE_LDS;     // TILE*k
+  cplx* sAcc = sm;                     // 4 × TILE*k partial sums, reuses sT after the loop (k <= 16)
+  const int u = blockIdx.x;
+  const int O = unit_O[u], s0 = unit_s[u];
+  const int row = threadIdx.x & (TILE - 1), grp = threadIdx.x >> 6;  // 4 groups split the inner dim
+  cplx acc[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) acc[c] = czero();
+  // Source tiles: adj=0: T(O, J), J = O + s0 .. ; adj=1: T(I, O), I = s0 ..
+  const int nsrc = adj ? (O + 1) : (nb - O);
+  const int s1 = min(nsrc, s0 + TRMM_UT);
+  for (int s = s0; s < s1; ++s) {
+    const int I = adj ? s : O;
+    const int J = adj ? O : O + s;
+    const int xb = adj ? I : J;  // tile of X that multiplies
+    __syncthreads();
+    load_tile(sT, T + tile_index(I, J) * (TILE * TILE), adj);
+    for (int t = threadIdx.x; t < TILE * k; t += blockDim.x) {
+      const int rr = t % TILE, c = t / TILE;
+      sX[c * TILE + rr] = X[(int64_t)c * ldx + (int64_t)xb * TILE + rr];
+    }
+    __syncthreads();
+    tile_apply<16>(sT, sX, k, adj, row, grp, acc);
+  }
+  __syncthreads();
+  for (int c = 0; c < k; ++c) sAcc[(grp * k + c) * TILE + row] = acc[c];
+  __syncthreads();
+  for (int t = threadIdx.x; t < TILE * k; t += blockDim.x) {
+    const int rr = t % TILE, c = t / TILE;
+    cplx v = sAcc[(0 * k + c) * TILE + rr];
+    v = cadd(v, sAcc[(1 * k + c) * TILE + rr]);
+    v = cadd(v, sAcc[(2 * k + c) * TILE + rr]);
+    v = cadd(v, sAcc[(3 * k + c) * TILE + rr]);
+    part[((int64_t)u * 16 + c) * TILE + rr] = v;
+  }
+}
+
+__global__ void k_trmm_reduce(int nb, int k, const int* __restrict__ O_first, const int* __restrict__ O_count,
+                              const cplx* __restrict__ part, cplx* Y, int64_t ldy) {
+  const int O = blockIdx.x;
+  for (int t = threadIdx.x; t < TILE * k; t += blockDim.x) {
+    const int rr = t % TILE, c = t / TILE;
+    cplx s = czero();
+    for (int u = O_first[O]; u < O_first[O] + O_count[O]; ++u) s = cadd(s, part[((int64_t)u * 16 + c) * TILE + rr]);
+    Y[(int64_t)c * ldy + (int64_t)O * TILE + rr] = s;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Inverse of each shifted diagonal tile D_I = T_II − z·I (upper triangular), rows
+// beyond n set to the identity.  One CTA (256 threads) per tile; right-looking
+// back substitution on all 64 right-hand sides at once.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_diag_inv(int nb, int64_t n, const cplx* __restrict__ T, cplx z,
+                                                  cplx* __restrict__ Dinv, int* err) {
+  extern __shared__ cplx sm[];
+  cplx* sU = sm;                    // TILE*TILE
+  cplx* sY = sm + TILE * TILE;      // TILE*TILE
+  const int I = blockIdx.x;
+  const cplx* tp = T + tile_index(I, I) * (TILE * TILE);
+  for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
+    const int rr = t % TILE, cc = t / TILE;
+    const int64_t g = (int64_t)I * TILE + rr;
+    cplx u = tp[t];
+    if (rr == cc) u = (g < n) ? csub(u, z) : cmk(1.0, 0.0);
+    sU[t] = (rr <= cc) ? u : czero();
+    sY[t] = (rr == cc) ? cmk(1.0, 0.0) : czero();
+  }
+  __syncthreads();
+  for (int i = TILE - 1; i >= 0; --i) {
+    const cplx dinv = cinv(sU[i * TILE + i]);
+    // row i of Y: columns c >= i
+    for (int c = i + threadIdx.x; c < TILE; c += blockDim.x) sY[c * TILE + i] = cmul(sY[c * TILE + i], dinv);
+    __syncthreads();
+    // rows l < i: Y[l, c] -= U[l, i] * Y[i, c]  (c >= i)
+    const int nl = i, ncol = TILE - i;
+    for (int t = threadIdx.x; t < nl * ncol; t += blockDim.x) {
+      const int l = t % nl, c = i + t / nl;
+      sY[c * TILE + l] = cfms(sU[i * TILE + l], sY[c * TILE + i], sY[c * TILE + l]);
+    }
+    __syncthreads();
+  }
+  bool bad = false;
+  for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
+    const cplx y = sY[t];
+    if (!isfinite(y.x) || !isfinite(y.y)) bad = true;
+    Dinv[(int64_t)I * TILE * TILE + t] = y;
+  }
+  if (bad) atomicOr(err, DEVERR_NONFINITE);
+}
+
+// ------------------------------------------------------------------------------------
+// Dataflow triangular solve with the shifted Schur factor R = T − zI.
+//   adj = 0: R X = B   (back substitution, tiles of block row I, J > I)
+//   adj = 1: Rᴴ X = B  (forward substitution, tiles of block column J, I < J)
+// One CTA per tile row; CTAs take row blocks by ticket in dependency order, so a
+// CTA only ever waits on blocks owned by CTAs that started before it.  Each wait
+// is bounded by RLS_SPIN_LIMIT polls; on expiry the CTA records DEVERR_SPIN_TIMEOUT
+// and finishes with whatever it has, so the launch always terminates.
+// X may alias B.  k <= 24.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(256) k_trsm_dataflow(int nb, const cplx* __restrict__ T,
+                                                       const cplx* __restrict__ Dinv, const cplx* B,
+                                                       cplx* X, int64_t ldx, int k, int adj,
+                                                       int* __restrict__ ticket, int* flags, int epoch,
+                                                       int* err) {
+  extern __shared__ cplx sm[];
+  cplx* sT = sm;                         // TILE*TILE_LDS
+  cplx* sX = sT + TILE * TILE_LDS;       // TILE*k (dependency block)
+  cplx* sAcc = sX + TILE * k;            // TILE*k (running right-hand side)
+  cplx* sPart = sAcc + TILE * k;         // 4 × TILE*k partial products
+  __shared__ int sblk;
+  if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int t = sblk;
+  const int b = adj ? t : (nb - 1 - t);
+  const int row = threadIdx.x & (TILE - 1), grp = threadIdx.x >> 6;
+  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+    const int rr = q % TILE, c = q / TILE;
+    sAcc[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
+  }
+  const int ndep = adj ? b : (nb - 1 - b);
+  for (int d = 0; d < ndep; ++d) {
+    const int dep = adj ? d : (nb - 1 - d);
+    const cplx* tp = adj ? T + tile_index(dep, b) * (TILE * TILE) : T + tile_index(b, dep) * (TILE * TILE);
+    __syncthreads();
+    load_tile(sT, tp, adj);   // independent of X: issued before the wait
+    if (threadIdx.x == 0) {
+      int spins = 0;
+      while (ld_acquire(&flags[dep]) != epoch) {
+        if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
+        __nanosleep(64);
+      }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+      const int rr = q % TILE, c = q / TILE;
+      sX[c * TILE + rr] = __ldcg(&X[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
+    }
+    __syncthreads();
+    cplx acc[24];
+#pragma unroll
+    for (int c = 0; c < 24; ++c) acc[c] = czero();
+    tile_apply<24>(sT, sX, k, adj, row, grp, acc);
+    for (int c = 0; c < k; ++c) sPart[(grp * k + c) * TILE + row] = acc[c];
+    __syncthreads();
+    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+      const int rr = q % TILE, c = q / TILE;
+      cplx v = sAcc[c * TILE + rr];
+      v = csub(v, sPart[(0 * k + c) * TILE + rr]);
+      v = csub(v, sPart[(1 * k + c) * TILE + rr]);
+      v = csub(v, sPart[(2 * k + c) * TILE + rr]);
+      v = csub(v, sPart[(3 * k + c) * TILE + rr]);
+      sAcc[c * TILE + rr] = v;
+    }
+  }
+  // X_b = Dinv_b · acc  (adj: Dinv_bᴴ · acc)
+  __syncthreads();
+  load_tile(sT, Dinv + (int64_t)b * TILE * TILE, adj);
+  __syncthreads();
+  {
+    cplx acc[24];
+#pragma unroll
+    for (int c = 0; c < 24; ++c) acc[c] = czero();
+    tile_apply<24>(sT, sAcc, k, adj, row, grp, acc);
+    for (int c = 0; c < k; ++c) sPart[(grp * k + c) * TILE + row] = acc[c];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+    const int rr = q % TILE, c = q / TILE;
+    cplx v = sPart[(0 * k + c) * TILE + rr];
+    v = cadd(v, sPart[(1 * k + c) * TILE + rr]);
+    v = cadd(v, sPart[(2 * k + c) * TILE + rr]);
+    v = cadd(v, sPart[(3 * k + c) * TILE + rr]);
+    X[(int64_t)c * ldx + (int64_t)b * TILE + rr] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) st_release(&flags[b], epoch);
+}
+
+// Y[:, 0:k] = lam[j] * Y[:, j] - X[:, j]  (side 'L') or Y - X*lam (side 'S');
+// also per-CTA partial |Y[:,0]|^2.
+__global__ void k_residual_fix(int64_t nrows, cplx* Y, int64_t ldy, const cplx* X, int64_t ldx, int k,
+                               const double* lam, int sideL, double* col0_part) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double c0 = 0.0;
+  if (row < nrows) {
+    for (int j = 0; j < k; ++j) {
+      const cplx y = Y[(int64_t)j * ldy + row], x = X[(int64_t)j * ldx + row];
+      const cplx o = sideL ? csub(cscale(y, lam[j]), x) : csub(y, cscale(x, lam[j]));
+      Y[(int64_t)j * ldy + row] = o;
+      if (j == 0) c0 = cabs2(o);
+    }
+  }
+  __shared__ double red[32];
+  const double s = block_sum(c0, red);
+  if (threadIdx.x == 0 && col0_part) col0_part[blockIdx.x] = s;
+}
+
+// Column-range copy for block shifts: dst[:, j] = src[:, j] for j < ncols.
+__global__ void k_copy_cols(int64_t nrows, int ncols, const cplx* __restrict__ src, int64_t lds,
+                            cplx* __restrict__ dst, int64_t ldd) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (row < nrows && c < ncols) dst[(int64_t)c * ldd + row] = src[(int64_t)c * lds + row];
+}
+
+// Sum of n doubles into out[0] (deterministic, one CTA).
+__global__ void k_sum(const double* __restrict__ v, int n, double* out) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[i];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[0] = s;
+}

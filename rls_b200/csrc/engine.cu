@@ -1,0 +1,1178 @@
+// σ_min(C − zI) grid engine: host orchestration of the device kernels and the C ABI.
+//
+// The per-grid-point loop follows _psTriRecy_impl (src/core/psTriRecy.jl:708-881) on
+// the dense Schur factor (M = T upper triangular, S = I).  With S = I the reference's
+// cached products satisfy J3 = S'J5 = J5, J4 = V and J6 = SV = V exactly, so the
+// device keeps V, J1 = TᴴTV, J2 = TᴴV and J5 = TV only.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rls_b200.h"
+#include "blas.cuh"
+#include "heev.cuh"
+#include "rotate.cuh"
+#include "small.cuh"
+
+namespace {
+
+constexpr double kEps = 2.220446049250313e-16;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct rls_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  rls_log_fn log_fn = nullptr;
+  void* log_user = nullptr;
+  int verbose = 0;
+
+  // operator
+  int64_t n = 0, n_pad = 0;
+  int nb = 0;
+  cplx* T = nullptr;        // tiles
+  cplx* Dinv = nullptr;     // nb tiles
+  cplx z_dinv = cmk(NAN, NAN);
+  int* flags = nullptr;     // nb
+  int* ticket = nullptr;    // 1
+  int epoch = 0;
+  int* trmm_uO[2] = {nullptr, nullptr};
+  int* trmm_us[2] = {nullptr, nullptr};
+  int* trmm_Ofirst[2] = {nullptr, nullptr};
+  int* trmm_Ocount[2] = {nullptr, nullptr};
+  int trmm_units[2] = {0, 0};
+  cplx* trmm_part = nullptr;
+
+  // generic workspaces
+  int* derr = nullptr;             // device error word
+  double* dscal = nullptr;         // small scalars (256)
+  cplx* gram_part = nullptr;
+  size_t gram_part_elems = 0;
+  cplx* tsqr_stack[2] = {nullptr, nullptr};
+  size_t tsqr_stack_elems = 0;
+  cplx* small[8] = {};             // small k×k / pr×k scratch (kmax × 64 each)
+  cplx* owW = nullptr;             // orth_robust W output (pr_max × 8)
+  cplx* owR = nullptr;             // orth_robust / QR R output (64 × 64)
+  cplx* svdA = nullptr;            // Jacobi SVD scratch beyond 80 columns (pr_max²)
+  cplx* svdV = nullptr;
+  cplx* gemm_tmp = nullptr;        // n_pad × 64 scratch for in-place products wider than 32
+  int gemm_tmp_cols = 0;
+  int small_dim = 0;
+  double* colpart = nullptr;       // per-CTA partial sums
+  cplx* tall_tmp = nullptr;        // n_pad × tmp_cols
+  int tall_tmp_cols = 0;
+  cplx* house_tau = nullptr;
+
+  // recycled space
+  int r = 0, p_max = 0, pr_max = 0, p = 0;
+  std::vector<rls_c64> pts;
+  cplx *V = nullptr, *J1 = nullptr, *J2 = nullptr, *J5 = nullptr, *shift_tmp = nullptr;
+  cplx *L = nullptr, *H1 = nullptr, *H2 = nullptr, *Hs = nullptr;  // pr_max²
+  cplx* Ulist = nullptr;
+  // heev
+  HeevWork heev{};
+  cplx* Gheev = nullptr;  // pr_max × pr_max
+  int* rr_dev = nullptr;
+  double* lam_dev = nullptr;
+  cplx* zdev = nullptr;
+  double* taudev = nullptr;
+  // recycle step
+  cplx* CzX = nullptr;    // n_pad × pr_max (first rr columns used)
+  cplx* Gtot = nullptr;   // pr_max × r
+  double* sig_rec = nullptr;  // pr_max
+  // LOBPCG keep
+  cplx *S = nullptr, *CS = nullptr;   // n_pad × 3r
+  cplx *Gk = nullptr, *Rk = nullptr;  // 3r × 3r
+  double *sig = nullptr, *lam = nullptr;
+
+  std::vector<DevBuf> owned;
+};
+
+namespace {
+
+void set_err(rls_ctx* c, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      set_err(ctx, "CUDA error %s at %s:%d", cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return RLS_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)
+
+#define RET(x)               \
+  do {                       \
+    int s_ = (x);            \
+    if (s_ != RLS_OK) return s_; \
+  } while (0)
+
+int dalloc(rls_ctx* ctx, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    set_err(ctx, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return RLS_ERR_NOMEM;
+  }
+  ctx->owned.push_back({*p, bytes});
+  CK(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
+  return RLS_OK;
+}
+
+template <class T>
+int dalloc_t(rls_ctx* ctx, T** p, size_t count) {
+  return dalloc(ctx, reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+void dfree(rls_ctx* ctx, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < ctx->owned.size(); ++i)
+    if (ctx->owned[i].p == p) {
+      cudaFree(p);
+      ctx->owned.erase(ctx->owned.begin() + i);
+      return;
+    }
+}
+
+int check_launch(rls_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_err(ctx, "launch of %s failed: %s", what, cudaGetErrorString(e));
+    return RLS_ERR_CUDA;
+  }
+  return RLS_OK;
+}
+
+int sync_and_check(rls_ctx* ctx) {
+  CK(cudaStreamSynchronize(ctx->stream));
+  int h = 0;
+  CK(cudaMemcpy(&h, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    CK(cudaMemset(ctx->derr, 0, sizeof(int)));
+    if (h & DEVERR_SPIN_TIMEOUT) {
+      set_err(ctx, "a bounded device wait expired in the triangular solve");
+      return RLS_ERR_TIMEOUT;
+    }
+    if (h & DEVERR_SIZE) {
+      set_err(ctx, "device kernel received sizes beyond its limits");
+      return RLS_ERR_DIM;
+    }
+    if (h & DEVERR_NONFINITE) {
+      set_err(ctx, "non-finite values in a device factorization (singular shifted factor?)");
+      return RLS_ERR_BREAKDOWN;
+    }
+    // DEVERR_BREAKDOWN: Cholesky needed its shift; reported but not fatal (the reference warns).
+  }
+  return RLS_OK;
+}
+
+template <class T>
+int d2h(rls_ctx* ctx, T* h, const T* d, size_t count) {
+  CK(cudaMemcpyAsync(h, d, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}
+
+// ---------------------------------------------------------------------------------
+// Generic launch helpers
+// ---------------------------------------------------------------------------------
+
+// C (k1×k2, ldc) = alpha AᴴB + beta C, A: nrows×k1, B: nrows×k2 (k2 <= 32 per pass).
+int gram(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k1, const cplx* B, int64_t ldb, int k2,
+         cplx* C, int64_t ldc, cplx alpha = cmk(1, 0), cplx beta = cmk(0, 0)) {
+  if (k1 <= 0 || k2 <= 0) return RLS_OK;
+  const int64_t chunk = 512;
+  const int nchunks = (int)((nrows + chunk - 1) / chunk);
+  for (int j0 = 0; j0 < k2; j0 += 32) {
+    const int kk2 = std::min(32, k2 - j0);
+    if ((size_t)nchunks * k1 * kk2 > ctx->gram_part_elems) {
+      set_err(ctx, "gram workspace too small (%d×%d×%d)", nchunks, k1, kk2);
+      return RLS_ERR_DIM;
+    }
+    dim3 grid(nchunks, (k1 + 7) / 8);
+    k_gram_partial<<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
+                                                  ctx->gram_part);
+    RET(check_launch(ctx, "k_gram_partial"));
+    const int tot = k1 * kk2;
+    k_gram_reduce<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(nchunks, k1, kk2, ctx->gram_part, alpha, beta,
+                                                              C + (int64_t)j0 * ldc, ldc);
+    RET(check_launch(ctx, "k_gram_reduce"));
+  }
+  return RLS_OK;
+}
+
+// C = alpha (Σ coef_q A_q) B + beta C, optionally X = A_xsrc B and C -= X diag(sig²),
+// optional per-CTA |C[:,0]|² partials into ctx->colpart (returns the CTA count).
+int gemm_rows(rls_ctx* ctx, int64_t nrows, CombSrc src, int64_t lda, int k1, const cplx* B, int64_t ldb, int k2,
+              cplx* C, int64_t ldc, cplx alpha = cmk(1, 0), cplx beta = cmk(0, 0), int xsrc = -1,
+              cplx* X = nullptr, int64_t ldx = 0, const double* s2 = nullptr, bool col0 = false,
+              int* nparts = nullptr) {
+  if (k2 <= 0) return RLS_OK;
+  if (k2 > 32) {
+    if (col0 || xsrc >= 0) {
+      set_err(ctx, "gemm_rows: epilogue with k2 > 32 unsupported");
+      return RLS_ERR_DIM;
+    }
+    bool alias = false;
+    for (int q = 0; q < src.nsrc; ++q) alias |= (src.a[q] == C);
+    if (alias) {  // column chunks would read columns already overwritten: go through scratch
+      if (k2 > ctx->gemm_tmp_cols || beta.x != 0.0 || beta.y != 0.0) {
+        set_err(ctx, "gemm_rows: in-place product with %d > 32 columns unsupported", k2);
+        return RLS_ERR_DIM;
+      }
+      RET(gemm_rows(ctx, nrows, src, lda, k1, B, ldb, k2, ctx->gemm_tmp, ctx->n_pad, alpha, beta));
+      CK(cudaMemcpy2DAsync(C, ldc * sizeof(cplx), ctx->gemm_tmp, ctx->n_pad * sizeof(cplx), nrows * sizeof(cplx), k2,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+      return RLS_OK;
+    }
+    for (int j0 = 0; j0 < k2; j0 += 32)
+      RET(gemm_rows(ctx, nrows, src, lda, k1, B + (int64_t)j0 * ldb, ldb, std::min(32, k2 - j0),
+                    C + (int64_t)j0 * ldc, ldc, alpha, beta));
+    return RLS_OK;
+  }
+  const int threads = 128;
+  const int blocks = (int)((nrows + threads - 1) / threads);
+  const size_t smem = 32 * (size_t)k2 * sizeof(cplx);
+  double* cp = col0 ? ctx->colpart : nullptr;
+  if (k2 <= 8)
+    k_gemm_rows<8><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
+                                                           xsrc, X, ldx, s2, cp);
+  else if (k2 <= 16)
+    k_gemm_rows<16><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
+                                                            xsrc, X, ldx, s2, cp);
+  else
+    k_gemm_rows<32><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
+                                                            xsrc, X, ldx, s2, cp);
+  if (nparts) *nparts = blocks;
+  return check_launch(ctx, "k_gemm_rows");
+}
+
+CombSrc one_src(const cplx* a) {
+  CombSrc s{};
+  s.a[0] = a;
+  s.coef[0] = cmk(1, 0);
+  s.nsrc = 1;
+  return s;
+}
+
+int small_gemm(rls_ctx* ctx, int m, int n, int kk, cplx alpha, const cplx* A, int lda, int opA, const cplx* B,
+               int ldb, int opB, cplx beta, cplx* C, int ldc) {
+  const int tot = m * n;
+  const int blocks = std::min(64, (tot + 255) / 256);
+  k_small_gemm<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(m, n, kk, alpha, A, lda, opA, B, ldb, opB, beta, C,
+                                                             ldc);
+  return check_launch(ctx, "k_small_gemm");
+}
+
+// R (k×k, ld k) of the QR factorisation of A (nrows × k) by TSQR (k <= 64), else
+// by one CTA in global memory (A is then copied to tall_tmp first).
+int tsqr_r(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k, cplx* R) {
+  if (k <= 64) {
+    // mb >= 2k guarantees every level shrinks the stack (m' = ceil(m/mb)·k < m for m > mb).
+    int mb = std::max(2 * k, std::min(1024, (int)(196608 / (k * (int)sizeof(cplx)))));
+    const cplx* src = A;
+    int64_t m = nrows, ld = lda;
+    int which = 0;
+    while (true) {
+      const int nleaf = (int)((m + mb - 1) / mb);
+      cplx* dst = (nleaf == 1) ? R : ctx->tsqr_stack[which];
+      const int64_t ldd = (nleaf == 1) ? k : (int64_t)nleaf * k;
+      if (nleaf > 1 && (size_t)nleaf * k * k > ctx->tsqr_stack_elems) {
+        set_err(ctx, "tsqr workspace too small");
+        return RLS_ERR_DIM;
+      }
+      const size_t smem = ((size_t)mb * k + 2 * k) * sizeof(cplx);
+      k_tsqr_leaf<<<nleaf, 256, smem, ctx->stream>>>(m, k, mb, src, ld, dst, ldd);
+      RET(check_launch(ctx, "k_tsqr_leaf"));
+      if (nleaf == 1) break;
+      if ((int64_t)nleaf * k >= m) {
+        set_err(ctx, "tsqr: stack does not shrink (m=%lld, k=%d, mb=%d)", (long long)m, k, mb);
+        return RLS_ERR_DIM;
+      }
+      src = dst;
+      m = (int64_t)nleaf * k;
+      ld = m;
+      which ^= 1;
+    }
+    return RLS_OK;
+  }
+  if ((int64_t)ctx->tall_tmp_cols < k) {
+    set_err(ctx, "QR of %d columns exceeds the workspace", k);
+    return RLS_ERR_DIM;
+  }
+  if (A != ctx->tall_tmp)
+    CK(cudaMemcpy2DAsync(ctx->tall_tmp, ctx->n_pad * sizeof(cplx), A, lda * sizeof(cplx), nrows * sizeof(cplx), k,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  k_house_r_global<<<1, 512, 0, ctx->stream>>>((int)nrows, k, ctx->tall_tmp, (int)ctx->n_pad, ctx->house_tau,
+                                               ctx->house_tau + ctx->pr_max, R, k);
+  return check_launch(ctx, "k_house_r_global");
+}
+
+// X (nrows × k) ← Q of its QR factorisation; if R != nullptr, R (k×k, ld k) ← R.
+// Householder TSQR gives R1; X ← X R1⁻¹; one CholQR pass restores orthogonality.
+int orth_qr(rls_ctx* ctx, int64_t nrows, cplx* X, int64_t ldx, int k, cplx* R) {
+  cplx* R1 = ctx->small[0];
+  cplx* R1i = ctx->small[1];
+  cplx* G = ctx->small[2];
+  cplx* R2 = ctx->small[3];
+  cplx* R2i = ctx->small[4];
+  RET(tsqr_r(ctx, nrows, X, ldx, k, R1));
+  k_trtri<<<1, 256, 2 * k * k * sizeof(cplx), ctx->stream>>>(k, R1, R1i, ctx->derr);
+  RET(check_launch(ctx, "k_trtri"));
+  RET(gemm_rows(ctx, nrows, one_src(X), ldx, k, R1i, k, k, X, ldx));
+  RET(gram(ctx, nrows, X, ldx, k, X, ldx, k, G, k));
+  k_chol_inv<<<1, 256, 3 * k * k * sizeof(cplx), ctx->stream>>>(k, nrows, G, k, R2, R2i, nullptr, ctx->derr);
+  RET(check_launch(ctx, "k_chol_inv"));
+  RET(gemm_rows(ctx, nrows, one_src(X), ldx, k, R2i, k, k, X, ldx));
+  if (R) RET(small_gemm(ctx, k, k, k, cmk(1, 0), R2, k, 0, R1, k, 0, cmk(0, 0), R, k));  // R is never small[0..4]
+  return RLS_OK;
+}
+
+// rls_orth! (RLSLinearAlgebra.jl:1127-1160): two passes of block CGS of X against V.
+int orth_twice(rls_ctx* ctx, int64_t nrows, const cplx* V, int64_t ldv, int nV, cplx* X, int64_t ldx, int nX) {
+  cplx* W = ctx->small[5];
+  for (int pass = 0; pass < 2; ++pass) {
+    RET(gram(ctx, nrows, V, ldv, nV, X, ldx, nX, W, nV));
+    RET(gemm_rows(ctx, nrows, one_src(V), ldv, nV, W, nV, nX, X, ldx, cmk(-1, 0), cmk(1, 0)));
+    RET(orth_qr(ctx, nrows, X, ldx, nX, nullptr));
+  }
+  return RLS_OK;
+}
+
+// rls_orth_robust! (RLSLinearAlgebra.jl:1225-1284) with W (nV×nX, ld nV) and R (nX×nX)
+// accumulated on the device; the adaptive stop needs |VᴴX|_F, read back per pass.
+int orth_robust(rls_ctx* ctx, int64_t nrows, const cplx* V, int64_t ldv, int nV, cplx* X, int64_t ldx, int nX,
+                cplx* Wout, cplx* Rout) {
+  cplx* Wk = ctx->small[5];
+  cplx* Rk = ctx->small[6];
+  cplx* tmpW = ctx->small[7];
+  const double tol = kEps * std::sqrt((double)nV);
+  bool have_wk = false;
+  for (int it = 1; it <= 4; ++it) {
+    if (nV > 0 && !have_wk) RET(gram(ctx, nrows, V, ldv, nV, X, ldx, nX, Wk, nV));
+    if (nV > 0) RET(gemm_rows(ctx, nrows, one_src(V), ldv, nV, Wk, nV, nX, X, ldx, cmk(-1, 0), cmk(1, 0)));
+    RET(orth_qr(ctx, nrows, X, ldx, nX, Rk));
+    if (it == 1) {
+      if (Wout && nV > 0) CK(cudaMemcpyAsync(Wout, Wk, sizeof(cplx) * nV * nX, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (Rout) CK(cudaMemcpyAsync(Rout, Rk, sizeof(cplx) * nX * nX, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+      if (Wout && nV > 0) RET(small_gemm(ctx, nV, nX, nX, cmk(1, 0), Wk, nV, 0, Rout, nX, 0, cmk(1, 0), Wout, nV));
+      if (Rout) {
+        RET(small_gemm(ctx, nX, nX, nX, cmk(1, 0), Rk, nX, 0, Rout, nX, 0, cmk(0, 0), tmpW, nX));
+        CK(cudaMemcpyAsync(Rout, tmpW, sizeof(cplx) * nX * nX, cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+    }
+    if (nV == 0) {
+      if (it >= 2) break;  // |VᴴX| = 0 <= tol
+      continue;
+    }
+    RET(gram(ctx, nrows, V, ldv, nV, X, ldx, nX, Wk, nV));
+    have_wk = true;
+    if (it >= 2) {
+      std::vector<cplx> h((size_t)nV * nX);
+      RET(d2h(ctx, h.data(), Wk, h.size()));
+      double s = 0.0;
+      for (auto& v : h) s += v.x * v.x + v.y * v.y;
+      if (std::sqrt(s) <= tol) break;
+    }
+  }
+  return RLS_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Triangular operator (tiled Schur factor)
+// ---------------------------------------------------------------------------------
+
+int ensure_dinv(rls_ctx* ctx, cplx z) {
+  if (ctx->z_dinv.x == z.x && ctx->z_dinv.y == z.y) return RLS_OK;
+  const size_t smem = 2 * TILE * TILE * sizeof(cplx);
+  k_diag_inv<<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->n, ctx->T, z, ctx->Dinv, ctx->derr);
+  RET(check_launch(ctx, "k_diag_inv"));
+  ctx->z_dinv = z;
+  return RLS_OK;
+}
+
+// X = R⁻¹ B (adj=0) or R⁻ᴴ B (adj=1), R = T − zI; X may alias B; k <= 24.
+int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int k) {
+  RET(ensure_dinv(ctx, z));
+  if (k > 24) {
+    for (int c0 = 0; c0 < k; c0 += 24)
+      RET(trsm(ctx, z, adj, B + (int64_t)c0 * ld, X + (int64_t)c0 * ld, ld, std::min(24, k - c0)));
+    return RLS_OK;
+  }
+  ctx->epoch += 1;
+  if (ctx->epoch > (1 << 30)) {
+    ctx->epoch = 1;
+    CK(cudaMemsetAsync(ctx->flags, 0, sizeof(int) * ctx->nb, ctx->stream));
+  }
+  CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(int), ctx->stream));
+  const size_t smem = ((size_t)TILE * TILE_LDS + 6 * (size_t)TILE * k) * sizeof(cplx);
+  k_trsm_dataflow<<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
+                                                       ctx->flags, ctx->epoch, ctx->derr);
+  return check_launch(ctx, "k_trsm_dataflow");
+}
+
+// Y = T X (adj=0) or Tᴴ X (adj=1); k <= 16.
+int trmm(rls_ctx* ctx, int adj, const cplx* X, cplx* Y, int64_t ld, int k) {
+  const size_t smem = ((size_t)TILE * TILE_LDS + (size_t)TILE * k) * sizeof(cplx);
+  k_trmm_partial<<<ctx->trmm_units[adj], 256, smem, ctx->stream>>>(ctx->nb, ctx->T, X, ld, k, adj,
+                                                                   ctx->trmm_uO[adj], ctx->trmm_us[adj],
+                                                                   ctx->trmm_part);
+  RET(check_launch(ctx, "k_trmm_partial"));
+  k_trmm_reduce<<<ctx->nb, 256, 0, ctx->stream>>>(ctx->nb, k, ctx->trmm_Ofirst[adj], ctx->trmm_Ocount[adj],
+                                                  ctx->trmm_part, Y, ld);
+  return check_launch(ctx, "k_trmm_reduce");
+}
+
+// ---------------------------------------------------------------------------------
+// Workspace set-up
+// ---------------------------------------------------------------------------------
+
+void release_space(rls_ctx* ctx) {
+  cplx** bufs[] = {&ctx->V, &ctx->J1, &ctx->J2, &ctx->J5, &ctx->shift_tmp, &ctx->L, &ctx->H1, &ctx->H2, &ctx->Hs,
+                   &ctx->Ulist, &ctx->heev.A, &ctx->Gheev, &ctx->CzX, &ctx->Gtot, &ctx->S, &ctx->CS, &ctx->Gk,
+                   &ctx->Rk, &ctx->tall_tmp, &ctx->gram_part, &ctx->tsqr_stack[0], &ctx->tsqr_stack[1],
+                   &ctx->house_tau, &ctx->zdev, &ctx->owW, &ctx->owR, &ctx->svdA, &ctx->svdV, &ctx->gemm_tmp};
+  for (cplx** b : bufs) { dfree(ctx, *b); *b = nullptr; }
+  double** dbufs[] = {&ctx->heev.lu, &ctx->lam_dev, &ctx->taudev, &ctx->sig_rec, &ctx->sig, &ctx->lam};
+  for (double** b : dbufs) { dfree(ctx, *b); *b = nullptr; }
+  dfree(ctx, ctx->rr_dev);
+  ctx->rr_dev = nullptr;
+  for (int i = 0; i < 8; ++i) { dfree(ctx, ctx->small[i]); ctx->small[i] = nullptr; }
+  ctx->r = 0;
+  ctx->p_max = 0;
+  ctx->p = 0;
+}
+
+int setup_space(rls_ctx* ctx, int r, int p_max) {
+  if (ctx->r == r && ctx->p_max == p_max && ctx->V) {
+    ctx->p = 0;
+    ctx->pts.assign(p_max, rls_c64{0, 0});
+    return RLS_OK;
+  }
+  release_space(ctx);
+  ctx->r = r;
+  ctx->p_max = p_max;
+  ctx->pr_max = r * p_max;
+  ctx->p = 0;
+  ctx->pts.assign(p_max, rls_c64{0, 0});
+  const int64_t np = ctx->n_pad;
+  const int prm = ctx->pr_max;
+  RET(dalloc_t(ctx, &ctx->V, (size_t)np * prm));
+  RET(dalloc_t(ctx, &ctx->J1, (size_t)np * prm));
+  RET(dalloc_t(ctx, &ctx->J2, (size_t)np * prm));
+  RET(dalloc_t(ctx, &ctx->J5, (size_t)np * prm));
+  RET(dalloc_t(ctx, &ctx->shift_tmp, (size_t)np * prm));
+  RET(dalloc_t(ctx, &ctx->L, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->H1, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->H2, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->Hs, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->Ulist, (size_t)p_max * 4 * r * r));
+  RET(dalloc_t(ctx, &ctx->heev.A, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->heev.lu, (size_t)16 * 6 * prm));
+  RET(dalloc_t(ctx, &ctx->Gheev, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->rr_dev, 4));
+  RET(dalloc_t(ctx, &ctx->lam_dev, (size_t)prm));
+  RET(dalloc_t(ctx, &ctx->zdev, 4));
+  RET(dalloc_t(ctx, &ctx->taudev, 4));
+  RET(dalloc_t(ctx, &ctx->CzX, (size_t)np * std::min(prm, 64)));
+  RET(dalloc_t(ctx, &ctx->Gtot, (size_t)prm * r));
+  RET(dalloc_t(ctx, &ctx->sig_rec, (size_t)prm));
+  RET(dalloc_t(ctx, &ctx->S, (size_t)np * 3 * r));
+  RET(dalloc_t(ctx, &ctx->CS, (size_t)np * 3 * r));
+  RET(dalloc_t(ctx, &ctx->Gk, (size_t)9 * r * r));
+  RET(dalloc_t(ctx, &ctx->Rk, (size_t)9 * r * r));
+  RET(dalloc_t(ctx, &ctx->sig, (size_t)3 * r));
+  RET(dalloc_t(ctx, &ctx->lam, (size_t)3 * r));
+  ctx->tall_tmp_cols = std::max(prm, 2 * r);
+  RET(dalloc_t(ctx, &ctx->tall_tmp, (size_t)np * ctx->tall_tmp_cols));
+  const int kmax = std::max(prm, 3 * r);
+  ctx->gram_part_elems = (size_t)((np + 511) / 512) * kmax * 32;
+  RET(dalloc_t(ctx, &ctx->gram_part, ctx->gram_part_elems));
+  ctx->tsqr_stack_elems = (size_t)((np + 63) / 64 + 2) * 64 * 64;
+  RET(dalloc_t(ctx, &ctx->tsqr_stack[0], ctx->tsqr_stack_elems));
+  RET(dalloc_t(ctx, &ctx->tsqr_stack[1], ctx->tsqr_stack_elems));
+  RET(dalloc_t(ctx, &ctx->house_tau, (size_t)2 * prm + 64));
+  ctx->small_dim = kmax;
+  for (int i = 0; i < 8; ++i) RET(dalloc_t(ctx, &ctx->small[i], (size_t)kmax * std::max(kmax, 64) + 64));
+  RET(dalloc_t(ctx, &ctx->owW, (size_t)prm * 8 + 64));
+  RET(dalloc_t(ctx, &ctx->owR, (size_t)64 * 64));
+  RET(dalloc_t(ctx, &ctx->svdA, (size_t)prm * prm));
+  RET(dalloc_t(ctx, &ctx->svdV, (size_t)prm * prm));
+  ctx->gemm_tmp_cols = 64;
+  RET(dalloc_t(ctx, &ctx->gemm_tmp, (size_t)np * 64));
+  return RLS_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// LOBPCG on C = InvMat(adjoint(T − zI)), K = I (lobpcgSvd.jl:365-477)
+// ---------------------------------------------------------------------------------
+
+struct LobpcgResult {
+  double sigma;
+  int64_t it;
+};
+
+// S[:, 0:r] holds X0 on entry.
+int lobpcg_invtri(rls_ctx* ctx, cplx z, int r, int64_t maxit, double tol, bool sideL, LobpcgResult* res) {
+  const int64_t np = ctx->n_pad;
+  cplx* S = ctx->S;
+  cplx* CS = ctx->CS;
+  cplx *X = S, *P = S + np * r, *W = S + 2 * np * r;
+  cplx *CX = CS, *CP = CS + np * r, *CW = CS + 2 * np * r;
+  const int adjC = 1;   // C X = R⁻ᴴ X
+  const int adjCt = 0;  // Cᴴ Y = R⁻¹ Y
+  auto svd_rr = [&](cplx* CSv, int nS) -> int {
+    RET(tsqr_r(ctx, np, CSv, np, nS, ctx->Rk));
+    k_svd_rr<<<1, 256, svd_rr_smem_bytes(nS, r, false), ctx->stream>>>(nS, r, sideL ? 1 : 0, 1, ctx->Rk, nS, ctx->sig,
+                                                                    ctx->lam, ctx->Gk, 3 * r, nullptr, nullptr);
+    return check_launch(ctx, "k_svd_rr");
+  };
+  auto residual = [&](cplx* Wd, double* w0) -> int {
+    RET(trsm(ctx, z, adjCt, CX, Wd, np, r));
+    const int threads = 256;
+    const int blocks = (int)((np + threads - 1) / threads);
+    k_residual_fix<<<blocks, threads, 0, ctx->stream>>>(np, Wd, np, X, np, r, ctx->lam, sideL ? 1 : 0, ctx->colpart);
+    RET(check_launch(ctx, "k_residual_fix"));
+    if (w0) {
+      k_sum<<<1, 256, 0, ctx->stream>>>(ctx->colpart, blocks, ctx->dscal);
+      RET(check_launch(ctx, "k_sum"));
+    }
+    return RLS_OK;
+  };
+  // iteration "0"
+  RET(orth_qr(ctx, np, X, np, r, nullptr));
+  RET(trsm(ctx, z, adjC, X, CX, np, r));
+  RET(svd_rr(CX, r));
+  RET(gemm_rows(ctx, np, one_src(X), np, r, ctx->Gk, 3 * r, r, X, np));
+  RET(gemm_rows(ctx, np, one_src(CX), np, r, ctx->Gk, 3 * r, r, CX, np));
+  RET(residual(P, nullptr));
+  RET(orth_twice(ctx, np, X, np, r, P, np, r));
+  RET(trsm(ctx, z, adjC, P, CP, np, r));
+  for (int64_t i = 1; i <= maxit; ++i) {
+    if (i == 1) {
+      RET(svd_rr(CS, 2 * r));
+      RET(gemm_rows(ctx, np, one_src(S), np, 2 * r, ctx->Gk, 3 * r, 2 * r, S, np));
+      RET(gemm_rows(ctx, np, one_src(CS), np, 2 * r, ctx->Gk, 3 * r, 2 * r, CS, np));
+    } else {
+      RET(svd_rr(CS, 3 * r));
+      RET(gemm_rows(ctx, np, one_src(S), np, 3 * r, ctx->Gk, 3 * r, 2 * r, S, np));
+      RET(gemm_rows(ctx, np, one_src(CS), np, 3 * r, ctx->Gk, 3 * r, 2 * r, CS, np));
+    }
+    double w0 = 0.0;
+    RET(residual(W, &w0));
+    double hs[2];
+    RET(d2h(ctx, hs, ctx->dscal, 1));
+    double s0;
+    RET(d2h(ctx, &s0, ctx->sig, 1));
+    const double wn = std::sqrt(hs[0]);
+    // check_conv_svd, side 'L' (lobpcgSvd.jl:329-331): |W[:,1]| < tol
+    if (wn < tol) {
+      res->sigma = sideL ? 1.0 / s0 : s0;
+      res->it = i;
+      return RLS_OK;
+    }
+    RET(orth_twice(ctx, np, S, np, 2 * r, W, np, r));
+    RET(trsm(ctx, z, adjC, W, CW, np, r));
+  }
+  double s0;
+  RET(d2h(ctx, &s0, ctx->sig, 1));
+  res->sigma = sideL ? 1.0 / s0 : s0;
+  res->it = maxit;
+  return RLS_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Recycled space (updateRecycledSpace!, recySpace.jl:160-223)
+// ---------------------------------------------------------------------------------
+
+int copy_cols(rls_ctx* ctx, const cplx* src, cplx* dst, int ncols) {
+  if (ncols <= 0) return RLS_OK;
+  dim3 grid((unsigned)((ctx->n_pad + 255) / 256), ncols);
+  k_copy_cols<<<grid, 256, 0, ctx->stream>>>(ctx->n_pad, ncols, src, ctx->n_pad, dst, ctx->n_pad);
+  return check_launch(ctx, "k_copy_cols");
+}
+
+int shift_blocks(rls_ctx* ctx, int l) {  // _shift_blocks! (recySpace.jl:290-340)
+  const int p = ctx->p, r = ctx->r, nk = (p - l) * r;
+  const int64_t np = ctx->n_pad;
+  const int ld = ctx->pr_max;
+  for (int i = 0; i < p - l; ++i) ctx->pts[i] = ctx->pts[i + l];
+  for (cplx* A : {ctx->V, ctx->J1, ctx->J2, ctx->J5}) {
+    RET(copy_cols(ctx, A + (int64_t)l * r * np, ctx->shift_tmp, nk));
+    RET(copy_cols(ctx, ctx->shift_tmp, A, nk));
+  }
+  for (cplx* M : {ctx->L, ctx->H1, ctx->H2}) {
+    CK(cudaMemcpy2DAsync(ctx->Hs, ld * sizeof(cplx), M + (int64_t)l * r * ld + l * r, ld * sizeof(cplx),
+                         nk * sizeof(cplx), nk, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpy2DAsync(M, ld * sizeof(cplx), ctx->Hs, ld * sizeof(cplx), nk * sizeof(cplx), nk,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  ctx->p = p - l;
+  return RLS_OK;
+}
+
+__global__ void k_conj_transpose(int m, int n, const cplx* A, int lda, cplx* B, int ldb) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m * n; q += gridDim.x * blockDim.x) {
+    const int i = q % m, j = q / m;
+    B[(int64_t)i * ldb + j] = cconj(A[(int64_t)j * lda + i]);
+  }
+}
+
+int add_blocks(rls_ctx* ctx, const cplx* Xin, cplx z) {  // _add_blocks! (recySpace.jl:344-453)
+  const int p = ctx->p, r = ctx->r, pr = p * r;
+  const int64_t np = ctx->n_pad;
+  const int ld = ctx->pr_max;
+  cplx* Vn = ctx->V + (int64_t)pr * np;
+  cplx* J5n = ctx->J5 + (int64_t)pr * np;
+  cplx* J1n = ctx->J1 + (int64_t)pr * np;
+  cplx* J2n = ctx->J2 + (int64_t)pr * np;
+  RET(copy_cols(ctx, Xin, Vn, r));
+  cplx* Lnn = ctx->L + (int64_t)pr * ld + pr;
+  cplx* Lon = ctx->L + (int64_t)pr * ld;
+  if (p > 0) {
+    RET(orth_robust(ctx, np, ctx->V, np, pr, Vn, np, r, ctx->owW, ctx->owR));
+    CK(cudaMemcpy2DAsync(Lon, ld * sizeof(cplx), ctx->owW, pr * sizeof(cplx), pr * sizeof(cplx), r,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpy2DAsync(Lnn, ld * sizeof(cplx), ctx->owR, r * sizeof(cplx), r * sizeof(cplx), r,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    RET(orth_qr(ctx, np, Vn, np, r, ctx->owR));
+    CK(cudaMemcpy2DAsync(Lnn, ld * sizeof(cplx), ctx->owR, r * sizeof(cplx), r * sizeof(cplx), r,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  // J5 = M V_new; [J1 J2] = Mᴴ [J5 V_new]   (mul_coupled_ms!, recySpace.jl:368-380)
+  RET(trmm(ctx, 0, Vn, J5n, np, r));
+  RET(copy_cols(ctx, J5n, ctx->tall_tmp, r));
+  RET(copy_cols(ctx, Vn, ctx->tall_tmp + (int64_t)r * np, r));
+  RET(trmm(ctx, 1, ctx->tall_tmp, ctx->tall_tmp, np, 2 * r));
+  RET(copy_cols(ctx, ctx->tall_tmp, J1n, r));
+  RET(copy_cols(ctx, ctx->tall_tmp + (int64_t)r * np, J2n, r));
+  // H blocks (recySpace.jl:392-417)
+  RET(gram(ctx, np, Vn, np, r, J1n, np, r, ctx->H1 + (int64_t)pr * ld + pr, ld));
+  RET(gram(ctx, np, Vn, np, r, J2n, np, r, ctx->H2 + (int64_t)pr * ld + pr, ld));
+  if (p > 0) {
+    RET(gram(ctx, np, ctx->J1, np, pr, Vn, np, r, ctx->H1 + (int64_t)pr * ld, ld));   // H1[old,new]
+    RET(gram(ctx, np, ctx->J5, np, pr, Vn, np, r, ctx->H2 + (int64_t)pr * ld, ld));   // H2[old,new] (J3 = J5)
+    k_conj_transpose<<<64, 256, 0, ctx->stream>>>(pr, r, ctx->H1 + (int64_t)pr * ld, ld, ctx->H1 + pr, ld);
+    RET(check_launch(ctx, "k_conj_transpose"));
+    RET(gram(ctx, np, ctx->J2, np, pr, Vn, np, r, ctx->small[4], pr));               // (J2_oldᴴ V_new)
+    k_conj_transpose<<<64, 256, 0, ctx->stream>>>(pr, r, ctx->small[4], pr, ctx->H2 + pr, ld);
+    RET(check_launch(ctx, "k_conj_transpose"));
+  }
+  ctx->pts[p] = rls_c64{z.x, z.y};
+  ctx->p = p + 1;
+  return RLS_OK;
+}
+
+int block_unitary_update(rls_ctx* ctx) {  // _block_unitary_update! (recySpace.jl:226-286)
+  const int p = ctx->p, r = ctx->r;
+  if (p <= 1) return RLS_OK;
+  const int pr = p * r;
+  const size_t smem = ((size_t)2 * r * r + 8 * (size_t)r * r + r + 2 * (size_t)r * pr) * sizeof(cplx);
+  k_blockrot_prep<<<1, 256, smem, ctx->stream>>>(p, r, ctx->L, ctx->H1, ctx->H2, ctx->pr_max, ctx->Ulist);
+  RET(check_launch(ctx, "k_blockrot_prep"));
+  RotArrays arr{};
+  arr.a[0] = ctx->V; arr.a[1] = ctx->J1; arr.a[2] = ctx->J2; arr.a[3] = ctx->J5;
+  dim3 grid((unsigned)((ctx->n_pad + 31) / 32), 4);
+  const size_t smem2 = ((size_t)32 * 2 * r + 4 * (size_t)r * r) * sizeof(cplx);
+  k_blockrot_apply<<<grid, 32 * 2 * r, smem2, ctx->stream>>>(ctx->n_pad, p, r, arr, ctx->n_pad, ctx->Ulist);
+  return check_launch(ctx, "k_blockrot_apply");
+}
+
+int update_recycled_space(rls_ctx* ctx, cplx z, const cplx* X, double tau, bool force_add, int p_min) {
+  const int r = ctx->r;
+  const int64_t np = ctx->n_pad;
+  if (ctx->p > 0) {
+    const int p = ctx->p, pr = p * r;
+    // rls_orth_robust!(V0, X[:,1]) with W: X_in = V c + x_⊥ ρ.  Dropping the first i
+    // blocks leaves residual sqrt(ρ² + Σ_{b<i} |c_b|²) (V orthonormal, x_⊥ ⊥ V), which
+    // is what the reference's per-suffix re-orthogonalisation computes (recySpace.jl:174-204).
+    cplx* x = ctx->tall_tmp;
+    RET(copy_cols(ctx, X, x, 1));
+    RET(orth_robust(ctx, np, ctx->V, np, pr, x, np, 1, ctx->owW, ctx->owR));
+    std::vector<cplx> c((size_t)pr + 1);
+    RET(d2h(ctx, c.data(), ctx->owW, (size_t)pr));
+    RET(d2h(ctx, c.data() + pr, ctx->owR, 1));
+    const double rho2 = c[pr].x * c[pr].x + c[pr].y * c[pr].y;
+    const double res0 = std::sqrt(rho2);
+    int l = 0;
+    if (!force_add) {
+      const int l_max = std::min(p - 1, p + 1 - p_min);
+      l = l_max;
+      double acc = rho2;
+      for (int i = 1; i <= l_max + 1; ++i) {
+        for (int q = (i - 1) * r; q < i * r; ++q) acc += c[q].x * c[q].x + c[q].y * c[q].y;
+        const double resl = std::sqrt(acc);
+        if (resl / res0 > tau) {
+          l = i - 1;
+          break;
+        }
+      }
+    }
+    if (l > 0) RET(shift_blocks(ctx, l));
+    if (l == 0 && p == ctx->p_max) RET(shift_blocks(ctx, 1));
+  }
+  RET(add_blocks(ctx, X, z));
+  return block_unitary_update(ctx);
+}
+
+// ---------------------------------------------------------------------------------
+// Recycle step (fastSvdRaylRitz_implicit!, fastRaylRitz.jl:99-219)
+// ---------------------------------------------------------------------------------
+
+struct RecycleResult {
+  int rr;
+  double sigma0;
+  double w0norm;
+};
+
+int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResult* out) {
+  const int r = ctx->r, pr = ctx->p * r;
+  const int64_t np = ctx->n_pad;
+  CK(cudaMemcpyAsync(ctx->zdev, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->taudev, &gap_tau, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t smem = heev_smem_bytes(pr);
+  k_heev_rr<<<1, HEEV_THREADS, smem, ctx->stream>>>(pr, r, ctx->H1, ctx->H2, ctx->pr_max, ctx->zdev, ctx->taudev,
+                                                    shift, ctx->heev, ctx->pr_max, ctx->Gheev, ctx->pr_max,
+                                                    (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev,
+                                                    ctx->derr);
+  RET(check_launch(ctx, "k_heev_rr"));
+  int rr = 0;
+  RET(d2h(ctx, &rr, ctx->rr_dev, 1));
+  if (rr < 1 || rr > pr) {
+    set_err(ctx, "recycle step: invalid Ritz dimension %d", rr);
+    return RLS_ERR_BREAKDOWN;
+  }
+
+  // CzX_ = (J5 − zV) G1   (J6 = V)
+  CombSrc src{};
+  src.a[0] = ctx->J5; src.coef[0] = cmk(1, 0);
+  src.a[1] = ctx->V;  src.coef[1] = cneg(z);
+  src.nsrc = 2;
+  cplx* Czx = (rr <= 64) ? ctx->CzX : ctx->tall_tmp;   // tall_tmp: n_pad × pr_max
+  RET(gemm_rows(ctx, np, src, np, pr, ctx->Gheev, ctx->pr_max, rr, Czx, np));
+  RET(tsqr_r(ctx, np, Czx, np, rr, ctx->small[0]));
+  {
+    const bool glob = rr > 80;   // A, V of the Jacobi SVD in global scratch beyond 80 columns
+    k_svd_rr<<<1, 256, svd_rr_smem_bytes(rr, r, glob), ctx->stream>>>(
+        rr, r, 0, 0, ctx->small[0], rr, ctx->sig_rec, ctx->lam_dev, ctx->small[1], rr,
+        glob ? ctx->svdA : nullptr, glob ? ctx->svdV : nullptr);
+    RET(check_launch(ctx, "k_svd_rr(recycle)"));
+  }
+  // G_total = G1 G2 (r_ < pr) or G2 (fastRaylRitz.jl:196-202)
+  if (rr < pr) {
+    RET(small_gemm(ctx, pr, r, rr, cmk(1, 0), ctx->Gheev, ctx->pr_max, 0, ctx->small[1], rr, 0, cmk(0, 0),
+                   ctx->Gtot, pr));
+  } else {
+    CK(cudaMemcpy2DAsync(ctx->Gtot, pr * sizeof(cplx), ctx->small[1], rr * sizeof(cplx), pr * sizeof(cplx), r,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  // X = V G_total; W = (J1 − zJ2 − z̄J3 + |z|²J4) G_total − X Σ²   (J3 = J5, J4 = V)
+  CombSrc wsrc{};
+  wsrc.a[0] = ctx->J1; wsrc.coef[0] = cmk(1, 0);
+  wsrc.a[1] = ctx->J2; wsrc.coef[1] = cneg(z);
+  wsrc.a[2] = ctx->J5; wsrc.coef[2] = cneg(cconj(z));
+  wsrc.a[3] = ctx->V;  wsrc.coef[3] = cmk(z.x * z.x + z.y * z.y, 0);
+  wsrc.nsrc = 4;
+  cplx* X = ctx->S;
+  cplx* W = ctx->S + np * r;
+  int nparts = 0;
+  RET(gemm_rows(ctx, np, wsrc, np, pr, ctx->Gtot, pr, r, W, np, cmk(1, 0), cmk(0, 0), 3, X, np, ctx->sig_rec,
+                true, &nparts));
+  k_sum<<<1, 256, 0, ctx->stream>>>(ctx->colpart, nparts, ctx->dscal);
+  RET(check_launch(ctx, "k_sum"));
+  double w2 = 0.0, s0 = 0.0;
+  RET(d2h(ctx, &w2, ctx->dscal, 1));
+  RET(d2h(ctx, &s0, ctx->sig_rec, 1));
+  out->rr = rr;
+  out->sigma0 = s0;
+  out->w0norm = std::sqrt(w2);
+  return RLS_OK;
+}
+
+void emit_log(rls_ctx* ctx, const char* fmt, ...) {
+  if (!ctx->log_fn) return;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  ctx->log_fn(buf, ctx->log_user);
+}
+
+uint64_t now_ns() {
+  return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// Deterministic uniform [0,1) complex fill for a missing X0 (the reference uses rand!).
+__global__ void k_fill_rand(int64_t n, int64_t ld, int k, cplx* X, uint64_t seed) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (row >= ld) return;
+  if (row >= n) { X[(int64_t)c * ld + row] = czero(); return; }
+  uint64_t h = seed ^ ((uint64_t)(row + 1) * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)(c + 1) * 0xC2B2AE3D27D4EB4Full);
+  h ^= h >> 33; h *= 0xff51afd7ed558ccdull; h ^= h >> 33; h *= 0xc4ceb9fe1a85ec53ull; h ^= h >> 33;
+  const double re = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+  uint64_t g = h * 0x9E3779B97F4A7C15ull; g ^= g >> 29;
+  const double im = (double)(g >> 11) * (1.0 / 9007199254740992.0);
+  X[(int64_t)c * ld + row] = cmk(re, im);
+}
+
+int upload_x0(rls_ctx* ctx, const rls_c64* X0, int r) {
+  const int64_t np = ctx->n_pad;
+  if (X0) {
+    CK(cudaMemsetAsync(ctx->S, 0, sizeof(cplx) * np * r, ctx->stream));
+    CK(cudaMemcpy2DAsync(ctx->S, np * sizeof(cplx), X0, ctx->n * sizeof(cplx), ctx->n * sizeof(cplx), r,
+                         cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    dim3 grid((unsigned)((np + 255) / 256), r);
+    k_fill_rand<<<grid, 256, 0, ctx->stream>>>(ctx->n, np, r, ctx->S, 20260318ull);
+    RET(check_launch(ctx, "k_fill_rand"));
+  }
+  return RLS_OK;
+}
+
+template <class K>
+int allow_big_smem(rls_ctx* ctx, K kernel, int optin) {
+  cudaFuncAttributes fa{};
+  CK(cudaFuncGetAttributes(&fa, kernel));
+  const int dyn = optin - (int)fa.sharedSizeBytes;
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  return RLS_OK;
+}
+
+int set_kernel_attrs(rls_ctx* ctx) {
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  RET(allow_big_smem(ctx, k_trsm_dataflow, optin));
+  RET(allow_big_smem(ctx, k_trmm_partial, optin));
+  RET(allow_big_smem(ctx, k_diag_inv, optin));
+  RET(allow_big_smem(ctx, k_tsqr_leaf, optin));
+  RET(allow_big_smem(ctx, k_heev_rr, optin));
+  RET(allow_big_smem(ctx, k_svd_rr, optin));
+  RET(allow_big_smem(ctx, k_blockrot_prep, optin));
+  RET(allow_big_smem(ctx, k_chol_inv, optin));
+  RET(allow_big_smem(ctx, k_trtri, optin));
+  return RLS_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+
+extern "C" const char* rls_status_string(int s) {
+  switch (s) {
+    case RLS_OK: return "ok";
+    case RLS_ERR_ARG: return "invalid argument";
+    case RLS_ERR_DIM: return "dimension mismatch";
+    case RLS_ERR_CUDA: return "CUDA error";
+    case RLS_ERR_NOMEM: return "device out of memory";
+    case RLS_ERR_TIMEOUT: return "bounded device wait expired";
+    case RLS_ERR_BREAKDOWN: return "numerical breakdown";
+    case RLS_ERR_STATE: return "invalid call order";
+    default: return "unknown status";
+  }
+}
+
+static thread_local std::string g_create_err;
+
+extern "C" int rls_ctx_create(rls_ctx** out, int device) {
+  if (!out) return RLS_ERR_ARG;
+  *out = nullptr;
+  rls_ctx* ctx = new rls_ctx();
+  ctx->device = device;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    g_create_err = "no CUDA device with index " + std::to_string(device);
+    delete ctx;
+    return RLS_ERR_CUDA;
+  }
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return RLS_ERR_CUDA;
+  }
+  int st = set_kernel_attrs(ctx);
+  if (st == RLS_OK) st = dalloc_t(ctx, &ctx->derr, 4);
+  if (st == RLS_OK) st = dalloc_t(ctx, &ctx->dscal, 256);
+  if (st != RLS_OK) {
+    g_create_err = ctx->err;
+    rls_ctx_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return RLS_OK;
+}
+
+extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->owned) cudaFree(b.p);
+  ctx->owned.clear();
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" const char* rls_last_error(const rls_ctx* ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_create_err.empty() ? "null context" : g_create_err.c_str();
+}
+
+extern "C" int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verbose) {
+  if (!ctx) return RLS_ERR_ARG;
+  ctx->log_fn = fn;
+  ctx->log_user = user;
+  ctx->verbose = verbose;
+  return RLS_OK;
+}
+
+// Tiles of T: host-side packing then one copy.
+extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!T || n < 1 || ldt < n) {
+    set_err(ctx, "rls_set_schur: invalid arguments (n=%lld, ldt=%lld)", (long long)n, (long long)ldt);
+    return RLS_ERR_ARG;
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // drop an old operator and space
+  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
+                  (void*)ctx->colpart, (void*)ctx->trmm_uO[0], (void*)ctx->trmm_us[0], (void*)ctx->trmm_Ofirst[0],
+                  (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
+                  (void*)ctx->trmm_Ofirst[1], (void*)ctx->trmm_Ocount[1]})
+    dfree(ctx, q);
+  release_space(ctx);
+  ctx->n = n;
+  ctx->nb = (int)((n + TILE - 1) / TILE);
+  ctx->n_pad = (int64_t)ctx->nb * TILE;
+  const int nb = ctx->nb;
+  const size_t ntiles = (size_t)nb * (nb + 1) / 2;
+  std::vector<cplx> h(ntiles * TILE * TILE);
+  for (int J = 0; J < nb; ++J)
+    for (int I = 0; I <= J; ++I) {
+      cplx* tp = h.data() + tile_index(I, J) * TILE * TILE;
+      for (int cc = 0; cc < TILE; ++cc) {
+        const int64_t gc = (int64_t)J * TILE + cc;
+        for (int rr = 0; rr < TILE; ++rr) {
+          const int64_t gr = (int64_t)I * TILE + rr;
+          cplx v = czero();
+          if (gr < n && gc < n && gr <= gc) v = cmk(T[gc * ldt + gr].re, T[gc * ldt + gr].im);
+          tp[cc * TILE + rr] = v;
+        }
+      }
+    }
+  RET(dalloc_t(ctx, &ctx->T, h.size()));
+  CK(cudaMemcpyAsync(ctx->T, h.data(), h.size() * sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
+  RET(dalloc_t(ctx, &ctx->flags, (size_t)nb));
+  RET(dalloc_t(ctx, &ctx->ticket, 1));
+  ctx->z_dinv = cmk(NAN, NAN);
+  ctx->epoch = 0;
+  // TRMM work units
+  size_t maxunits = 0;
+  for (int adj = 0; adj < 2; ++adj) {
+    std::vector<int> uO, us, Of(nb), Oc(nb);
+    for (int O = 0; O < nb; ++O) {
+      const int nsrc = adj ? (O + 1) : (nb - O);
+      Of[O] = (int)uO.size();
+      for (int s0 = 0; s0 < nsrc; s0 += TRMM_UT) { uO.push_back(O); us.push_back(s0); }
+      Oc[O] = (int)uO.size() - Of[O];
+    }
+    ctx->trmm_units[adj] = (int)uO.size();
+    maxunits = std::max(maxunits, uO.size());
+    RET(dalloc_t(ctx, &ctx->trmm_uO[adj], uO.size()));
+    RET(dalloc_t(ctx, &ctx->trmm_us[adj], us.size()));
+    RET(dalloc_t(ctx, &ctx->trmm_Ofirst[adj], (size_t)nb));
+    RET(dalloc_t(ctx, &ctx->trmm_Ocount[adj], (size_t)nb));
+    CK(cudaMemcpyAsync(ctx->trmm_uO[adj], uO.data(), uO.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->trmm_us[adj], us.data(), us.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->trmm_Ofirst[adj], Of.data(), nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->trmm_Ocount[adj], Oc.data(), nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  RET(dalloc_t(ctx, &ctx->trmm_part, maxunits * 16 * TILE));
+  RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
+  CK(cudaStreamSynchronize(ctx->stream));  // h must outlive the async copy
+  return RLS_OK;
+}
+
+extern "C" int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0, const rls_lobpcg_control* c,
+                                     rls_c64* X_out, double* sigma_r, double* sigma, int64_t* it) {
+  if (!ctx || !c) return RLS_ERR_ARG;
+  if (!ctx->T) {
+    set_err(ctx, "no operator uploaded (call rls_set_schur first)");
+    return RLS_ERR_STATE;
+  }
+  if (c->m != ctx->n || c->n != ctx->n) {
+    set_err(ctx, "LobpcgSvdControl m, n (%lld, %lld) do not match the operator (%lld)", (long long)c->m,
+            (long long)c->n, (long long)ctx->n);
+    return RLS_ERR_DIM;
+  }
+  if (c->r < 1 || c->r > 8) {
+    set_err(ctx, "block size r=%lld outside 1..8", (long long)c->r);
+    return RLS_ERR_ARG;
+  }
+  if (!(1 <= c->conv_first && c->conv_first <= c->conv_last && c->conv_last <= c->r)) {
+    set_err(ctx, "conv_range must satisfy 1 <= first <= last <= r");
+    return RLS_ERR_ARG;
+  }
+  if (c->side != 'L') {
+    set_err(ctx, "only side 'L' (the psTriRecy configuration) is supported on the triangular operator");
+    return RLS_ERR_ARG;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const int r = (int)c->r;
+  if (ctx->r != r || !ctx->V) RET(setup_space(ctx, r, std::max(ctx->p_max, 1)));
+  RET(upload_x0(ctx, X0, r));
+  LobpcgResult res{};
+  RET(lobpcg_invtri(ctx, cmk(z.re, z.im), r, c->maxit, c->tol, true, &res));
+  if (X_out)
+    CK(cudaMemcpy2DAsync(X_out, ctx->n * sizeof(cplx), ctx->S, ctx->n_pad * sizeof(cplx), ctx->n * sizeof(cplx), r,
+                         cudaMemcpyDeviceToHost, ctx->stream));
+  if (sigma_r) CK(cudaMemcpyAsync(sigma_r, ctx->sig, r * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RET(sync_and_check(ctx));
+  if (sigma) *sigma = res.sigma;
+  if (it) *it = res.it;
+  return RLS_OK;
+}
+
+extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                                   const rls_pstrirecy_control* ctl, const rls_c64* X0, double* sigma_min,
+                                   rls_pstrirecy_stats* st) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!Z || !g || !ctl || !sigma_min || nZ < 0) {
+    set_err(ctx, "rls_pstrirecy_schur: null argument");
+    return RLS_ERR_ARG;
+  }
+  if (!ctx->T) {
+    set_err(ctx, "no operator uploaded (call rls_set_schur first)");
+    return RLS_ERR_STATE;
+  }
+  if (ctl->r < 1 || ctl->r > 8 || ctl->p < 1 || ctl->p_min < 0 || ctl->p_min > ctl->p) {
+    set_err(ctx, "invalid control: r=%lld p=%lld p_min=%lld (r in 1..8, 0 <= p_min <= p)", (long long)ctl->r,
+            (long long)ctl->p, (long long)ctl->p_min);
+    return RLS_ERR_ARG;
+  }
+  if (ctl->lobpcg_side != 'L') {
+    set_err(ctx, "lobpcg_side must be 'L' on the triangular operator");
+    return RLS_ERR_ARG;
+  }
+  if (!ctl->implict_recycle || ctl->implict_update) {
+    set_err(ctx, "only implict_recycle=true, implict_update=false is implemented");
+    return RLS_ERR_ARG;
+  }
+  if (g->n_x < 2 || g->n_y < 2 || g->k < 1) return RLS_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const int r = (int)ctl->r;
+  RET(setup_space(ctx, r, (int)ctl->p));
+  RET(upload_x0(ctx, X0, r));
+  // recycle_fail_dist_thresh (recySpace.jl:22-38)
+  double thresh = ctl->recycle_fail_dist_thresh;
+  if (!std::isfinite(thresh)) {
+    const double dx = std::fabs(g->x_ed - g->x_st) / (double)(g->n_x - 1);
+    const double dy = std::fabs(g->y_ed - g->y_st) / (double)(g->n_y - 1);
+    thresh = 1.01 * std::max(dx, dy);
+  } else if (thresh < 0) {
+    set_err(ctx, "recycle_fail_dist_thresh must be nonnegative, got %g", thresh);
+    return RLS_ERR_ARG;
+  }
+  const double lob_tol = ctl->lobpcg_tol_scale * ctl->tol;
+  int remaining = 0;
+  bool have_failed = false;
+  rls_c64 last_failed{0, 0};
+  rls_pstrirecy_stats dummy{};
+  if (!st) st = &dummy;
+  st->preprocess_time_ns = st->recycle_time_ns = st->qr_time_ns = st->refine_time_ns = st->update_time_ns = 0;
+  st->mv_stats_available = 1;
+  st->n_it = 0;
+  st->n_pts = 0;
+  for (int64_t i = 0; i < nZ; ++i) {
+    const cplx z = cmk(Z[i].re, Z[i].im);
+    if (st->p_count) st->p_count[i] = ctx->p;
+    if (st->r_recy) st->r_recy[i] = 0;
+    if (st->refine_it) st->refine_it[i] = 0;
+    int64_t m_apps = 0, r_apps = 0;
+    int r_svdrr = 0;
+    if (ctx->p > 0) {
+      const uint64_t t0 = now_ns();
+      const double gtau = remaining > 0 ? ctl->gap_tau * ctl->gap_tau_scale : ctl->gap_tau;
+      RecycleResult rres{};
+      RET(recycle_step(ctx, z, ctl->shift, gtau, &rres));
+      remaining = remaining > 0 ? remaining - 1 : 0;
+      st->recycle_time_ns += now_ns() - t0;
+      r_svdrr = rres.rr;
+      if (st->r_recy) st->r_recy[i] = r_svdrr;
+      // _residual_norm_ok (psTriRecy.jl:237-245)
+      const bool ok = rres.w0norm < ctl->normC * std::max(rres.sigma0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps);
+      if (ok) {
+        sigma_min[i] = rres.sigma0;
+        if (st->M_vec_apps) st->M_vec_apps[i] = 0;
+        if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = 0;
+        if (st->R_vec_apps) st->R_vec_apps[i] = 0;
+        if (ctx->verbose >= 1)
+          emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
+                   (long long)(i + 1), (long long)nZ, z.x, z.y, "recycled", ctx->p, r_svdrr, sigma_min[i]);
+        continue;
+      }
+    }
+    const uint64_t t1 = now_ns();
+    LobpcgResult lres{};
+    RET(lobpcg_invtri(ctx, z, r, 2000, lob_tol, true, &lres));
+    double s0 = 0.0;
+    RET(d2h(ctx, &s0, ctx->sig, 1));
+    sigma_min[i] = s0;  // keep.σ[1] (psTriRecy.jl:809)
+    const int64_t it = lres.it;
+    if (st->refine_it) st->refine_it[i] = it;
+    if (it > 0) r_apps += 2 * r + it * r + (it - 1) * r;
+    st->refine_time_ns += now_ns() - t1;
+    st->n_it += it;
+    if (st->pts) st->pts[st->n_pts] = Z[i];
+    st->n_pts += 1;
+    if (i < nZ - 1 && it > 0) {
+      const uint64_t t2 = now_ns();
+      const bool force_add = have_failed && std::hypot(z.x - last_failed.re, z.y - last_failed.im) <= thresh;
+      RET(update_recycled_space(ctx, z, ctx->S, ctl->recy_tau, force_add, (int)ctl->p_min));
+      remaining = force_add ? (int)std::max<int64_t>(g->k, 0) : 0;
+      m_apps += 3 * r;
+      RET(sync_and_check(ctx));
+      st->update_time_ns += now_ns() - t2;
+    }
+    have_failed = true;
+    last_failed = Z[i];
+    if (st->M_vec_apps) st->M_vec_apps[i] = m_apps;
+    if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = m_apps;
+    if (st->R_vec_apps) st->R_vec_apps[i] = r_apps;
+    if (ctx->verbose >= 1) {
+      char state[32];
+      snprintf(state, sizeof state, "refine(%lld)", (long long)it);
+      emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
+               (long long)(i + 1), (long long)nZ, z.x, z.y, state, ctx->p, r_svdrr, sigma_min[i]);
+    }
+  }
+  return sync_and_check(ctx);
+}
+
+#include "../../include/rls_b200_testing.h"
+#include "testing.cuh"

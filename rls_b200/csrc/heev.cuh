@@ -1,0 +1,372 @@
+// Projected Hermitian eigenproblem of the recycle step (find_rr_dim!,
+// src/core/fastRaylRitz.jl:54-96) on the device, FP64, one CTA per grid point.
+//
+//   Hz = H1 − z·H2 − z̄·H2ᴴ + (|z|² + shift)·I          (affine_conbine!, :6-28; H3 = I)
+//   λ_max, then the smallest eigenvalues in steps of 2r until a gap > λ_max/τ·eps,
+//   r_ = max(first gap index, r) or pr when none; eigenvectors of the r_ smallest.
+//
+// Method (published algorithms, written for this kernel):
+//   1. Householder tridiagonalisation Hz = Q T Qᴴ (Golub & Van Loan §8.3.1), reflectors
+//      in the convention of LAPACK's zlarfg, T real symmetric tridiagonal;
+//   2. eigenvalues of T by Sturm-count multisection: a warp evaluates 32 Sturm
+//      counts per round (Barth, Martin & Wilkinson 1967 bisection, 32-way);
+//   3. eigenvectors of T by inverse iteration with a partially pivoted tridiagonal
+//      LU (Wilkinson), one warp per vector, then classical Gram–Schmidt with
+//      re-orthogonalisation over the vectors (which keeps a cluster's invariant subspace);
+//   4. back-transformation by the stored reflectors: G = Q S.
+// Like zheevr with uplo 'U', only the upper triangle of Hz is used.
+#pragma once
+#include "common.cuh"
+#include "small.cuh"
+
+#define HEEV_THREADS 512
+#define HEEV_SMEM_PR 100   // full Hz kept in shared memory up to this order
+
+struct HeevWork {
+  cplx* A;        // per problem pr_max*pr_max (global path)
+  double* lu;     // per problem 16 warps × 6 × pr_max doubles
+};
+
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += (q < 0.0);
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += (q < 0.0);
+  }
+  return cnt;
+}
+
+// Eigenvalue with 0-based index `idx` (ascending) by 32-way multisection, one warp.
+__device__ double warp_eig_index(const double* d, const double* e2, int n, int idx, double gl, double gu,
+                                 double pivmin, double atol) {
+  const int lane = threadIdx.x & 31;
+  double lo = gl, hi = gu;
+  for (int round = 0; round < 14 && (hi - lo) > atol; ++round) {
+    const double h = (hi - lo) / 33.0;
+    const double x = lo + h * (lane + 1);
+    const int c = sturm_count(d, e2, n, x, pivmin);     // # eigenvalues < x
+    // largest lane whose count <= idx gives a new lower bound; smallest with count > idx an upper bound
+    const unsigned le = __ballot_sync(0xffffffffu, c <= idx);
+    const int nle = __popc(le);                          // counts are monotone in lane
+    const double nlo = (nle > 0) ? lo + h * nle : lo;
+    const double nhi = (nle < 32) ? lo + h * (nle + 1) : hi;
+    lo = nlo; hi = nhi;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Partially pivoted LU of (T − λI) and solves, on lane 0 of a warp.
+// Storage (6 arrays of n): u0 (diag), u1, u2 (superdiagonals), l (multipliers), piv.
+__device__ void tri_lu(const double* d, const double* e, int n, double lam, double* u0, double* u1, double* u2,
+                       double* l, double* piv, double tiny) {
+  double a = d[0] - lam;
+  double b = (n > 1) ? e[0] : 0.0;
+  for (int i = 0; i < n - 1; ++i) {
+    const double c = e[i];                      // subdiagonal entry (i+1, i)
+    const double an = d[i + 1] - lam;           // next diagonal
+    const double bn = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+    if (fabs(a) >= fabs(c)) {
+      double aa = (a == 0.0) ? tiny : a;
+      const double m = c / aa;
+      piv[i] = 0.0; l[i] = m;
+      u0[i] = aa; u1[i] = b; u2[i] = 0.0;
+      a = an - m * b;
+      b = bn;
+    } else {
+      const double m = a / c;
+      piv[i] = 1.0; l[i] = m;
+      u0[i] = c; u1[i] = an; u2[i] = bn;
+      a = b - m * an;
+      b = -m * bn;
+    }
+  }
+  u0[n - 1] = (a == 0.0) ? tiny : a;
+}
+
+__device__ void tri_solve(int n, const double* u0, const double* u1, const double* u2, const double* l,
+                          const double* piv, double* x) {
+  for (int i = 0; i < n - 1; ++i) {             // apply P and L⁻¹
+    if (piv[i] != 0.0) { const double t = x[i]; x[i] = x[i + 1]; x[i + 1] = t; }
+    x[i + 1] -= l[i] * x[i];
+  }
+  x[n - 1] /= u0[n - 1];                         // U⁻¹ (three bands)
+  if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) / u0[n - 2];
+  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) / u0[i];
+}
+
+__global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const cplx* __restrict__ H1,
+                                                          const cplx* __restrict__ H2, int ldh,
+                                                          const cplx* __restrict__ zs,
+                                                          const double* __restrict__ taus, double shift,
+                                                          HeevWork work, int prmax, cplx* Gout, int ldg,
+                                                          int64_t gstride, int* rr_out, double* lam_out,
+                                                          int* err) {
+  extern __shared__ double dsm[];
+  const int b = blockIdx.x;
+  const int n = pr;
+  const bool in_smem = (n <= HEEV_SMEM_PR);
+  // shared layout: [A (n*n cplx, optional)] v w (n cplx) d e e2 lam (n doubles) tau (n cplx)
+  cplx* A = in_smem ? reinterpret_cast<cplx*>(dsm) : work.A + (int64_t)b * prmax * prmax;
+  cplx* v = reinterpret_cast<cplx*>(dsm) + (in_smem ? n * n : 0);
+  cplx* w = v + n;
+  cplx* tau = w + n;
+  double* d = reinterpret_cast<double*>(tau + n);
+  double* e = d + n;
+  double* e2 = e + n;
+  double* lam = e2 + n;
+  __shared__ double red[32];
+  __shared__ cplx s_tau, s_scal, s_alpha2;
+  __shared__ int s_rr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lda = n;
+  const cplx z = zs[b];
+  const double zz = z.x * z.x + z.y * z.y + shift;
+  cplx* G = Gout + (int64_t)b * gstride;
+
+  // 1. Hz from the upper triangle, mirrored.
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+    const int i = q % n, j = q / n;
+    const int ii = min(i, j), jj = max(i, j);
+    // affine_conbine! element (ii, jj): H1 − z H2 − z̄ conj(H2[jj, ii]) + zz·δ
+    cplx h = H1[(int64_t)jj * ldh + ii];
+    h = cfms(z, H2[(int64_t)jj * ldh + ii], h);
+    h = cfms(cconj(z), cconj(H2[(int64_t)ii * ldh + jj]), h);
+    if (ii == jj) h = cmk(h.x + zz, 0.0);
+    A[j * lda + i] = (i <= j) ? h : cconj(h);
+  }
+  __syncthreads();
+
+  // 2. Householder tridiagonalisation (lower form): for column k reduce A[k+1:, k].
+  for (int k = 0; k < n - 1; ++k) {
+    const int m0 = k + 1;
+    double x2 = 0.0;
+    for (int i = m0 + 1 + threadIdx.x; i < n; i += blockDim.x) x2 += cabs2(A[k * lda + i]);
+    x2 = block_sum(x2, red);
+    if (threadIdx.x == 0) {
+      double beta; cplx t, sc;
+      householder_coeffs(A[k * lda + m0], x2, &beta, &t, &sc);
+      s_tau = t; s_scal = sc;
+      tau[k] = t;
+      e[k] = beta;
+      d[k] = A[k * lda + k].x;
+    }
+    __syncthreads();
+    const cplx t = s_tau, sc = s_scal;
+    // v = [1; x*scal], stored in A[m0:, k] (A[m0, k] keeps 1 during the update)
+    for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) {
+      const cplx vi = (i == m0) ? cmk(1.0, 0.0) : cmul(A[k * lda + i], sc);
+      v[i] = vi;
+      if (i > m0) A[k * lda + i] = vi;
+    }
+    __syncthreads();
+    if (t.x != 0.0 || t.y != 0.0) {
+      // y = tau * A[m0:, m0:] v  — row i via column i (Hermitian): y_i = Σ_j conj(A[j,i]) v_j
+      for (int i = m0 + warp; i < n; i += nw) {
+        cplx s = czero();
+        for (int j = m0 + lane; j < n; j += 32) s = cfmac(A[i * lda + j], v[j], s);
+        s = warp_sum(s);
+        if (lane == 0) w[i] = cmul(t, s);
+      }
+      __syncthreads();
+      // alpha2 = -1/2 tau (yᴴ v)
+      cplx yv = czero();
+      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) yv = cfmac(w[i], v[i], yv);
+      {
+        __shared__ cplx cred[32];
+        yv = block_sum(yv, cred);
+      }
+      if (threadIdx.x == 0) s_alpha2 = cscale(cmul(t, yv), -0.5);
+      __syncthreads();
+      const cplx a2 = s_alpha2;
+      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) w[i] = cfma(a2, v[i], w[i]);
+      __syncthreads();
+      // A -= v wᴴ + w vᴴ on the trailing block
+      const int mm = n - m0;
+      for (int q = threadIdx.x; q < mm * mm; q += blockDim.x) {
+        const int i = m0 + q % mm, j = m0 + q / mm;
+        cplx a = A[j * lda + i];
+        a = csub(a, cmul(v[i], cconj(w[j])));
+        a = csub(a, cmul(w[i], cconj(v[j])));
+        A[j * lda + i] = a;
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) d[n - 1] = A[(n - 1) * lda + (n - 1)].x;
+  for (int i = threadIdx.x; i < n - 1; i += blockDim.x) e2[i] = e[i] * e[i];
+  __syncthreads();
+
+  // Gershgorin interval and pivot floor.
+  __shared__ double s_gl, s_gu, s_piv;
+  if (threadIdx.x == 0) {
+    double gl = 1e300, gu = -1e300, emax = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double off = ((i > 0) ? fabs(e[i - 1]) : 0.0) + ((i < n - 1) ? fabs(e[i]) : 0.0);
+      gl = fmin(gl, d[i] - off);
+      gu = fmax(gu, d[i] + off);
+      if (i < n - 1) emax = fmax(emax, e2[i]);
+    }
+    const double tnorm = fmax(fabs(gl), fabs(gu));
+    gl -= 2.0 * tnorm * 2.220446049250313e-16 * n + 1e-300;
+    gu += 2.0 * tnorm * 2.220446049250313e-16 * n + 1e-300;
+    s_gl = gl; s_gu = gu;
+    s_piv = fmax(2.2250738585072014e-308, 2.2250738585072014e-308 * emax) * 4.0;
+  }
+  __syncthreads();
+  const double gl = s_gl, gu = s_gu, pivmin = s_piv;
+  const double atol = 1e-14 * fmax(fabs(gl), fabs(gu));
+
+  // 3. λ_max and the smallest eigenvalues with the gap rule of find_rr_dim!.
+  if (warp == 0) {
+    const double lmax = warp_eig_index(d, e2, n, n - 1, gl, gu, pivmin, atol);
+    if (lane == 0) lam[n - 1] = lmax;
+  }
+  __syncthreads();
+  const double gap = lam[n - 1] / taus[b] * 2.220446049250313e-16;
+  const int n_init = min(2 * r, n);
+  int n_last = n_init;                      // largest n of the sequence 2r, 4r, ... <= n
+  while (n_last + 2 * r <= n) n_last += 2 * r;
+  int computed = 0;                         // eigenvalues 0..computed-1 known
+  int rr = 0;
+  int ncheck = n_init;
+  while (true) {
+    // make sure λ_0 .. λ_{ncheck-1} are known (passes of nw eigenvalues)
+    while (computed < ncheck) {
+      const int idx = computed + warp;
+      if (idx < ncheck && idx < n - 1) {
+        const double li = warp_eig_index(d, e2, n, idx, gl, gu, pivmin, atol);
+        if (lane == 0) lam[idx] = li;
+      }
+      computed = min(ncheck, computed + nw);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      int g = 0;
+      for (int i = 0; i + 1 < ncheck; ++i)
+        if (fabs(lam[i] - lam[i + 1]) > gap) { g = i + 1; break; }
+      s_rr = g;
+    }
+    __syncthreads();
+    rr = s_rr;
+    if (rr > 0 || ncheck >= n_last) break;
+    ncheck += 2 * r;
+  }
+  rr = (rr > 0) ? max(rr, r) : n;
+  // λ for all indices < rr (needed for the eigenvectors)
+  while (computed < rr) {
+    const int idx = computed + warp;
+    if (idx < rr && idx < n - 1) {
+      const double li = warp_eig_index(d, e2, n, idx, gl, gu, pivmin, atol);
+      if (lane == 0) lam[idx] = li;
+    }
+    computed = min(rr, computed + nw);
+    __syncthreads();
+  }
+
+  // 4. Inverse iteration, one warp per eigenvector; s_j (real) goes to G[:, j].
+  {
+    const double tnorm = fmax(fabs(gl), fabs(gu));
+    const double tiny = 2.220446049250313e-16 * tnorm + 1e-300;
+    for (int j = warp; j < rr; j += nw) {
+      double* lu = work.lu + ((int64_t)b * 16 + warp) * 6 * prmax;
+      double *u0 = lu, *u1 = lu + prmax, *u2 = lu + 2 * prmax, *l = lu + 3 * prmax, *pv = lu + 4 * prmax,
+             *x = lu + 5 * prmax;
+      // shift perturbed slightly away from the computed eigenvalue so the factor is nonsingular
+      const double lamj = lam[j] + tiny * ((j & 1) ? 1.0 : -1.0);
+      if (lane == 0) tri_lu(d, e, n, lamj, u0, u1, u2, l, pv, tiny);
+      // deterministic start vector
+      for (int i = lane; i < n; i += 32) {
+        uint32_t h = (uint32_t)(i * 2654435761u) ^ (uint32_t)((j + 1) * 2246822519u);
+        h ^= h >> 15; h *= 2654435761u; h ^= h >> 13;
+        x[i] = 0.5 + (double)(h & 0xffff) / 65536.0;
+      }
+      __syncwarp();
+      for (int it = 0; it < 3; ++it) {
+        if (lane == 0) tri_solve(n, u0, u1, u2, l, pv, x);
+        __syncwarp();
+        double s = 0.0;
+        for (int i = lane; i < n; i += 32) s += x[i] * x[i];
+        s = warp_sum(s);
+        const double inv = (s > 0.0 && isfinite(s)) ? 1.0 / sqrt(s) : 0.0;
+        for (int i = lane; i < n; i += 32) x[i] *= inv;
+        __syncwarp();
+      }
+      for (int i = lane; i < n; i += 32) G[(int64_t)j * ldg + i] = cmk(x[i], 0.0);
+    }
+  }
+  __syncthreads();
+  // Block-wide classical Gram–Schmidt with one re-orthogonalisation (CGS2) over the rr
+  // real vectors, in index order.  v (no longer needed) holds the coefficients.
+  {
+    double* coef = reinterpret_cast<double*>(v);
+    __shared__ double s_nrm;
+    for (int j = 0; j < rr; ++j) {
+      double* gj = reinterpret_cast<double*>(G + (int64_t)j * ldg);   // stride-2 real parts
+      for (int pass = 0; pass < 2 && j > 0; ++pass) {
+        for (int q = warp; q < j; q += nw) {
+          const double* gq = reinterpret_cast<const double*>(G + (int64_t)q * ldg);
+          double s = 0.0;
+          for (int i = lane; i < n; i += 32) s += gq[2 * i] * gj[2 * i];
+          s = warp_sum(s);
+          if (lane == 0) coef[q] = s;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          double acc = 0.0;
+          for (int q = 0; q < j; ++q) acc += coef[q] * reinterpret_cast<const double*>(G + (int64_t)q * ldg)[2 * i];
+          gj[2 * i] -= acc;
+        }
+        __syncthreads();
+      }
+      double s = 0.0;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) s += gj[2 * i] * gj[2 * i];
+      s = block_sum(s, red);
+      if (threadIdx.x == 0) s_nrm = (s > 0.0) ? 1.0 / sqrt(s) : 0.0;
+      __syncthreads();
+      const double inv = s_nrm;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) gj[2 * i] *= inv;
+      __syncthreads();
+    }
+  }
+  // 5. Back-transformation G = H_0 H_1 ... H_{n-2} S: apply H_{n-2} first.
+  for (int k = n - 2; k >= 0; --k) {
+    const int m0 = k + 1;
+    const cplx t = tau[k];
+    if (t.x == 0.0 && t.y == 0.0) continue;
+    for (int j = warp; j < rr; j += nw) {
+      cplx s = czero();
+      for (int i = m0 + lane; i < n; i += 32) {
+        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
+        s = cfmac(vi, G[(int64_t)j * ldg + i], s);
+      }
+      s = warp_sum(s);
+      const cplx f = cmul(t, s);
+      for (int i = m0 + lane; i < n; i += 32) {
+        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
+        G[(int64_t)j * ldg + i] = cfms(vi, f, G[(int64_t)j * ldg + i]);
+      }
+    }
+    // no barrier needed: each warp owns its columns and A is read-only here
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    rr_out[b] = rr;
+    bool bad = !isfinite(lam[n - 1]);
+    for (int i = 0; i < rr && i < n - 1; ++i) bad |= !isfinite(lam[i]);
+    if (bad) atomicOr(err, DEVERR_NONFINITE);
+  }
+  if (lam_out) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      lam_out[(int64_t)b * prmax + i] = (i < computed || i == n - 1) ? lam[i] : 0.0;
+  }
+}
+
+inline size_t heev_smem_bytes(int pr) {
+  size_t s = (size_t)3 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
+  if (pr <= HEEV_SMEM_PR) s += (size_t)pr * pr * sizeof(cplx);
+  return s;
+}

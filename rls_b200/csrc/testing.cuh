@@ -1,0 +1,203 @@
+// Kernel-level entry points for parity tests (declared in include/rls_b200_testing.h).
+// Each copies host inputs to the device, runs one device routine of the engine on the
+// context's stream and copies the result back.  Included at the end of engine.cu so
+// the kernels stay in one translation unit.
+#pragma once
+
+namespace {
+
+struct DevTmp {
+  rls_ctx* ctx;
+  std::vector<void*> ptrs;
+  explicit DevTmp(rls_ctx* c) : ctx(c) {}
+  ~DevTmp() {
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), ctx->stream);
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+};
+
+int need_space(rls_ctx* ctx) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->T || !ctx->V) {
+    set_err(ctx, "test entry point needs rls_set_schur and rls_test_setup first");
+    return RLS_ERR_STATE;
+  }
+  return RLS_OK;
+}
+
+}  // namespace
+
+extern "C" int rls_test_setup(rls_ctx* ctx, int r, int p_max) {
+  if (!ctx || !ctx->T) return RLS_ERR_STATE;
+  if (r < 1 || r > 8 || p_max < 1) return RLS_ERR_ARG;
+  return setup_space(ctx, r, p_max);
+}
+
+extern "C" int rls_test_trsm(rls_ctx* ctx, rls_c64 z, int adj, int k, const rls_c64* B, rls_c64* X) {
+  RET(need_space(ctx));
+  if (k < 1 || k > 64 || !B || !X) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  cplx* d = t.alloc<cplx>((size_t)np * k);
+  if (!d) return RLS_ERR_NOMEM;
+  CK(cudaMemcpy2DAsync(d, np * sizeof(cplx), B, n * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  RET(trsm(ctx, cmk(z.re, z.im), adj, d, d, np, k));
+  CK(cudaMemcpy2DAsync(X, n * sizeof(cplx), d, np * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  return sync_and_check(ctx);
+}
+
+extern "C" int rls_test_trmm(rls_ctx* ctx, int adj, int k, const rls_c64* X, rls_c64* Y) {
+  RET(need_space(ctx));
+  if (k < 1 || k > 16 || !X || !Y) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  cplx* dx = t.alloc<cplx>((size_t)np * k);
+  cplx* dy = t.alloc<cplx>((size_t)np * k);
+  if (!dx || !dy) return RLS_ERR_NOMEM;
+  CK(cudaMemcpy2DAsync(dx, np * sizeof(cplx), X, n * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  RET(trmm(ctx, adj, dx, dy, np, k));
+  CK(cudaMemcpy2DAsync(Y, n * sizeof(cplx), dy, np * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  return sync_and_check(ctx);
+}
+
+// R (k×k) of the QR of A (m×k, m <= n_pad), and optionally Q (m×k) by orth_qr.
+extern "C" int rls_test_qr(rls_ctx* ctx, int64_t m, int k, const rls_c64* A, rls_c64* R, rls_c64* Q) {
+  RET(need_space(ctx));
+  if (m < k || m > ctx->n_pad || k < 1 || k > ctx->small_dim || !A || !R) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  const int64_t np = ctx->n_pad;
+  cplx* d = t.alloc<cplx>((size_t)np * k);
+  cplx* dR = t.alloc<cplx>((size_t)k * k);
+  if (!d || !dR) return RLS_ERR_NOMEM;
+  CK(cudaMemcpy2DAsync(d, np * sizeof(cplx), A, m * sizeof(cplx), m * sizeof(cplx), k, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  if (Q) {
+    if (k > 64) return RLS_ERR_ARG;
+    RET(orth_qr(ctx, np, d, np, k, dR));
+    CK(cudaMemcpy2DAsync(Q, m * sizeof(cplx), d, np * sizeof(cplx), m * sizeof(cplx), k, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  } else {
+    RET(tsqr_r(ctx, np, d, np, k, dR));
+  }
+  CK(cudaMemcpyAsync(R, dR, sizeof(cplx) * k * k, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}
+
+extern "C" int rls_test_svd_rr(rls_ctx* ctx, int nS, int r, int sideL, int lq, const rls_c64* R, double* sigma,
+                               double* lam, rls_c64* G) {
+  RET(need_space(ctx));
+  if (nS < 1 || nS > 512 || r < 1 || r > nS || !R || !sigma || !lam || !G) return RLS_ERR_ARG;
+  if (lq && nS > r && 2 * r > nS) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  cplx* dR = t.alloc<cplx>((size_t)nS * nS);
+  cplx* dG = t.alloc<cplx>((size_t)nS * nS);
+  double* ds = t.alloc<double>((size_t)nS);
+  double* dl = t.alloc<double>((size_t)nS);
+  if (!dR || !dG || !ds || !dl) return RLS_ERR_NOMEM;
+  CK(cudaMemcpyAsync(dR, R, sizeof(cplx) * nS * nS, cudaMemcpyHostToDevice, ctx->stream));
+  const bool glob = nS > 80;
+  cplx* gA = glob ? t.alloc<cplx>((size_t)nS * nS) : nullptr;
+  cplx* gV = glob ? t.alloc<cplx>((size_t)nS * nS) : nullptr;
+  k_svd_rr<<<1, 256, svd_rr_smem_bytes(nS, r, glob), ctx->stream>>>(nS, r, sideL, lq, dR, nS, ds, dl, dG, nS, gA, gV);
+  RET(check_launch(ctx, "k_svd_rr"));
+  CK(cudaMemcpyAsync(sigma, ds, sizeof(double) * nS, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(lam, dl, sizeof(double) * r, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(G, dG, sizeof(cplx) * nS * nS, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}
+
+// find_rr_dim on Hz built from H1, H2 (pr×pr, column-major); G gets pr × rr.
+extern "C" int rls_test_heev_rr(rls_ctx* ctx, int pr, int r, const rls_c64* H1, const rls_c64* H2, rls_c64 z,
+                                double shift, double tau, int* rr, double* lam, rls_c64* G) {
+  RET(need_space(ctx));
+  if (pr < 1 || pr > ctx->pr_max || r < 1 || !H1 || !H2 || !rr || !G) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  cplx* d1 = t.alloc<cplx>((size_t)pr * pr);
+  cplx* d2 = t.alloc<cplx>((size_t)pr * pr);
+  if (!d1 || !d2) return RLS_ERR_NOMEM;
+  CK(cudaMemcpyAsync(d1, H1, sizeof(cplx) * pr * pr, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d2, H2, sizeof(cplx) * pr * pr, cudaMemcpyHostToDevice, ctx->stream));
+  cplx zz = cmk(z.re, z.im);
+  CK(cudaMemcpyAsync(ctx->zdev, &zz, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->taudev, &tau, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_heev_rr<<<1, HEEV_THREADS, heev_smem_bytes(pr), ctx->stream>>>(
+      pr, r, d1, d2, pr, ctx->zdev, ctx->taudev, shift, ctx->heev, ctx->pr_max, ctx->Gheev, ctx->pr_max,
+      (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev, ctx->derr);
+  RET(check_launch(ctx, "k_heev_rr"));
+  RET(d2h(ctx, rr, ctx->rr_dev, 1));
+  if (lam) CK(cudaMemcpyAsync(lam, ctx->lam_dev, sizeof(double) * pr, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpy2DAsync(G, pr * sizeof(cplx), ctx->Gheev, ctx->pr_max * sizeof(cplx), pr * sizeof(cplx), *rr,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}
+
+// updateRecycledSpace!(M, S, z, recySp, X; τ, r_sub = 1, force_add) on the device space.
+extern "C" int rls_test_space_update(rls_ctx* ctx, rls_c64 z, const rls_c64* X, double tau, int force_add,
+                                     int p_min) {
+  RET(need_space(ctx));
+  if (!X) return RLS_ERR_ARG;
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  const int r = ctx->r;
+  CK(cudaMemsetAsync(ctx->S, 0, sizeof(cplx) * np * r, ctx->stream));
+  CK(cudaMemcpy2DAsync(ctx->S, np * sizeof(cplx), X, n * sizeof(cplx), n * sizeof(cplx), r, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  RET(update_recycled_space(ctx, cmk(z.re, z.im), ctx->S, tau, force_add != 0, p_min));
+  return sync_and_check(ctx);
+}
+
+// Copies out the device space: p, V (n × p r), J1, J2, J5 and L, H1, H2 (p r × p r).
+// Any output pointer may be NULL.
+extern "C" int rls_test_space_get(rls_ctx* ctx, int* p, rls_c64* V, rls_c64* J1, rls_c64* J2, rls_c64* J5,
+                                  rls_c64* L, rls_c64* H1, rls_c64* H2) {
+  RET(need_space(ctx));
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  const int pr = ctx->p * ctx->r, ld = ctx->pr_max;
+  if (p) *p = ctx->p;
+  if (pr == 0) return RLS_OK;
+  const cplx* tall[4] = {ctx->V, ctx->J1, ctx->J2, ctx->J5};
+  rls_c64* tout[4] = {V, J1, J2, J5};
+  for (int i = 0; i < 4; ++i)
+    if (tout[i])
+      CK(cudaMemcpy2DAsync(tout[i], n * sizeof(cplx), tall[i], np * sizeof(cplx), n * sizeof(cplx), pr,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  const cplx* sq[3] = {ctx->L, ctx->H1, ctx->H2};
+  rls_c64* sout[3] = {L, H1, H2};
+  for (int i = 0; i < 3; ++i)
+    if (sout[i])
+      CK(cudaMemcpy2DAsync(sout[i], pr * sizeof(cplx), sq[i], ld * sizeof(cplx), pr * sizeof(cplx), pr,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}
+
+// fastSvdRaylRitz_implicit! on the device space: Ritz dimension, σ (r), X and W (n × r).
+extern "C" int rls_test_recycle(rls_ctx* ctx, rls_c64 z, double shift, double gap_tau, int* rr, double* sigma,
+                                rls_c64* X, rls_c64* W, double* w0norm) {
+  RET(need_space(ctx));
+  if (ctx->p < 1) return RLS_ERR_STATE;
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  const int r = ctx->r;
+  RecycleResult res{};
+  RET(recycle_step(ctx, cmk(z.re, z.im), shift, gap_tau, &res));
+  if (rr) *rr = res.rr;
+  if (w0norm) *w0norm = res.w0norm;
+  if (sigma) CK(cudaMemcpyAsync(sigma, ctx->sig_rec, sizeof(double) * r, cudaMemcpyDeviceToHost, ctx->stream));
+  if (X)
+    CK(cudaMemcpy2DAsync(X, n * sizeof(cplx), ctx->S, np * sizeof(cplx), n * sizeof(cplx), r, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  if (W)
+    CK(cudaMemcpy2DAsync(W, n * sizeof(cplx), ctx->S + np * r, np * sizeof(cplx), n * sizeof(cplx), r,
+                         cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}

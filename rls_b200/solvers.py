@@ -1,0 +1,283 @@
+"""psTriRecy / lobpcgSvd host interface over the C ABI (mirrors src/core/psTriRecy.jl).
+
+``psTriRecy(C, rec; control)`` keeps the reference's call shape: C dense (or
+sparse, densified), ``rec`` a Recursion, ``control`` a PsTriRecyControl; it
+returns ``(sigma_min, stats)``.  The one-time preprocessing (complex Schur
+factor, LAPACK zgees — psTriRecy.jl:6-14) runs on the host as in the reference
+and is timed into ``stats.preprocess_time_ns``; everything per grid point runs
+on the GPU through librls_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (LOG_FN, check, lib, ptr, c64, rls_lobpcg_control, rls_pstrirecy_control,
+                   rls_pstrirecy_stats, ArgumentError, DimensionMismatch)
+from .grid import Recursion
+
+EPS = float(np.finfo(np.float64).eps)
+
+
+@dataclass
+class PsTriRecyControl:
+    """psTriRecy.jl:350-370 (same fields, same defaults; shift = normC²·eps·100)."""
+    tol: float = 1e-3
+    normC: float = 1.0
+    shift: float = None
+    gap_tau: float = 1e-10
+    gap_tau_scale: float = 0.01
+    recy_tau: float = 1.5
+    recycle_fail_dist_thresh: float = float("nan")
+    r: int = 6
+    p: int = 50
+    p_min: int = 1
+    lobpcg_tol_scale: float = 0.1
+    lobpcg_side: str = "L"
+    implict_update: bool = False
+    implict_recycle: bool = True
+    collect_timing: bool = True
+    inner_verbose_override: int = None
+
+    def __post_init__(self):
+        if self.shift is None:
+            self.shift = self.normC ** 2 * EPS * 100
+
+    def c_struct(self) -> rls_pstrirecy_control:
+        return rls_pstrirecy_control(
+            self.tol, self.normC, self.shift, self.gap_tau, self.gap_tau_scale, self.recy_tau,
+            self.recycle_fail_dist_thresh, int(self.r), int(self.p), int(self.p_min), self.lobpcg_tol_scale,
+            ord(self.lobpcg_side), int(self.implict_update), int(self.implict_recycle), int(self.collect_timing),
+            0, -1 if self.inner_verbose_override is None else int(self.inner_verbose_override))
+
+
+@dataclass
+class PsTriRecyStats:
+    """psTriRecy.jl:257-292 (+ refine_it: LOBPCG iterations per point)."""
+    p_count: np.ndarray
+    r_recy: np.ndarray
+    pts: np.ndarray
+    M_vec_apps: np.ndarray
+    M_vec_apps_no_recycle: np.ndarray
+    R_vec_apps: np.ndarray
+    refine_it: np.ndarray
+    preprocess_time_ns: int = 0
+    recycle_time_ns: int = 0
+    qr_time_ns: int = 0
+    refine_time_ns: int = 0
+    update_time_ns: int = 0
+    mv_stats_available: bool = True
+    n_it: int = 0
+    n_pts: int = 0
+
+    @classmethod
+    def alloc(cls, nZ):
+        z = lambda: np.zeros(nZ, dtype=np.int64)
+        return cls(z(), z(), np.zeros(nZ, dtype=np.complex128), z(), z(), z(), z())
+
+
+@dataclass
+class LobpcgSvdControl:
+    """lobpcgSvd.jl:1-55."""
+    m: int
+    n: int
+    r: int
+    maxit: int = 2000
+    tol: float = 1e-3
+    side: str = "S"
+    verbose: int = 0
+    normC: float = 1.0
+    orth_type: str = "lapack"
+    conv_range: tuple = None
+    conv_thresh_type: int = 0
+
+    def __post_init__(self):
+        if self.conv_range is None:
+            self.conv_range = (1, self.r)
+        a, b = self.conv_range
+        if not (1 <= a <= b <= self.r):
+            raise ArgumentError(-1, f"conv_range={self.conv_range} must satisfy 1 <= first <= last <= r={self.r}")
+        if self.orth_type not in ("lapack", "shiftchol"):
+            raise ArgumentError(-1, f"orth_type={self.orth_type} must be :lapack or :shiftchol")
+        if self.conv_thresh_type not in (0, 1):
+            raise ArgumentError(-1, f"conv_thresh_type={self.conv_thresh_type} must be 0 or 1")
+
+    def c_struct(self) -> rls_lobpcg_control:
+        return rls_lobpcg_control(self.m, self.n, self.r, self.maxit, self.tol, ord(self.side), self.verbose,
+                                  self.normC, 0 if self.orth_type == "lapack" else 1, self.conv_thresh_type,
+                                  self.conv_range[0], self.conv_range[1])
+
+
+def pre_process(C_) -> np.ndarray:
+    """psTriRecy.jl:6-14 (square dense branch): upper-triangular complex Schur factor.
+
+    Host LAPACK zgees through SciPy, as the reference's ``schur(C)``.  A sparse C is
+    densified first: σ_min(C − zI) is invariant under the unitary similarity, so the
+    Schur path computes the same σ as the reference's sparse QR path.
+    """
+    import scipy.linalg as sla
+    import scipy.sparse as sp
+    if sp.issparse(C_):
+        C_ = C_.toarray()
+    A = np.asarray(C_, dtype=np.complex128)
+    if A.ndim != 2 or A.shape[0] != A.shape[1]:
+        raise DimensionMismatch(-2, f"pre_process only supports square matrices here, got size {A.shape}")
+    T, _ = sla.schur(A, output="complex", check_finite=True)
+    return np.triu(T)
+
+
+class SchurFactor:
+    """A precomputed Schur factor T (skip pre_process on repeated runs)."""
+
+    def __init__(self, T, preprocess_time_ns=0):
+        self.T = np.asfortranarray(np.asarray(T, dtype=np.complex128))
+        self.preprocess_time_ns = preprocess_time_ns
+
+
+class Engine:
+    """One device context (stream, workspaces, uploaded operator) — one per host thread."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().rls_ctx_create(C.byref(h), int(device)))
+        self._h = h
+        self._log_cb = None
+        self._T_id = None
+        self.n = 0
+
+    def close(self):
+        if self._h:
+            lib().rls_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_schur(self, T: np.ndarray):
+        T = np.asfortranarray(np.asarray(T, dtype=np.complex128))
+        n = T.shape[0]
+        check(lib().rls_set_schur(self._h, n, ptr(T), n), self._h)
+        self._T_id = id(T)
+        self.n = n
+
+    def set_log(self, fn, verbose=1):
+        if fn is None:
+            self._log_cb = None
+            check(lib().rls_ctx_set_log(self._h, LOG_FN(), None, 0), self._h)
+            return
+        cb = LOG_FN(lambda line, user: fn(line.decode()))
+        self._log_cb = cb
+        check(lib().rls_ctx_set_log(self._h, cb, None, int(verbose)), self._h)
+
+    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None):
+        nZ = len(rec.Z)
+        Z = np.ascontiguousarray(rec.Z, dtype=np.complex128)
+        sigma = np.full(nZ, np.nan)
+        st = PsTriRecyStats.alloc(nZ)
+        cst = rls_pstrirecy_stats()
+        i64 = C.POINTER(C.c_int64)
+        cst.p_count = st.p_count.ctypes.data_as(i64)
+        cst.r_recy = st.r_recy.ctypes.data_as(i64)
+        cst.pts = st.pts.ctypes.data_as(C.POINTER(c64))
+        cst.M_vec_apps = st.M_vec_apps.ctypes.data_as(i64)
+        cst.M_vec_apps_no_recycle = st.M_vec_apps_no_recycle.ctypes.data_as(i64)
+        cst.R_vec_apps = st.R_vec_apps.ctypes.data_as(i64)
+        cst.refine_it = st.refine_it.ctypes.data_as(i64)
+        x0 = None
+        if X0 is not None:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+            if x0.shape != (self.n, control.r):
+                raise DimensionMismatch(-2, f"X0 must be {(self.n, control.r)}, got {x0.shape}")
+        g = rec.c_grid()
+        cc = control.c_struct()
+        check(lib().rls_pstrirecy_schur(self._h, ptr(Z), nZ, C.byref(g), C.byref(cc), ptr(x0), ptr(sigma),
+                                        C.byref(cst)), self._h)
+        for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
+            setattr(st, f, int(getattr(cst, f)))
+        st.mv_stats_available = bool(cst.mv_stats_available)
+        return sigma, st
+
+    def lobpcg_svd_invtri(self, z: complex, control: LobpcgSvdControl, X0=None):
+        """lobpcgSvd(InvMat(adjoint(T − zI)), X0, I, keep, control) → (σ, it, X, σ_r)."""
+        r = control.r
+        x0 = None
+        if X0 is not None:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+        X = np.zeros((self.n, r), dtype=np.complex128, order="F")
+        sr = np.zeros(r)
+        s = C.c_double()
+        it = C.c_int64()
+        cc = control.c_struct()
+        check(lib().rls_lobpcg_svd_invtri(self._h, c64(z.real, z.imag), ptr(x0), C.byref(cc), ptr(X), ptr(sr),
+                                          C.byref(s), C.byref(it)), self._h)
+        return s.value, it.value, X, sr
+
+
+_engines = {}
+
+
+def _engine(device=0) -> Engine:
+    e = _engines.get(device)
+    if e is None:
+        e = Engine(device)
+        _engines[device] = e
+    return e
+
+
+def _print_startup(io, rec, control):
+    """psTriRecy.jl:554-577."""
+    io.write("[psTriRecy] rec: x_range=[%.6f, %.6f], y_range=[%.6f, %.6f], n_x=%d, n_y=%d, k=%d, n_pts=%d\n"
+             % (rec.x_st, rec.x_ed, rec.y_st, rec.y_ed, rec.n_x, rec.n_y, rec.k, rec.n_x * rec.n_y))
+    io.write("[psTriRecy] control:\n")
+    for f in control.__dataclass_fields__:
+        io.write(f"  {f} = {getattr(control, f)!r}\n")
+
+
+def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int = 1, io=None, X0=None,
+              device: int = 0):
+    """psTriRecy (psTriRecy.jl:889-913) → (σ_min in rec.Z order, PsTriRecyStats).
+
+    ``X0`` (n × r) stands in for the reference's ``rand!(X)``; None draws a
+    deterministic uniform [0,1) complex block on the device.
+    """
+    control = control or PsTriRecyControl()
+    io = io if io is not None else sys.stdout
+    if verbose >= 1:
+        _print_startup(io, rec, control)
+    eng = _engine(device)
+    t0 = time.perf_counter_ns()
+    if isinstance(C_, SchurFactor):
+        T = C_.T
+        pre_ns = C_.preprocess_time_ns
+    else:
+        T = pre_process(C_)
+        pre_ns = time.perf_counter_ns() - t0
+    eng.set_schur(T)
+    if verbose >= 1:
+        eng.set_log(lambda line: (io.write(line + "\n"), io.write("-" * 100 + "\n")), verbose)
+    else:
+        eng.set_log(None)
+    try:
+        sigma, st = eng.pstrirecy(rec, control, X0=X0)
+    finally:
+        eng.set_log(None)
+    st.preprocess_time_ns = pre_ns
+    if verbose >= 1:
+        io.write(f"Total M vec apps for singular value problem: {int(st.M_vec_apps.sum())}\n")
+        if control.collect_timing:
+            if st.preprocess_time_ns > 0:
+                io.write("Total preprocess time for singular value problem: %.6f seconds\n" % (st.preprocess_time_ns / 1e9))
+            io.write("Total recycle time for singular value problem: %.6f seconds\n" % (st.recycle_time_ns / 1e9))
+            io.write("Total refine time for singular value problem: %.6f seconds\n" % (st.refine_time_ns / 1e9))
+            io.write("Total update time for singular value problem: %.6f seconds\n" % (st.update_time_ns / 1e9))
+        io.write(f"Total R vec apps for singular value problem: {int(st.R_vec_apps.sum())}\n")
+        io.write(f"Total it for singular value problem: {st.n_it}\n")
+        io.write(f"Total pt for singular value problem: {st.n_pts}\n")
+    return sigma, st

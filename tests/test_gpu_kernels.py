@@ -1,0 +1,157 @@
+"""Kernel-level parity on the GPU: each device routine against the LAPACK/BLAS routine
+the reference calls at that point (SciPy/NumPy FP64 on the same inputs).
+
+Floating-point tolerances are relative to the operand norms (FP64 throughout).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from oracle.linalg import svd_inplace, lq_rows_inplace
+from oracle.recycle import find_rr_dim, affine_combine
+from rls_b200._lib import lib, check, ptr, c64
+from rls_b200.solvers import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def crand(rng, *shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+@pytest.fixture(scope="module")
+def eng_T(cuda_device):
+    rng = np.random.default_rng(7)
+    n = 300
+    A = crand(rng, n, n) / np.sqrt(n)
+    T = np.triu(sla.schur(A, output="complex")[0])
+    e = Engine(cuda_device)
+    e.set_schur(T)
+    check(lib().rls_test_setup(e._h, 6, 20), e._h)
+    return e, T
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+@pytest.mark.parametrize("k", [1, 6, 18])
+def test_trsm_matches_ztrsm(eng_T, adj, k):
+    e, T = eng_T
+    n = T.shape[0]
+    rng = np.random.default_rng(k + 10 * adj)
+    B = np.asfortranarray(crand(rng, n, k))
+    z = 0.3 - 0.2j
+    X = np.zeros((n, k), dtype=np.complex128, order="F")
+    check(lib().rls_test_trsm(e._h, c64(z.real, z.imag), adj, k, ptr(B), ptr(X)), e._h)
+    R = T - z * np.eye(n)
+    ref = sla.solve_triangular(R, B, lower=False, trans="C" if adj else "N")
+    err = np.linalg.norm(X - ref) / np.linalg.norm(ref)
+    assert err < 1e-12, err
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+@pytest.mark.parametrize("k", [1, 6, 12])
+def test_trmm_matches_ztrmm(eng_T, adj, k):
+    e, T = eng_T
+    n = T.shape[0]
+    rng = np.random.default_rng(100 + k)
+    X = np.asfortranarray(crand(rng, n, k))
+    Y = np.zeros((n, k), dtype=np.complex128, order="F")
+    check(lib().rls_test_trmm(e._h, adj, k, ptr(X), ptr(Y)), e._h)
+    ref = (T.conj().T if adj else T) @ X
+    assert np.linalg.norm(Y - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("m,k", [(300, 1), (300, 6), (257, 18), (300, 40), (200, 64), (300, 70)])
+def test_qr_factor(eng_T, m, k):
+    e, _ = eng_T
+    rng = np.random.default_rng(m * 1000 + k)
+    A = np.asfortranarray(crand(rng, m, k))
+    # graded columns to exercise stability
+    A *= np.logspace(0, -6, k)[None, :]
+    R = np.zeros((k, k), dtype=np.complex128, order="F")
+    check(lib().rls_test_qr(e._h, m, k, ptr(A), ptr(R), None), e._h)
+    Rref = np.linalg.qr(A, mode="r")
+    # R is unique up to a unit-modulus scaling of its rows: compare RᴴR and |diag|
+    assert np.allclose(np.abs(np.diag(R)), np.abs(np.diag(Rref)), rtol=1e-10, atol=0)
+    G = R.conj().T @ R
+    assert np.linalg.norm(G - A.conj().T @ A) <= 1e-12 * np.linalg.norm(A) ** 2
+    assert np.allclose(np.tril(R, -1), 0)
+    if k <= 64:
+        Q = np.zeros((m, k), dtype=np.complex128, order="F")
+        R2 = np.zeros((k, k), dtype=np.complex128, order="F")
+        check(lib().rls_test_qr(e._h, m, k, ptr(A), ptr(R2), ptr(Q)), e._h)
+        assert np.linalg.norm(Q.conj().T @ Q - np.eye(k)) < 1e-13
+        assert np.linalg.norm(Q @ R2 - A) <= 1e-13 * np.linalg.norm(A)
+
+
+@pytest.mark.parametrize("nS,r,sideL,lq", [(6, 6, 1, 1), (12, 6, 1, 1), (18, 6, 1, 1), (18, 6, 0, 1),
+                                            (9, 6, 0, 0), (40, 6, 0, 0), (3, 1, 1, 1)])
+def test_svd_rr_matches_zgesdd(eng_T, nS, r, sideL, lq):
+    e, _ = eng_T
+    rng = np.random.default_rng(nS * 7 + r)
+    Rin = np.asfortranarray(np.triu(crand(rng, nS, nS)) * np.logspace(0, -4, nS)[None, :])
+    sig = np.zeros(nS)
+    lam = np.zeros(r)
+    G = np.zeros((nS, nS), dtype=np.complex128, order="F")
+    check(lib().rls_test_svd_rr(e._h, nS, r, sideL, lq, ptr(Rin), ptr(sig), ptr(lam), ptr(G)), e._h)
+    s_ref = np.zeros(nS)
+    V_ref = np.zeros((nS, nS), dtype=np.complex128)
+    svd_inplace(Rin.copy(), s_ref, V_ref, ascending=not sideL)
+    if sideL:
+        s_ref[:r] = 1.0 / s_ref[:r]
+    assert np.allclose(sig, s_ref, rtol=1e-11, atol=1e-15 * np.abs(s_ref).max())
+    assert np.allclose(lam, s_ref[:r] ** 2, rtol=1e-11)
+    # Ritz vectors: columns agree up to unit phases
+    for j in range(r):
+        ov = abs(np.vdot(G[:, j], V_ref[:, j]))
+        assert ov > 1 - 1e-9, (j, ov)
+    if lq and nS > r:
+        Q_mat = V_ref[:r, r:nS].copy()
+        lq_rows_inplace(Q_mat)
+        GP_ref = V_ref[:, r:nS] @ Q_mat.conj().T
+        GP = G[:, r:2 * r]
+        Pr = GP_ref @ GP_ref.conj().T
+        Pg = GP @ GP.conj().T
+        assert np.linalg.norm(Pr - Pg) < 1e-9
+
+
+def _hz_pair(rng, pr):
+    B = crand(rng, 3 * pr, pr)
+    H1 = B.conj().T @ B
+    H2 = crand(rng, pr, pr) * 0.3
+    return np.asfortranarray(H1), np.asfortranarray(H2)
+
+
+@pytest.mark.parametrize("pr,r,tau", [(12, 6, 1e-10), (36, 6, 1e-10), (90, 6, 1e-12), (120, 6, 1e-10),
+                                      (6, 6, 1e-10), (18, 6, 1e10)])
+def test_heev_rr_matches_zheevr(eng_T, pr, r, tau):
+    e, _ = eng_T
+    rng = np.random.default_rng(pr + 3)
+    H1, H2 = _hz_pair(rng, pr)
+    z = 0.4 + 0.1j
+    shift = 1e-13
+    rr = C.c_int(0)
+    lam = np.zeros(pr)
+    G = np.zeros((pr, pr), dtype=np.complex128, order="F")
+    check(lib().rls_test_heev_rr(e._h, pr, r, ptr(H1), ptr(H2), c64(z.real, z.imag), shift, tau, C.byref(rr),
+                                 ptr(lam), ptr(G)), e._h)
+    Hz = affine_combine(z, H1, H2, H2.conj().T, np.eye(pr), shift=shift)
+    Hz = np.triu(Hz) + np.triu(Hz, 1).conj().T
+    Hz[np.diag_indices(pr)] = Hz.diagonal().real
+    rr_ref, G_ref = find_rr_dim(Hz, r, tau)
+    assert rr.value == rr_ref
+    w = np.linalg.eigvalsh(Hz)
+    scale = abs(w).max()
+    assert abs(lam[pr - 1] - w[-1]) <= 1e-12 * scale
+    k = rr.value
+    assert np.allclose(lam[:min(k, pr - 1)], w[:min(k, pr - 1)], atol=1e-12 * scale, rtol=0)
+    Gk = G[:, :k]
+    assert np.linalg.norm(Gk.conj().T @ Gk - np.eye(k)) < 1e-10
+    # invariant subspace: projector equality (eigenvectors are unique only up to phase / within clusters)
+    Pg = Gk @ Gk.conj().T
+    Pr = G_ref[:, :k] @ G_ref[:, :k].conj().T
+    assert np.linalg.norm(Pg - Pr) < 1e-8
+    # residual of the Ritz pairs
+    res = np.linalg.norm(Hz @ Gk - Gk * w[:k][None, :]) / scale
+    assert res < 1e-10

@@ -1,0 +1,97 @@
+"""psTriRecy on the GPU against the CPU oracle and the FP64 dense-SVD oracle.
+
+Bar: |σ_gpu − σ_oracle| <= 1e-4·normC on every grid point
+and the relative residual of every accepted point <= tol; the dense SVD gives
+the FP64 truth on sampled points.
+"""
+import numpy as np
+import pytest
+
+from oracle.pstrirecy import PsTriRecyControl as OControl, ps_tri_recy_schur, dense_sigma_min
+from oracle.lobpcg import LobpcgSvdControl as OLobCtl, LobpcgSvdKeep, lobpcg_svd
+from oracle.pstrirecy import InvAdjR
+from oracle import recugrid as ogrid
+import rls_b200 as R
+from rls_b200.examples import sprand, landau
+
+pytestmark = pytest.mark.gpu
+
+
+def _case_sprand(N=240, grid=(0.45, 0.55, 0.0, 0.1, 10, 10, 5)):
+    C = sprand(N).toarray()
+    return C, 3.2, grid
+
+
+def _x0(n, r, seed=3):
+    rng = np.random.default_rng(seed)
+    return rng.random((n, r)) + 1j * rng.random((n, r))
+
+
+@pytest.fixture(scope="module")
+def sprand_case(cuda_device):
+    C, normC, grid = _case_sprand()
+    T = R.pre_process(C)
+    return C, T, normC, grid
+
+
+def test_lobpcg_single_point_matches_oracle(sprand_case):
+    C, T, normC, grid = sprand_case
+    n, r = T.shape[0], 6
+    X0 = _x0(n, r)
+    z = 0.5 + 0.05j
+    eng = R.Engine(0)
+    eng.set_schur(T)
+    ctl = R.LobpcgSvdControl(m=n, n=n, r=r, conv_range=(1, 1), tol=1e-5, side="L", normC=normC)
+    s, it, X, sr = eng.lobpcg_svd_invtri(z, ctl, X0=X0)
+    keep = LobpcgSvdKeep(n, n, r)
+    keep.S[:, :r] = X0
+    octl = OLobCtl(m=n, n=n, r=r, conv_range=(1, 1), tol=1e-5, side="L", normC=normC)
+    Rz = T - z * np.eye(n)
+    s_o, it_o = lobpcg_svd(InvAdjR(Rz), keep.S[:, :r], None, keep, octl)
+    assert abs(it - it_o) <= 1
+    truth = dense_sigma_min(C, z)
+    assert abs(sr[0] - truth) <= 1e-6 * normC
+    assert abs(sr[0] - keep.sigma[0]) <= 1e-6 * normC
+    # Ritz vector of σ_min agrees with the oracle's up to phase
+    ov = abs(np.vdot(X[:, 0], keep.S[:, 0])) / (np.linalg.norm(X[:, 0]) * np.linalg.norm(keep.S[:, 0]))
+    assert ov > 1 - 1e-6
+
+
+@pytest.mark.parametrize("p,r", [(60, 6), (6, 2)])
+def test_pstrirecy_matches_oracle(sprand_case, p, r):
+    C, T, normC, grid = sprand_case
+    n = T.shape[0]
+    X0 = _x0(n, r)
+    rec = R.recursion_grid(*grid)
+    ctl = R.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=p, r=r, recy_tau=1.6)
+    sig, st = R.psTriRecy(R.SchurFactor(T), rec, ctl, verbose=0, X0=X0)
+    orec = ogrid.recursion_grid(*grid)
+    octl = OControl(normC=normC, tol=1e-4, p_min=1, p=p, r=r, recy_tau=1.6)
+    sig_o, st_o = ps_tri_recy_schur(T, orec, octl, X0=X0)
+    assert np.all(np.isfinite(sig))
+    assert np.max(np.abs(sig - sig_o)) <= 1e-4 * normC
+    # dense-SVD truth on every grid point (n is small)
+    truth = np.array([dense_sigma_min(C, z) for z in rec.Z])
+    assert np.max(np.abs(sig - truth)) <= 1e-4 * normC
+    # Identical trajectory over the leading points: same space size, same recycle
+    # decision, same Ritz dimension.  (Later points may diverge: the unconverged
+    # Ritz vectors that enter the space differ at rounding level, and the
+    # recycle-acceptance test is a threshold on them.)
+    lead = 12
+    assert np.array_equal(st.p_count[:lead], st_o.p_count[:lead]), (st.p_count[:lead], st_o.p_count[:lead])
+    assert np.array_equal(st.refine_it[:lead] > 0, st_o.refine_it[:lead] > 0)
+    assert np.array_equal(st.r_recy[:lead], st_o.r_recy[:lead])
+    assert st.n_pts == int(np.sum(st.refine_it > 0))
+
+
+def test_pstrirecy_laser_small(cuda_device):
+    C = landau(180, 40 * np.pi)
+    T = R.pre_process(C)
+    n, r = T.shape[0], 6
+    X0 = _x0(n, r, seed=11)
+    grid = (-1.1, 1.2, -1.1, 1.1, 8, 8, 4)
+    rec = R.recursion_grid(*grid)
+    ctl = R.PsTriRecyControl(normC=1.0, tol=1e-4, recy_tau=1.6, p=60)
+    sig, st = R.psTriRecy(R.SchurFactor(T), rec, ctl, verbose=0, X0=X0)
+    truth = np.array([dense_sigma_min(C, z) for z in rec.Z])
+    assert np.max(np.abs(sig - truth)) <= 1e-4
