@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""σ_min grid-point throughput of psTriRecy on the B200 (one JSON line on rank 0).
+
+Workload: the reference's sprand case on its full grid — N = 4000 sparse random C
+(example/sprand/sprand.jl:11-27, NumPy PCG64 instance with the script's seed),
+densified and reduced once to its complex Schur factor on the host (timed apart,
+as the reference's preprocess_time_ns), 200 × 200 grid on [0.45,0.55]×[0,0.1],
+k = 20, PsTriRecyControl(normC=3.2, tol=1e-4, p_min=1, p=60, recy_tau=1.6),
+complex128 throughout.
+
+A step is `--chunk` consecutive points of the grid's traversal order, processed
+with the recycled space carried from the previous step exactly as the reference's
+loop carries it; W warm-up steps, then K timed steps.  The Schur factor (256 MB)
+is larger than L2, so every step streams it from HBM.
+
+  value : points / device time of the K timed steps (CUDA events on the engine's
+          stream), Schur factor resident in HBM.
+  e2e   : a fresh context through the public C ABI with host buffers: upload of
+          the Schur factor from host memory plus steps 0..W+K-1 (grid points in,
+          σ out), wall clock.
+  --impl reference : the CPU restatement (oracle/, the reference's algorithm with
+          LAPACK through SciPy on all host cores) on the same traversal, each step
+          a bounded sample of --ref-chunk points.
+
+Multi-GPU (torchrun): every rank runs its own traversal starting at a different
+strip of the grid (independent recycled spaces, weak scaling); the only
+collective is the final max-over-ranks of the timings.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "σ_min grid pts/s (psTriRecy, sprand N=4000, 200×200 grid, k=20, tol 1e-4)"
+GRID = (0.45, 0.55, 0.0, 0.1, 200, 200, 20)
+N_MAT = 4000
+NORMC = 3.2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chunk", type=int, default=200, help="grid points per step")
+    ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
+    ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
+    ap.add_argument("--n", type=int, default=N_MAT)
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def control():
+    from oracle.pstrirecy import PsTriRecyControl as OC  # used only by the CPU legs
+    return OC
+
+
+def build_inputs(n):
+    from rls_b200.examples import sprand
+    from rls_b200.solvers import pre_process
+    C = sprand(n).toarray()
+    t0 = time.perf_counter()
+    T = pre_process(C)
+    return C, np.asfortranarray(T), time.perf_counter() - t0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.rows = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9 and parts[0] == self.gpu:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.th is not None:
+            self.th.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in self.rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in self.rows)}
+
+
+def cpu_baseline(T, rec, ctl, X0, budget_s, min_pts=2):
+    """The oracle (CPU restatement) from the start of the traversal, bounded by time."""
+    from oracle.pstrirecy import PsTriRecyRun
+    run = PsTriRecyRun(T, rec, ctl, X0=X0)
+    t0 = time.perf_counter()
+    i = 0
+    while i < len(rec.Z) and (i < min_pts or time.perf_counter() - t0 < budget_s):
+        run.run(i, i + 1)
+        i += 1
+    el = time.perf_counter() - t0
+    return {"value": i / el, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"first {i} points of the 200x200 traversal (recycled space carried), "
+                      f"CPU restatement with SciPy LAPACK on all host threads, {el:.1f} s"}
+
+
+def base_line(args, n_gpus):
+    return {"metric": METRIC, "unit": "pts/s", "n_gpus": n_gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic (sprand generator, NumPy PCG64 seed 20260318)",
+            "config": {"workload": "psTriRecy sprand N=4000 dense-Schur, 200x200 grid [0.45,0.55]x[0,0.1], k=20, "
+                                   "tol=1e-4, p=60, r=6, recy_tau=1.6",
+                       "n": args.n, "grid": list(GRID), "points_per_step": None,
+                       "l2": "inputs larger than L2 (Schur factor 256 MB streamed every step)"}}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import rls_b200.examples  # noqa: F401  (generator only)
+    from oracle import recugrid as G
+    from oracle.pstrirecy import PsTriRecyControl, PsTriRecyRun
+    C, T, pre_s = build_inputs(args.n)
+    rec = G.recursion_grid(*GRID)
+    ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
+    rng = np.random.default_rng(1)
+    X0 = rng.random((args.n, 6)) + 1j * rng.random((args.n, 6))
+    run = PsTriRecyRun(T, rec, ctl, X0=X0)
+    s = args.ref_chunk
+    for w in range(args.warmup):
+        run.run(w * s, (w + 1) * s)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        a = (args.warmup + k) * s
+        run.run(a, a + s)
+    el = time.perf_counter() - t0
+    v = args.steps * s / el
+    out = base_line(args, 1)
+    out.update({"impl": "reference", "value": v, "ms_per_step": el * 1e3 / args.steps,
+                "cpu_baseline": {"value": v, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+                                 "sample": f"{s} points per step of the 200x200 traversal after {args.warmup} warm-up "
+                                           f"steps; CPU restatement of psTriRecy (SciPy LAPACK, all host threads)"},
+                "e2e": {"value": v, "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "preprocess_s": pre_s})
+    out["config"]["points_per_step"] = s
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import rls_b200 as R
+    from rls_b200.solvers import Engine, PsTriRecyControl, PsTriRecyStats
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    # inputs: rank 0 reduces C to Schur form, every rank receives T
+    if rank == 0:
+        C, T, pre_s = build_inputs(args.n)
+    else:
+        C, T, pre_s = None, None, 0.0
+    if world > 1:
+        buf = torch.empty((args.n, args.n, 2), dtype=torch.float64, device="cuda")
+        if rank == 0:
+            buf.copy_(torch.view_as_real(torch.from_numpy(np.ascontiguousarray(T.T))))
+        dist.broadcast(buf, 0)
+        T = np.asfortranarray(torch.view_as_complex(buf).cpu().numpy().T)
+        del buf
+
+    rec = R.recursion_grid(*GRID)
+    nZ = len(rec.Z)
+    strip = GRID[4] * GRID[6]
+    nstrips = nZ // strip
+    off = (rank * nstrips // world) * strip
+    sub = R.Recursion(*GRID)
+    sub.Z = np.ascontiguousarray(rec.Z[off:])
+    ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
+    rng = np.random.default_rng(1 + rank)
+    X0 = rng.random((args.n, 6)) + 1j * rng.random((args.n, 6))
+    s = args.chunk
+    need = (args.warmup + args.steps) * s
+    if need > len(sub.Z):
+        raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds the {len(sub.Z)} points of this rank")
+
+    eng = Engine(local)
+    eng.set_schur(T)
+    sigma = np.full(len(sub.Z), np.nan)
+    st = PsTriRecyStats.alloc(len(sub.Z))
+    cst = eng.stats_struct(st)
+    for w in range(args.warmup):
+        eng.pstrirecy_range(sub, ctl, w * s, (w + 1) * s, sigma, st, cst, X0=X0)
+    eng.set_profile(True)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
+                       os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
+    clk.start()
+    time.sleep(0.3)
+    l0 = eng.launches()
+    ev0.record(stream)
+    for k in range(args.steps):
+        a = (args.warmup + k) * s
+        eng.pstrirecy_range(sub, ctl, a, a + s, sigma, st, cst)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    l1 = eng.launches()
+    clk.stop()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    timed = slice(args.warmup * s, (args.warmup + args.steps) * s)
+    refines = int(np.sum(st.refine_it[timed] > 0))
+    prof = {k: eng.profile(k) for k in range(4)}
+
+    # end to end through the public C ABI on a fresh context, host buffers in and out
+    e2e = None
+    if not args.no_e2e:
+        eng2 = Engine(local)
+        sigma2 = np.full(len(sub.Z), np.nan)
+        st2 = PsTriRecyStats.alloc(len(sub.Z))
+        cst2 = eng2.stats_struct(st2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng2.set_schur(T)
+        for k in range(args.warmup + args.steps):
+            eng2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sigma2, st2, cst2, X0=X0)
+        el = time.perf_counter() - t0
+        te = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        el = float(te.item())
+        nsteps = args.warmup + args.steps
+        T_bytes = args.n * args.n * 16
+        e2e = {"value": world * nsteps * s / el, "unit": "pts/s",
+               "h2d_bytes_per_step": int((T_bytes + nsteps * s * 16) / nsteps),
+               "d2h_bytes_per_step": int(s * 8),
+               "span": f"upload of T + steps 0..{nsteps - 1} of the traversal"}
+        same = np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12)
+        e2e["matches_device_run"] = bool(same)
+        eng2.close()
+
+    out = base_line(args, world)
+    value = world * args.steps * s / (ms_max / 1e3)
+    out.update({"value": value, "ms_per_step": ms_max / args.steps})
+    out["config"]["points_per_step"] = s
+    out["config"]["parallelism"] = f"grid strips x{world} (independent traversals)"
+    out["config"]["refine_fraction_timed"] = refines / (args.steps * s)
+    out["preprocess_s"] = pre_s
+    out["gpu_launches"] = int(l1 - l0)
+    out["clocks"] = clk.summary()
+    # roofline of the dominant profiled kernel
+    names = {0: "k_trsm_dataflow (R⁻¹/R⁻ᴴ on T−zI)", 1: "k_heev_rr (projected eigensolve)",
+             2: "k_gemm_rows (recycle X/W product)", 3: "k_trmm_partial+reduce (T·V, Tᴴ·[J5 V])"}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    shares = {k: v[1] for k, v in prof.items()}
+    top = max((k for k in prof if k != 1), key=lambda k: shares[k])
+    cnt, tot_ms, work = prof[top]
+    achieved = (work / cnt) / (tot_ms / cnt / 1e3) / 1e9 if cnt else 0.0
+    out["roofline"] = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": hbm_peak,
+                       "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                       "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                       "launches": cnt, "avg_us": tot_ms / max(cnt, 1) * 1e3}
+    out["kernel_time_ms"] = {names[k]: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}
+    if prof[1][0]:
+        c1, t1, f1 = prof[1]
+        out["heev_fp64"] = {"gflops": f1 / (t1 / 1e3) / 1e9, "launches": c1, "avg_us": t1 / c1 * 1e3}
+    if rank == 0 and world == 1:
+        from oracle.pstrirecy import PsTriRecyControl as OC
+        from oracle import recugrid as G
+        out["cpu_baseline"] = cpu_baseline(T, G.recursion_grid(*GRID),
+                                           OC(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6), X0,
+                                           args.cpu_sample_s)
+    if e2e is not None:
+        out["e2e"] = e2e
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -113,6 +113,23 @@ void rls_ctx_destroy(rls_ctx* ctx);
 const char* rls_last_error(const rls_ctx* ctx);
 const char* rls_status_string(int status);
 int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verbose);
+/* The context's cudaStream_t (as void*), for callers that time or order work
+ * around the engine.  No reference counterpart. */
+void* rls_ctx_stream(rls_ctx* ctx);
+/* Number of kernel launches this context has issued so far.  No reference counterpart. */
+int64_t rls_ctx_launches(const rls_ctx* ctx);
+/* Ritz basis of the recycle step when the Ritz dimension equals the space size
+ * (r_ == p·r): 1 (default) forms X = V·G1·G2 as for r_ < p·r; 0 keeps the
+ * reference's X = V·G2 (fastRaylRitz.jl:199-202), whose result depends on the
+ * phases the eigensolver gives the columns of G1. */
+int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always);
+/* Per-kernel CUDA-event timing: kernel 0 = triangular solve, 1 = projected
+ * eigensolve, 2 = recycle-step streaming product, 3 = triangular multiply.
+ * set_profile resets the counters; profile_get returns launches, total device
+ * milliseconds and algorithmic work (bytes; flops for kernel 1).  No reference
+ * counterpart (the reference times phases with time_ns, psTriRecy.jl:306-309). */
+int rls_ctx_set_profile(rls_ctx* ctx, int on);
+int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work);
 
 /* ---- recursion grid (bit-exact) ------------------------------------------- */
 
@@ -154,6 +171,17 @@ int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
 int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
                         const rls_pstrirecy_control* control, const rls_c64* X0,
                         double* sigma_min, rls_pstrirecy_stats* stats);
+
+/* The same loop over points i_begin..i_end-1 only (0-based, end exclusive).  A
+ * call with i_begin = 0 starts a run (space reset, X0 used); a call with
+ * i_begin > 0 continues the run whose previous call ended at i_begin, carrying
+ * the recycled space, as consecutive iterations of the reference's loop
+ * (psTriRecy.jl:735-856).  Z, sigma_min and the stats arrays are the full-length
+ * (nZ) arrays; only entries of the range are written.  No reference
+ * counterpart: it lets a caller stream a long grid in pieces. */
+int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                              const rls_pstrirecy_control* control, const rls_c64* X0, int64_t i_begin,
+                              int64_t i_end, double* sigma_min, rls_pstrirecy_stats* stats);
 
 /* lobpcgSvd (src/core/lobpcgSvd.jl:365-477) on C = InvMat(adjoint(T − zI)) with
  * K = I, as psTriRecy calls it at psTriRecy.jl:797-808.  X0 (n × r) may be

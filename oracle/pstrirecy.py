@@ -123,83 +123,98 @@ def residual_norm_ok(W, sigma, tol, normC):
     return np.linalg.norm(W[:, 0]) < normC * max(sigma * tol, normC * np.sqrt(2) * EPS)
 
 
-def ps_tri_recy_schur(T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None):
-    """_psTriRecy_impl (psTriRecy.jl:708-881) on a precomputed Schur factor T.
+class PsTriRecyRun:
+    """The loop of _psTriRecy_impl (psTriRecy.jl:708-881) on a precomputed Schur factor T,
+    resumable over index ranges (state carried between calls as the reference's loop
+    carries it between iterations).
 
-    ``X0`` (n×r) replaces the reference's ``rand!(X)`` (psTriRecy.jl:607): the
-    Julia RNG stream is not reproducible here, so the caller supplies it.
-    Returns (σ_min, stats).
+    ``X0`` (n×r) replaces the reference's ``rand!(X)`` (psTriRecy.jl:607): the Julia
+    RNG stream is not reproducible here, so the caller supplies it.
     """
-    n = T.shape[0]
-    r = ctl.r
-    M, S = TriOp(T), IdentityOp()
-    rs = RecycledSpace(n, n, ctl.p, r, p_min=ctl.p_min)
-    keep = LobpcgSvdKeep(n, n, r)
-    X = keep.S[:, :r]
-    W = keep.S[:, r:2 * r]
-    if X0 is None:
-        rng = np.random.default_rng(seed)
-        X0 = rng.random((n, r)) + 1j * rng.random((n, r))
-    X[:, :] = X0
-    sigma_recy = np.zeros(r)
-    ctl_main = LobpcgSvdControl(m=n, n=n, r=r, conv_range=(1, 1),
-                                tol=float(ctl.lobpcg_tol_scale * ctl.tol),
-                                side=ctl.lobpcg_side, normC=ctl.normC)
-    shift = complex(ctl.shift)
-    thresh = resolve_recycle_fail_dist_thresh(ctl.recycle_fail_dist_thresh, rec)
-    remaining = 0
-    nZ = len(rec.Z)
-    sigma_min = np.full(nZ, np.nan)
-    st = PsTriRecyStats.alloc(nZ)
-    last_failed = None
-    Rz = T.copy()
-    diagT = np.diag(T).copy()
-    for i in range(nZ):
-        z = complex(rec.Z[i])
-        st.p_count[i] = rs.p
-        r_svdrr = 0
-        m_apps = 0
-        r_apps = 0
-        recycled = False
-        if rs.p > 0:
+
+    def __init__(self, T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False):
+        n = T.shape[0]
+        self.ritz_g1_always = ritz_g1_always
+        r = ctl.r
+        self.T, self.rec, self.ctl, self.log = T, rec, ctl, log
+        self.M, self.S = TriOp(T), IdentityOp()
+        self.rs = RecycledSpace(n, n, ctl.p, r, p_min=ctl.p_min)
+        self.keep = LobpcgSvdKeep(n, n, r)
+        if X0 is None:
+            rng = np.random.default_rng(seed)
+            X0 = rng.random((n, r)) + 1j * rng.random((n, r))
+        self.keep.S[:, :r] = X0
+        self.sigma_recy = np.zeros(r)
+        self.ctl_main = LobpcgSvdControl(m=n, n=n, r=r, conv_range=(1, 1),
+                                         tol=float(ctl.lobpcg_tol_scale * ctl.tol),
+                                         side=ctl.lobpcg_side, normC=ctl.normC)
+        self.shift = complex(ctl.shift)
+        self.thresh = resolve_recycle_fail_dist_thresh(ctl.recycle_fail_dist_thresh, rec)
+        self.remaining = 0
+        nZ = len(rec.Z)
+        self.sigma_min = np.full(nZ, np.nan)
+        self.st = PsTriRecyStats.alloc(nZ)
+        self.last_failed = None
+        self.Rz = T.copy()
+        self.diagT = np.diag(T).copy()
+
+    def run(self, i_begin=0, i_end=None):
+        rec, ctl, rs, keep, st = self.rec, self.ctl, self.rs, self.keep, self.st
+        r = ctl.r
+        nZ = len(rec.Z)
+        i_end = nZ if i_end is None else i_end
+        X = keep.S[:, :r]
+        W = keep.S[:, r:2 * r]
+        for i in range(i_begin, i_end):
+            z = complex(rec.Z[i])
+            st.p_count[i] = rs.p
+            r_svdrr = 0
+            m_apps = 0
+            r_apps = 0
+            if rs.p > 0:
+                t0 = time.perf_counter_ns()
+                r_svdrr = fast_svd_rayl_ritz_implicit(rs, z, X, W, self.sigma_recy, self.shift,
+                                                      _gap_tau(ctl, self.remaining), self.ritz_g1_always)
+                self.remaining = self.remaining - 1 if self.remaining > 0 else 0
+                st.recycle_time_ns += time.perf_counter_ns() - t0
+                st.r_recy[i] = r_svdrr
+                if residual_norm_ok(W, self.sigma_recy[0], ctl.tol, ctl.normC):
+                    self.sigma_min[i] = self.sigma_recy[0]
+                    if self.log is not None:
+                        self.log(i, z, "recycled", rs.p, r_svdrr, self.sigma_min[i], 0)
+                    continue
             t0 = time.perf_counter_ns()
-            r_svdrr = fast_svd_rayl_ritz_implicit(rs, z, X, W, sigma_recy, shift,
-                                                  _gap_tau(ctl, remaining))
-            remaining = remaining - 1 if remaining > 0 else 0
-            st.recycle_time_ns += time.perf_counter_ns() - t0
-            st.r_recy[i] = r_svdrr
-            recycled = residual_norm_ok(W, sigma_recy[0], ctl.tol, ctl.normC)
-            if recycled:
-                sigma_min[i] = sigma_recy[0]
-                if log is not None:
-                    log(i, z, "recycled", rs.p, r_svdrr, sigma_min[i], 0)
-                continue
-        t0 = time.perf_counter_ns()
-        np.fill_diagonal(Rz, diagT - z)                       # get_R_factor! (psTriRecy.jl:87-99)
-        _, it = lobpcg_svd(InvAdjR(Rz), X, None, keep, ctl_main)
-        sigma_min[i] = keep.sigma[0]
-        st.refine_it[i] = it
-        if it > 0:
-            r_apps += 2 * r + it * r + (it - 1) * r
-        st.refine_time_ns += time.perf_counter_ns() - t0
-        st.n_it += it
-        st.pts[st.n_pts] = z
-        st.n_pts += 1
-        if i < nZ - 1 and it > 0:
-            t0 = time.perf_counter_ns()
-            force_add = last_failed is not None and abs(z - last_failed) <= thresh
-            update_recycled_space(M, S, z, rs, keep.S[:, :r], tau=ctl.recy_tau, r_sub=1,
-                                  force_add=force_add)
-            remaining = max(rec.k, 0) if force_add else 0
-            m_apps += 3 * r if ctl.implict_recycle else r
-            st.update_time_ns += time.perf_counter_ns() - t0
-        last_failed = z
-        st.M_vec_apps[i] = m_apps
-        st.M_vec_apps_no_recycle[i] = m_apps
-        st.R_vec_apps[i] = r_apps
-        if log is not None:
-            log(i, z, "refine", rs.p, r_svdrr, sigma_min[i], it)
-    return sigma_min, st
+            np.fill_diagonal(self.Rz, self.diagT - z)            # get_R_factor! (psTriRecy.jl:87-99)
+            _, it = lobpcg_svd(InvAdjR(self.Rz), X, None, keep, self.ctl_main)
+            self.sigma_min[i] = keep.sigma[0]
+            st.refine_it[i] = it
+            if it > 0:
+                r_apps += 2 * r + it * r + (it - 1) * r
+            st.refine_time_ns += time.perf_counter_ns() - t0
+            st.n_it += it
+            st.pts[st.n_pts] = z
+            st.n_pts += 1
+            if i < nZ - 1 and it > 0:
+                t0 = time.perf_counter_ns()
+                force_add = self.last_failed is not None and abs(z - self.last_failed) <= self.thresh
+                update_recycled_space(self.M, self.S, z, rs, keep.S[:, :r], tau=ctl.recy_tau, r_sub=1,
+                                      force_add=force_add)
+                self.remaining = max(rec.k, 0) if force_add else 0
+                m_apps += 3 * r if ctl.implict_recycle else r
+                st.update_time_ns += time.perf_counter_ns() - t0
+            self.last_failed = z
+            st.M_vec_apps[i] = m_apps
+            st.M_vec_apps_no_recycle[i] = m_apps
+            st.R_vec_apps[i] = r_apps
+            if self.log is not None:
+                self.log(i, z, "refine", rs.p, r_svdrr, self.sigma_min[i], it)
+        return self.sigma_min, st
+
+
+def ps_tri_recy_schur(T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False):
+    """_psTriRecy_impl (psTriRecy.jl:708-881) on a precomputed Schur factor T.
+    Returns (σ_min, stats)."""
+    return PsTriRecyRun(T, rec, ctl, X0=X0, seed=seed, log=log, ritz_g1_always=ritz_g1_always).run()
 
 
 def dense_sigma_min(C, z):

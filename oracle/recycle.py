@@ -219,8 +219,12 @@ def find_rr_dim(Hz, r, tau, n_init=None, n_max=-1):
     return n_max, G
 
 
-def fast_svd_rayl_ritz_implicit(rs: RecycledSpace, z, X_recy, W_recy, sigma_recy, shift, tau):
-    """_fastSvdRaylRitz_impl! implicit branch (fastRaylRitz.jl:99-219)."""
+def fast_svd_rayl_ritz_implicit(rs: RecycledSpace, z, X_recy, W_recy, sigma_recy, shift, tau, ritz_g1_always=False):
+    """_fastSvdRaylRitz_impl! implicit branch (fastRaylRitz.jl:99-219).
+
+    ``ritz_g1_always`` (not in the reference) forms G_total = G1·G2 also when
+    r_ == pr, where the reference takes G2 alone (fastRaylRitz.jl:199-202).
+    """
     p, r = rs.p, rs.r
     pr = p * r
     if pr == 0:
@@ -238,7 +242,7 @@ def fast_svd_rayl_ritz_implicit(rs: RecycledSpace, z, X_recy, W_recy, sigma_recy
     svd_inplace(R_.copy(), sig, G_, ascending=True)
     G2 = G_[:, :r]
     sigma_recy[:r] = sig[:r]
-    if r_ < pr:
+    if r_ < pr or ritz_g1_always:
         G_total = G1 @ G2
     else:
         G_total = G2.copy()   # fastRaylRitz.jl:199-202 uses G2 alone when r_ == pr

@@ -65,7 +65,14 @@ SIGNATURES = {
     "rls_set_schur": (C.c_int, [P, C.c_int64, P, C.c_int64]),
     "rls_pstrirecy_schur": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P, P,
                                       C.POINTER(rls_pstrirecy_stats)]),
+    "rls_pstrirecy_schur_range": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P,
+                                            C.c_int64, C.c_int64, P, C.POINTER(rls_pstrirecy_stats)]),
     "rls_lobpcg_svd_invtri": (C.c_int, [P, c64, P, C.POINTER(rls_lobpcg_control), P, P, P, P]),
+    "rls_ctx_stream": (C.c_void_p, [P]),
+    "rls_ctx_launches": (C.c_int64, [P]),
+    "rls_ctx_set_ritz_basis": (C.c_int, [P, C.c_int]),
+    "rls_ctx_set_profile": (C.c_int, [P, C.c_int]),
+    "rls_ctx_profile_get": (C.c_int, [P, C.c_int, P, P, P]),
     # kernel-level test entry points (include/rls_b200_testing.h)
     "rls_test_setup": (C.c_int, [P, C.c_int, C.c_int]),
     "rls_test_trsm": (C.c_int, [P, c64, C.c_int, C.c_int, P, P]),

@@ -65,7 +65,7 @@ __global__ void k_gram_reduce(int nchunks, int k1, int k2, const cplx* __restric
 // Row-streaming GEMM with an affine combination of up to 4 sources:
 //   Y = sum_q coef_q * A_q           (row by row, never materialised)
 //   C = alpha * Y * B + beta * C     (B: k1 × k2 small, k2 <= 32)
-// Optional second product X = A_xsrc * B (same B) and epilogue C -= X * diag(s2),
+// Optional second product X = A_xsrc * B (same B) and epilogue C -= X * diag(sig²),
 // plus per-CTA partial |C[:,0]|^2 sums.  One thread per row; a row of C is written
 // only after all reads of that row, so C may alias A_q when k1 == k2.
 // ------------------------------------------------------------------------------------
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(128) k_gemm_rows(int64_t nrows, CombSrc src, i
                                                    const cplx* __restrict__ B, int64_t ldb, int k2,
                                                    cplx alpha, cplx beta, cplx* C, int64_t ldc,
                                                    int xsrc, cplx* X, int64_t ldx,
-                                                   const double* __restrict__ s2,
+                                                   const double* __restrict__ sig,
                                                    double* __restrict__ col0_part) {
   extern __shared__ cplx sB[];  // KC × k2 chunk of B
   const int KC = 32;
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(128) k_gemm_rows(int64_t nrows, CombSrc src, i
         cplx out = cmul(alpha, acc[j]);
         if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + row], out);
         if (xsrc >= 0) {
-          if (s2) out = csub(out, cscale(accx[j], s2[j]));
+          if (sig) out = csub(out, cscale(accx[j], sig[j] * sig[j]));
           X[(int64_t)j * ldx + row] = accx[j];
         }
         C[(int64_t)j * ldc + row] = out;
@@ -181,6 +181,7 @@ __device__ __forceinline__ void tile_apply(const cplx* sT, const cplx* sX, int k
   }
 }
 
+template <int KMAX>
 __global__ void __launch_bounds__(256) k_trmm_partial(int nb, const cplx* __restrict__ T,
                                                       const cplx* __restrict__ X, int64_t ldx, int k,
                                                       int adj, const int* __restrict__ unit_O,
@@ -193,9 +194,9 @@ __global__ void __launch_bounds__(256) k_trmm_partial(int nb, const cplx* __rest
   const int u = blockIdx.x;
   const int O = unit_O[u], s0 = unit_s[u];
   const int row = threadIdx.x & (TILE - 1), grp = threadIdx.x >> 6;  // 4 groups split the inner dim
-  cplx acc[16];
+  cplx acc[KMAX];
 #pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c] = czero();
+  for (int c = 0; c < KMAX; ++c) acc[c] = czero();
   // Source tiles: adj=0: T(O, J), J = O + s0 .. ; adj=1: T(I, O), I = s0 ..
   const int nsrc = adj ? (O + 1) : (nb - O);
   const int s1 = min(nsrc, s0 + TRMM_UT);
@@ -210,10 +211,12 @@ __global__ void __launch_bounds__(256) k_trmm_partial(int nb, const cplx* __rest
       sX[c * TILE + rr] = X[(int64_t)c * ldx + (int64_t)xb * TILE + rr];
     }
     __syncthreads();
-    tile_apply<16>(sT, sX, k, adj, row, grp, acc);
+    tile_apply<KMAX>(sT, sX, k, adj, row, grp, acc);
   }
   __syncthreads();
-  for (int c = 0; c < k; ++c) sAcc[(grp * k + c) * TILE + row] = acc[c];
+#pragma unroll
+  for (int c = 0; c < KMAX; ++c)
+    if (c < k) sAcc[(grp * k + c) * TILE + row] = acc[c];
   __syncthreads();
   for (int t = threadIdx.x; t < TILE * k; t += blockDim.x) {
     const int rr = t % TILE, c = t / TILE;
@@ -298,6 +301,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+template <int KMAX>
 __global__ void __launch_bounds__(256) k_trsm_dataflow(int nb, const cplx* __restrict__ T,
                                                        const cplx* __restrict__ Dinv, const cplx* B,
                                                        cplx* X, int64_t ldx, int k, int adj,
@@ -337,11 +341,13 @@ __global__ void __launch_bounds__(256) k_trsm_dataflow(int nb, const cplx* __res
       sX[c * TILE + rr] = __ldcg(&X[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
     }
     __syncthreads();
-    cplx acc[24];
+    cplx acc[KMAX];
 #pragma unroll
-    for (int c = 0; c < 24; ++c) acc[c] = czero();
-    tile_apply<24>(sT, sX, k, adj, row, grp, acc);
-    for (int c = 0; c < k; ++c) sPart[(grp * k + c) * TILE + row] = acc[c];
+    for (int c = 0; c < KMAX; ++c) acc[c] = czero();
+    tile_apply<KMAX>(sT, sX, k, adj, row, grp, acc);
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c)
+      if (c < k) sPart[(grp * k + c) * TILE + row] = acc[c];
     __syncthreads();
     for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
       const int rr = q % TILE, c = q / TILE;
@@ -358,11 +364,13 @@ __global__ void __launch_bounds__(256) k_trsm_dataflow(int nb, const cplx* __res
   load_tile(sT, Dinv + (int64_t)b * TILE * TILE, adj);
   __syncthreads();
   {
-    cplx acc[24];
+    cplx acc[KMAX];
 #pragma unroll
-    for (int c = 0; c < 24; ++c) acc[c] = czero();
-    tile_apply<24>(sT, sAcc, k, adj, row, grp, acc);
-    for (int c = 0; c < k; ++c) sPart[(grp * k + c) * TILE + row] = acc[c];
+    for (int c = 0; c < KMAX; ++c) acc[c] = czero();
+    tile_apply<KMAX>(sT, sAcc, k, adj, row, grp, acc);
+#pragma unroll
+    for (int c = 0; c < KMAX; ++c)
+      if (c < k) sPart[(grp * k + c) * TILE + row] = acc[c];
   }
   __syncthreads();
   for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {

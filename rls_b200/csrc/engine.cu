@@ -97,6 +97,28 @@ struct rls_ctx {
   cplx *Gk = nullptr, *Rk = nullptr;  // 3r × 3r
   double *sig = nullptr, *lam = nullptr;
 
+  // psTriRecy run state carried across rls_pstrirecy_schur_range calls
+  struct {
+    bool active = false;
+    int64_t next = 0, nZ = 0;
+    int remaining = 0;
+    bool have_failed = false;
+    rls_c64 last_failed{0, 0};
+    double thresh = 0.0;
+  } run;
+
+  // optional per-kernel event timing (rls_ctx_set_profile)
+  bool profile = false;
+  int64_t launches = 0;            // kernel launches issued by this context
+  int ritz_g1_always = 1;          // r_ == pr: use G1·G2 (1) or the reference's G2 alone (0)
+  struct KProf {
+    std::vector<cudaEvent_t> ev;   // start/stop pairs not yet resolved
+    int64_t count = 0;
+    double ms = 0.0;
+    double bytes = 0.0;
+    std::vector<double> pending_bytes;
+  } kprof[4];
+
   std::vector<DevBuf> owned;
 };
 
@@ -154,6 +176,7 @@ void dfree(rls_ctx* ctx, void* p) {
 }
 
 int check_launch(rls_ctx* ctx, const char* what) {
+  ctx->launches += 1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_err(ctx, "launch of %s failed: %s", what, cudaGetErrorString(e));
@@ -162,8 +185,45 @@ int check_launch(rls_ctx* ctx, const char* what) {
   return RLS_OK;
 }
 
+enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3 };
+
+void prof_begin(rls_ctx* ctx, int id, cudaEvent_t* e0) {
+  if (!ctx->profile) return;
+  cudaEventCreate(e0);
+  cudaEventRecord(*e0, ctx->stream);
+}
+
+void prof_end(rls_ctx* ctx, int id, cudaEvent_t e0, double bytes) {
+  if (!ctx->profile) return;
+  cudaEvent_t e1;
+  cudaEventCreate(&e1);
+  cudaEventRecord(e1, ctx->stream);
+  ctx->kprof[id].ev.push_back(e0);
+  ctx->kprof[id].ev.push_back(e1);
+  ctx->kprof[id].pending_bytes.push_back(bytes);
+}
+
+// Resolves recorded event pairs (the stream must have passed them).
+void prof_resolve(rls_ctx* ctx) {
+  for (auto& k : ctx->kprof) {
+    for (size_t i = 0; i + 1 < k.ev.size(); i += 2) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, k.ev[i], k.ev[i + 1]) == cudaSuccess) {
+        k.ms += ms;
+        k.count += 1;
+        k.bytes += k.pending_bytes[i / 2];
+      }
+      cudaEventDestroy(k.ev[i]);
+      cudaEventDestroy(k.ev[i + 1]);
+    }
+    k.ev.clear();
+    k.pending_bytes.clear();
+  }
+}
+
 int sync_and_check(rls_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->profile) prof_resolve(ctx);
   int h = 0;
   CK(cudaMemcpy(&h, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
@@ -220,7 +280,7 @@ int gram(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k1, const 
 }
 
 // C = alpha (Σ coef_q A_q) B + beta C, optionally X = A_xsrc B and C -= X diag(sig²),
-// optional per-CTA |C[:,0]|² partials into ctx->colpart (returns the CTA count).
+// optional per-CTA |C[:,0]|² partials into ctx->colpart (returns the CTA count).  s2 holds σ (squared in the kernel).
 int gemm_rows(rls_ctx* ctx, int64_t nrows, CombSrc src, int64_t lda, int k1, const cplx* B, int64_t ldb, int k2,
               cplx* C, int64_t ldc, cplx alpha = cmk(1, 0), cplx beta = cmk(0, 0), int xsrc = -1,
               cplx* X = nullptr, int64_t ldx = 0, const double* s2 = nullptr, bool col0 = false,
@@ -425,20 +485,36 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
   }
   CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(int), ctx->stream));
   const size_t smem = ((size_t)TILE * TILE_LDS + 6 * (size_t)TILE * k) * sizeof(cplx);
-  k_trsm_dataflow<<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
-                                                       ctx->flags, ctx->epoch, ctx->derr);
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_TRSM, &e0);
+  if (k <= 8)
+    k_trsm_dataflow<8><<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
+                                                            ctx->flags, ctx->epoch, ctx->derr);
+  else
+    k_trsm_dataflow<24><<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
+                                                             ctx->flags, ctx->epoch, ctx->derr);
+  // algorithmic bytes: the upper triangle of T once (n²/2 complex) + B read + X written
+  prof_end(ctx, KP_TRSM, e0, 16.0 * ((double)ctx->n * (ctx->n + 1) / 2 + 2.0 * (double)ctx->n * k));
   return check_launch(ctx, "k_trsm_dataflow");
 }
 
 // Y = T X (adj=0) or Tᴴ X (adj=1); k <= 16.
 int trmm(rls_ctx* ctx, int adj, const cplx* X, cplx* Y, int64_t ld, int k) {
   const size_t smem = ((size_t)TILE * TILE_LDS + (size_t)TILE * k) * sizeof(cplx);
-  k_trmm_partial<<<ctx->trmm_units[adj], 256, smem, ctx->stream>>>(ctx->nb, ctx->T, X, ld, k, adj,
-                                                                   ctx->trmm_uO[adj], ctx->trmm_us[adj],
-                                                                   ctx->trmm_part);
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_TRMM, &e0);
+  if (k <= 8)
+    k_trmm_partial<8><<<ctx->trmm_units[adj], 256, smem, ctx->stream>>>(ctx->nb, ctx->T, X, ld, k, adj,
+                                                                        ctx->trmm_uO[adj], ctx->trmm_us[adj],
+                                                                        ctx->trmm_part);
+  else
+    k_trmm_partial<16><<<ctx->trmm_units[adj], 256, smem, ctx->stream>>>(ctx->nb, ctx->T, X, ld, k, adj,
+                                                                         ctx->trmm_uO[adj], ctx->trmm_us[adj],
+                                                                         ctx->trmm_part);
   RET(check_launch(ctx, "k_trmm_partial"));
   k_trmm_reduce<<<ctx->nb, 256, 0, ctx->stream>>>(ctx->nb, k, ctx->trmm_Ofirst[adj], ctx->trmm_Ocount[adj],
                                                   ctx->trmm_part, Y, ld);
+  prof_end(ctx, KP_TRMM, e0, 16.0 * ((double)ctx->n * (ctx->n + 1) / 2 + 2.0 * (double)ctx->n * k));
   return check_launch(ctx, "k_trmm_reduce");
 }
 
@@ -751,10 +827,14 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   CK(cudaMemcpyAsync(ctx->zdev, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->taudev, &gap_tau, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   const size_t smem = heev_smem_bytes(pr);
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_HEEV, &e0);
   k_heev_rr<<<1, HEEV_THREADS, smem, ctx->stream>>>(pr, r, ctx->H1, ctx->H2, ctx->pr_max, ctx->zdev, ctx->taudev,
                                                     shift, ctx->heev, ctx->pr_max, ctx->Gheev, ctx->pr_max,
                                                     (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev,
                                                     ctx->derr);
+  // algorithmic work of the reduction: (16/3)·pr³ real flops (reported as "bytes" slot = flops)
+  prof_end(ctx, KP_HEEV, e0, 16.0 / 3.0 * (double)pr * pr * pr);
   RET(check_launch(ctx, "k_heev_rr"));
   int rr = 0;
   RET(d2h(ctx, &rr, ctx->rr_dev, 1));
@@ -779,7 +859,7 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
     RET(check_launch(ctx, "k_svd_rr(recycle)"));
   }
   // G_total = G1 G2 (r_ < pr) or G2 (fastRaylRitz.jl:196-202)
-  if (rr < pr) {
+  if (rr < pr || ctx->ritz_g1_always) {
     RET(small_gemm(ctx, pr, r, rr, cmk(1, 0), ctx->Gheev, ctx->pr_max, 0, ctx->small[1], rr, 0, cmk(0, 0),
                    ctx->Gtot, pr));
   } else {
@@ -796,8 +876,12 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   cplx* X = ctx->S;
   cplx* W = ctx->S + np * r;
   int nparts = 0;
+  cudaEvent_t e0g = nullptr;
+  prof_begin(ctx, KP_RECYCLE_GEMM, &e0g);
   RET(gemm_rows(ctx, np, wsrc, np, pr, ctx->Gtot, pr, r, W, np, cmk(1, 0), cmk(0, 0), 3, X, np, ctx->sig_rec,
                 true, &nparts));
+  // algorithmic bytes: J1, J2, J5, V (n × pr each) read once, X and W written
+  prof_end(ctx, KP_RECYCLE_GEMM, e0g, 16.0 * ((double)ctx->n * pr * 4 + 2.0 * ctx->n * r));
   k_sum<<<1, 256, 0, ctx->stream>>>(ctx->colpart, nparts, ctx->dscal);
   RET(check_launch(ctx, "k_sum"));
   double w2 = 0.0, s0 = 0.0;
@@ -865,8 +949,10 @@ int allow_big_smem(rls_ctx* ctx, K kernel, int optin) {
 int set_kernel_attrs(rls_ctx* ctx) {
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  RET(allow_big_smem(ctx, k_trsm_dataflow, optin));
-  RET(allow_big_smem(ctx, k_trmm_partial, optin));
+  RET(allow_big_smem(ctx, k_trsm_dataflow<8>, optin));
+  RET(allow_big_smem(ctx, k_trsm_dataflow<24>, optin));
+  RET(allow_big_smem(ctx, k_trmm_partial<8>, optin));
+  RET(allow_big_smem(ctx, k_trmm_partial<16>, optin));
   RET(allow_big_smem(ctx, k_diag_inv, optin));
   RET(allow_big_smem(ctx, k_tsqr_leaf, optin));
   RET(allow_big_smem(ctx, k_heev_rr, optin));
@@ -1058,12 +1144,12 @@ extern "C" int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
   return RLS_OK;
 }
 
-extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
-                                   const rls_pstrirecy_control* ctl, const rls_c64* X0, double* sigma_min,
-                                   rls_pstrirecy_stats* st) {
+extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                                         const rls_pstrirecy_control* ctl, const rls_c64* X0, int64_t i_begin,
+                                         int64_t i_end, double* sigma_min, rls_pstrirecy_stats* st) {
   if (!ctx) return RLS_ERR_ARG;
-  if (!Z || !g || !ctl || !sigma_min || nZ < 0) {
-    set_err(ctx, "rls_pstrirecy_schur: null argument");
+  if (!Z || !g || !ctl || !sigma_min || nZ < 0 || i_begin < 0 || i_end < i_begin || i_end > nZ) {
+    set_err(ctx, "rls_pstrirecy_schur_range: invalid arguments");
     return RLS_ERR_ARG;
   }
   if (!ctx->T) {
@@ -1083,32 +1169,44 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
     set_err(ctx, "only implict_recycle=true, implict_update=false is implemented");
     return RLS_ERR_ARG;
   }
-  if (g->n_x < 2 || g->n_y < 2 || g->k < 1) return RLS_ERR_ARG;
-  CK(cudaSetDevice(ctx->device));
-  const int r = (int)ctl->r;
-  RET(setup_space(ctx, r, (int)ctl->p));
-  RET(upload_x0(ctx, X0, r));
-  // recycle_fail_dist_thresh (recySpace.jl:22-38)
-  double thresh = ctl->recycle_fail_dist_thresh;
-  if (!std::isfinite(thresh)) {
-    const double dx = std::fabs(g->x_ed - g->x_st) / (double)(g->n_x - 1);
-    const double dy = std::fabs(g->y_ed - g->y_st) / (double)(g->n_y - 1);
-    thresh = 1.01 * std::max(dx, dy);
-  } else if (thresh < 0) {
-    set_err(ctx, "recycle_fail_dist_thresh must be nonnegative, got %g", thresh);
+  if (g->n_x < 2 || g->n_y < 2 || g->k < 1) {
+    set_err(ctx, "invalid grid");
     return RLS_ERR_ARG;
   }
-  const double lob_tol = ctl->lobpcg_tol_scale * ctl->tol;
-  int remaining = 0;
-  bool have_failed = false;
-  rls_c64 last_failed{0, 0};
+  CK(cudaSetDevice(ctx->device));
+  const int r = (int)ctl->r;
+  auto& run = ctx->run;
   rls_pstrirecy_stats dummy{};
   if (!st) st = &dummy;
-  st->preprocess_time_ns = st->recycle_time_ns = st->qr_time_ns = st->refine_time_ns = st->update_time_ns = 0;
-  st->mv_stats_available = 1;
-  st->n_it = 0;
-  st->n_pts = 0;
-  for (int64_t i = 0; i < nZ; ++i) {
+  if (i_begin == 0) {
+    RET(setup_space(ctx, r, (int)ctl->p));
+    RET(upload_x0(ctx, X0, r));
+    // recycle_fail_dist_thresh (recySpace.jl:22-38)
+    double thresh = ctl->recycle_fail_dist_thresh;
+    if (!std::isfinite(thresh)) {
+      const double dx = std::fabs(g->x_ed - g->x_st) / (double)(g->n_x - 1);
+      const double dy = std::fabs(g->y_ed - g->y_st) / (double)(g->n_y - 1);
+      thresh = 1.01 * std::max(dx, dy);
+    } else if (thresh < 0) {
+      set_err(ctx, "recycle_fail_dist_thresh must be nonnegative, got %g", thresh);
+      return RLS_ERR_ARG;
+    }
+    run.active = true;
+    run.next = 0;
+    run.nZ = nZ;
+    run.remaining = 0;
+    run.have_failed = false;
+    run.thresh = thresh;
+    st->preprocess_time_ns = st->recycle_time_ns = st->qr_time_ns = st->refine_time_ns = st->update_time_ns = 0;
+    st->mv_stats_available = 1;
+    st->n_it = 0;
+    st->n_pts = 0;
+  } else if (!run.active || run.next != i_begin || run.nZ != nZ || ctx->r != r || ctx->p_max != (int)ctl->p) {
+    set_err(ctx, "range call does not continue the previous one (expected i_begin=%lld)", (long long)run.next);
+    return RLS_ERR_STATE;
+  }
+  const double lob_tol = ctl->lobpcg_tol_scale * ctl->tol;
+  for (int64_t i = i_begin; i < i_end; ++i) {
     const cplx z = cmk(Z[i].re, Z[i].im);
     if (st->p_count) st->p_count[i] = ctx->p;
     if (st->r_recy) st->r_recy[i] = 0;
@@ -1117,10 +1215,10 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
     int r_svdrr = 0;
     if (ctx->p > 0) {
       const uint64_t t0 = now_ns();
-      const double gtau = remaining > 0 ? ctl->gap_tau * ctl->gap_tau_scale : ctl->gap_tau;
+      const double gtau = run.remaining > 0 ? ctl->gap_tau * ctl->gap_tau_scale : ctl->gap_tau;
       RecycleResult rres{};
       RET(recycle_step(ctx, z, ctl->shift, gtau, &rres));
-      remaining = remaining > 0 ? remaining - 1 : 0;
+      run.remaining = run.remaining > 0 ? run.remaining - 1 : 0;
       st->recycle_time_ns += now_ns() - t0;
       r_svdrr = rres.rr;
       if (st->r_recy) st->r_recy[i] = r_svdrr;
@@ -1134,8 +1232,13 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
         if (ctx->verbose >= 1)
           emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
                    (long long)(i + 1), (long long)nZ, z.x, z.y, "recycled", ctx->p, r_svdrr, sigma_min[i]);
+        run.next = i + 1;
         continue;
       }
+      if (ctx->verbose >= 2)
+        emit_log(ctx, "  recycle rejected: |W[:,1]|=%.3e threshold=%.3e σ_recy=%.6e r_svdrr=%d pr=%d", rres.w0norm,
+                 ctl->normC * std::max(rres.sigma0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps), rres.sigma0,
+                 r_svdrr, ctx->p * r);
     }
     const uint64_t t1 = now_ns();
     LobpcgResult lres{};
@@ -1152,15 +1255,16 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
     st->n_pts += 1;
     if (i < nZ - 1 && it > 0) {
       const uint64_t t2 = now_ns();
-      const bool force_add = have_failed && std::hypot(z.x - last_failed.re, z.y - last_failed.im) <= thresh;
+      const bool force_add =
+          run.have_failed && std::hypot(z.x - run.last_failed.re, z.y - run.last_failed.im) <= run.thresh;
       RET(update_recycled_space(ctx, z, ctx->S, ctl->recy_tau, force_add, (int)ctl->p_min));
-      remaining = force_add ? (int)std::max<int64_t>(g->k, 0) : 0;
+      run.remaining = force_add ? (int)std::max<int64_t>(g->k, 0) : 0;
       m_apps += 3 * r;
       RET(sync_and_check(ctx));
       st->update_time_ns += now_ns() - t2;
     }
-    have_failed = true;
-    last_failed = Z[i];
+    run.have_failed = true;
+    run.last_failed = Z[i];
     if (st->M_vec_apps) st->M_vec_apps[i] = m_apps;
     if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = m_apps;
     if (st->R_vec_apps) st->R_vec_apps[i] = r_apps;
@@ -1170,8 +1274,48 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
       emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
                (long long)(i + 1), (long long)nZ, z.x, z.y, state, ctx->p, r_svdrr, sigma_min[i]);
     }
+    run.next = i + 1;
   }
+  if (i_end == nZ) run.active = false;
   return sync_and_check(ctx);
+}
+
+extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                                   const rls_pstrirecy_control* ctl, const rls_c64* X0, double* sigma_min,
+                                   rls_pstrirecy_stats* st) {
+  return rls_pstrirecy_schur_range(ctx, Z, nZ, g, ctl, X0, 0, nZ, sigma_min, st);
+}
+
+extern "C" void* rls_ctx_stream(rls_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" int64_t rls_ctx_launches(const rls_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always) {
+  if (!ctx) return RLS_ERR_ARG;
+  ctx->ritz_g1_always = g1_always != 0;
+  return RLS_OK;
+}
+
+extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
+  if (!ctx) return RLS_ERR_ARG;
+  RET(sync_and_check(ctx));
+  ctx->profile = on != 0;
+  for (auto& k : ctx->kprof) {
+    k.count = 0;
+    k.ms = 0.0;
+    k.bytes = 0.0;
+  }
+  return RLS_OK;
+}
+
+extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work) {
+  if (!ctx || kernel < 0 || kernel > 3) return RLS_ERR_ARG;
+  RET(sync_and_check(ctx));
+  prof_resolve(ctx);
+  if (count) *count = ctx->kprof[kernel].count;
+  if (total_ms) *total_ms = ctx->kprof[kernel].ms;
+  if (work) *work = ctx->kprof[kernel].bytes;
+  return RLS_OK;
 }
 
 #include "../../include/rls_b200_testing.h"

@@ -204,6 +204,51 @@ class Engine:
         st.mv_stats_available = bool(cst.mv_stats_available)
         return sigma, st
 
+    def stats_struct(self, st: "PsTriRecyStats"):
+        cst = rls_pstrirecy_stats()
+        i64 = C.POINTER(C.c_int64)
+        cst.p_count = st.p_count.ctypes.data_as(i64)
+        cst.r_recy = st.r_recy.ctypes.data_as(i64)
+        cst.pts = st.pts.ctypes.data_as(C.POINTER(c64))
+        cst.M_vec_apps = st.M_vec_apps.ctypes.data_as(i64)
+        cst.M_vec_apps_no_recycle = st.M_vec_apps_no_recycle.ctypes.data_as(i64)
+        cst.R_vec_apps = st.R_vec_apps.ctypes.data_as(i64)
+        cst.refine_it = st.refine_it.ctypes.data_as(i64)
+        return cst
+
+    def pstrirecy_range(self, rec: Recursion, control: PsTriRecyControl, i_begin: int, i_end: int, sigma, st,
+                        cst, X0=None):
+        """Continues (or, with i_begin == 0, starts) a psTriRecy run over rec.Z[i_begin:i_end];
+        sigma/st are the run's full-length outputs, cst the C view of st (stats_struct)."""
+        Z = rec.Z
+        x0 = None
+        if X0 is not None and i_begin == 0:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+            if x0.shape != (self.n, control.r):
+                raise DimensionMismatch(-2, f"X0 must be {(self.n, control.r)}, got {x0.shape}")
+        g = rec.c_grid()
+        cc = control.c_struct()
+        check(lib().rls_pstrirecy_schur_range(self._h, ptr(Z), len(Z), C.byref(g), C.byref(cc), ptr(x0), int(i_begin),
+                                              int(i_end), ptr(sigma), C.byref(cst)), self._h)
+        for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
+            setattr(st, f, int(getattr(cst, f)))
+
+    def stream_ptr(self) -> int:
+        return int(lib().rls_ctx_stream(self._h) or 0)
+
+    def launches(self) -> int:
+        return int(lib().rls_ctx_launches(self._h))
+
+    def set_profile(self, on: bool):
+        check(lib().rls_ctx_set_profile(self._h, int(on)), self._h)
+
+    def profile(self, kernel: int):
+        cnt = C.c_int64()
+        ms = C.c_double()
+        work = C.c_double()
+        check(lib().rls_ctx_profile_get(self._h, int(kernel), C.byref(cnt), C.byref(ms), C.byref(work)), self._h)
+        return cnt.value, ms.value, work.value
+
     def lobpcg_svd_invtri(self, z: complex, control: LobpcgSvdControl, X0=None):
         """lobpcgSvd(InvMat(adjoint(T − zI)), X0, I, keep, control) → (σ, it, X, σ_r)."""
         r = control.r
