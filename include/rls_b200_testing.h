@@ -28,9 +28,10 @@ int rls_test_qr(rls_ctx* ctx, int64_t m, int k, const rls_c64* A, rls_c64* R, rl
 int rls_test_svd_rr(rls_ctx* ctx, int nS, int r, int sideL, int lq, const rls_c64* R, double* sigma,
                     double* lam, rls_c64* G);
 /* find_rr_dim! on Hz = H1 − zH2 − z̄H2ᴴ + (|z|²+shift)I: Ritz dimension, eigenvalues
- * (entries not computed are 0) and G (pr × rr).  Compare ZHEEVR. */
+ * (entries not computed are 0) and G (pr × rr).  Compare ZHEEVR.  clk (6 values,
+ * may be NULL) receives the SM clock at the kernel's phase boundaries. */
 int rls_test_heev_rr(rls_ctx* ctx, int pr, int r, const rls_c64* H1, const rls_c64* H2, rls_c64 z,
-                     double shift, double tau, int* rr, double* lam, rls_c64* G);
+                     double shift, double tau, int* rr, double* lam, rls_c64* G, long long* clk);
 
 /* updateRecycledSpace! (recySpace.jl:160-223) with X (n × r) on the device space
  * (r_sub = 1).  Compare the CPU restatement. */

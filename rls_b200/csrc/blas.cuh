@@ -75,66 +75,74 @@ struct CombSrc {
   int nsrc;
 };
 
+// Tile of 32 rows per CTA; warp w of the 8 sums the inner index range
+// [w·kc, (w+1)·kc) for its lane's row, then the warps' partial sums are combined
+// through shared memory (8 × 32 × K2MAX cplx).  Rows are owned by one CTA and all
+// reads of a row precede the barrier before its writes, so C may alias a source.
 template <int K2MAX>
-__global__ void __launch_bounds__(128) k_gemm_rows(int64_t nrows, CombSrc src, int64_t lda, int k1,
+__global__ void __launch_bounds__(256) k_gemm_rows(int64_t nrows, CombSrc src, int64_t lda, int k1,
                                                    const cplx* __restrict__ B, int64_t ldb, int k2,
                                                    cplx alpha, cplx beta, cplx* C, int64_t ldc,
                                                    int xsrc, cplx* X, int64_t ldx,
                                                    const double* __restrict__ sig,
                                                    double* __restrict__ col0_part) {
-  extern __shared__ cplx sB[];  // KC × k2 chunk of B
-  const int KC = 32;
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ cplx red[];   // [2][8][K2MAX][32]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * 32 + lane;
+  const int kc = (k1 + 7) / 8;
+  const int kb = w * kc, ke = min(k1, kb + kc);
   cplx acc[K2MAX], accx[K2MAX];
 #pragma unroll
   for (int j = 0; j < K2MAX; ++j) { acc[j] = czero(); accx[j] = czero(); }
-  for (int kc = 0; kc < k1; kc += KC) {
-    const int kn = min(KC, k1 - kc);
-    __syncthreads();
-    for (int t = threadIdx.x; t < kn * k2; t += blockDim.x) {
-      const int kk = t % kn, j = t / kn;
-      sB[j * KC + kk] = B[(int64_t)j * ldb + kc + kk];
-    }
-    __syncthreads();
-    if (row < nrows) {
-      for (int kk = 0; kk < kn; ++kk) {
-        const int64_t off = (int64_t)(kc + kk) * lda + row;
-        cplx y = czero(), xv = czero();
-        for (int q = 0; q < src.nsrc; ++q) {
-          const cplx v = src.a[q][off];
-          y = cfma(src.coef[q], v, y);
-          if (q == xsrc) xv = v;
-        }
+  if (row < nrows) {
+    for (int kk = kb; kk < ke; ++kk) {
+      const int64_t off = (int64_t)kk * lda + row;
+      cplx y = czero(), xv = czero();
+      for (int q = 0; q < src.nsrc; ++q) {
+        const cplx v = src.a[q][off];
+        y = cfma(src.coef[q], v, y);
+        if (q == xsrc) xv = v;
+      }
 #pragma unroll
-        for (int j = 0; j < K2MAX; ++j) {
-          if (j < k2) {
-            const cplx b = sB[j * KC + kk];
-            acc[j] = cfma(y, b, acc[j]);
-            if (xsrc >= 0) accx[j] = cfma(xv, b, accx[j]);
-          }
+      for (int j = 0; j < K2MAX; ++j) {
+        if (j < k2) {
+          const cplx bb = __ldg(&B[(int64_t)j * ldb + kk]);
+          acc[j] = cfma(y, bb, acc[j]);
+          if (xsrc >= 0) accx[j] = cfma(xv, bb, accx[j]);
         }
       }
     }
   }
-  double c0 = 0.0;
-  if (row < nrows) {
 #pragma unroll
-    for (int j = 0; j < K2MAX; ++j) {
-      if (j < k2) {
-        cplx out = cmul(alpha, acc[j]);
-        if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + row], out);
-        if (xsrc >= 0) {
-          if (sig) out = csub(out, cscale(accx[j], sig[j] * sig[j]));
-          X[(int64_t)j * ldx + row] = accx[j];
-        }
-        C[(int64_t)j * ldc + row] = out;
-        if (j == 0) c0 = cabs2(out);
+  for (int j = 0; j < K2MAX; ++j) {
+    if (j < k2) {
+      red[((0 * 8 + w) * K2MAX + j) * 32 + lane] = acc[j];
+      if (xsrc >= 0) red[((1 * 8 + w) * K2MAX + j) * 32 + lane] = accx[j];
+    }
+  }
+  __syncthreads();
+  // thread (lane, w) finalises outputs j = w, w+8, ... of its lane's row
+  double c0 = 0.0;
+  for (int j = w; j < k2; j += 8) {
+    cplx sacc = czero(), sx = czero();
+    for (int q = 0; q < 8; ++q) {
+      sacc = cadd(sacc, red[((0 * 8 + q) * K2MAX + j) * 32 + lane]);
+      if (xsrc >= 0) sx = cadd(sx, red[((1 * 8 + q) * K2MAX + j) * 32 + lane]);
+    }
+    if (row < nrows) {
+      cplx out = cmul(alpha, sacc);
+      if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + row], out);
+      if (xsrc >= 0) {
+        if (sig) out = csub(out, cscale(sx, sig[j] * sig[j]));
+        X[(int64_t)j * ldx + row] = sx;
       }
+      C[(int64_t)j * ldc + row] = out;
+      if (j == 0) c0 = cabs2(out);
     }
   }
   if (col0_part) {
-    __shared__ double red[32];
-    const double s = block_sum(c0, red);
+    __shared__ double sred[32];
+    const double s = block_sum(c0, sred);
     if (threadIdx.x == 0) col0_part[blockIdx.x] = s;
   }
 }

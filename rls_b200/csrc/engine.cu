@@ -111,6 +111,7 @@ struct rls_ctx {
   bool profile = false;
   int64_t launches = 0;            // kernel launches issued by this context
   int ritz_g1_always = 1;          // r_ == pr: use G1·G2 (1) or the reference's G2 alone (0)
+  size_t heev_smem_avail = 0;      // dynamic shared memory k_heev_rr may use
   struct KProf {
     std::vector<cudaEvent_t> ev;   // start/stop pairs not yet resolved
     int64_t count = 0;
@@ -308,19 +309,18 @@ int gemm_rows(rls_ctx* ctx, int64_t nrows, CombSrc src, int64_t lda, int k1, con
                     C + (int64_t)j0 * ldc, ldc, alpha, beta));
     return RLS_OK;
   }
-  const int threads = 128;
-  const int blocks = (int)((nrows + threads - 1) / threads);
-  const size_t smem = 32 * (size_t)k2 * sizeof(cplx);
+  const int blocks = (int)((nrows + 31) / 32);
   double* cp = col0 ? ctx->colpart : nullptr;
+  const int nx = (xsrc >= 0) ? 2 : 1;
   if (k2 <= 8)
-    k_gemm_rows<8><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
-                                                           xsrc, X, ldx, s2, cp);
+    k_gemm_rows<8><<<blocks, 256, (size_t)nx * 8 * 8 * 32 * sizeof(cplx), ctx->stream>>>(
+        nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc, xsrc, X, ldx, s2, cp);
   else if (k2 <= 16)
-    k_gemm_rows<16><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
-                                                            xsrc, X, ldx, s2, cp);
+    k_gemm_rows<16><<<blocks, 256, (size_t)nx * 8 * 16 * 32 * sizeof(cplx), ctx->stream>>>(
+        nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc, xsrc, X, ldx, s2, cp);
   else
-    k_gemm_rows<32><<<blocks, threads, smem, ctx->stream>>>(nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc,
-                                                            xsrc, X, ldx, s2, cp);
+    k_gemm_rows<32><<<blocks, 256, (size_t)nx * 8 * 32 * 32 * sizeof(cplx), ctx->stream>>>(
+        nrows, src, lda, k1, B, ldb, k2, alpha, beta, C, ldc, xsrc, X, ldx, s2, cp);
   if (nparts) *nparts = blocks;
   return check_launch(ctx, "k_gemm_rows");
 }
@@ -347,7 +347,7 @@ int small_gemm(rls_ctx* ctx, int m, int n, int kk, cplx alpha, const cplx* A, in
 int tsqr_r(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k, cplx* R) {
   if (k <= 64) {
     // mb >= 2k guarantees every level shrinks the stack (m' = ceil(m/mb)·k < m for m > mb).
-    int mb = std::max(2 * k, std::min(1024, (int)(196608 / (k * (int)sizeof(cplx)))));
+    int mb = std::max(2 * k, std::min(256, (int)(196608 / (k * (int)sizeof(cplx)))));
     const cplx* src = A;
     int64_t m = nrows, ld = lda;
     int which = 0;
@@ -826,13 +826,14 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   const int64_t np = ctx->n_pad;
   CK(cudaMemcpyAsync(ctx->zdev, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->taudev, &gap_tau, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  const size_t smem = heev_smem_bytes(pr);
+  const HeevPlan plan = heev_plan(pr, ctx->heev_smem_avail);
+  const size_t smem = plan.bytes;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_HEEV, &e0);
   k_heev_rr<<<1, HEEV_THREADS, smem, ctx->stream>>>(pr, r, ctx->H1, ctx->H2, ctx->pr_max, ctx->zdev, ctx->taudev,
                                                     shift, ctx->heev, ctx->pr_max, ctx->Gheev, ctx->pr_max,
                                                     (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev,
-                                                    ctx->derr);
+                                                    ctx->derr, plan, nullptr);
   // algorithmic work of the reduction: (16/3)·pr³ real flops (reported as "bytes" slot = flops)
   prof_end(ctx, KP_HEEV, e0, 16.0 / 3.0 * (double)pr * pr * pr);
   RET(check_launch(ctx, "k_heev_rr"));
@@ -952,10 +953,18 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_trsm_dataflow<8>, optin));
   RET(allow_big_smem(ctx, k_trsm_dataflow<24>, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<8>, optin));
+  RET(allow_big_smem(ctx, k_gemm_rows<8>, optin));
+  RET(allow_big_smem(ctx, k_gemm_rows<16>, optin));
+  RET(allow_big_smem(ctx, k_gemm_rows<32>, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<16>, optin));
   RET(allow_big_smem(ctx, k_diag_inv, optin));
   RET(allow_big_smem(ctx, k_tsqr_leaf, optin));
   RET(allow_big_smem(ctx, k_heev_rr, optin));
+  {
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_heev_rr));
+    ctx->heev_smem_avail = (size_t)(optin - (int)fa.sharedSizeBytes);
+  }
   RET(allow_big_smem(ctx, k_svd_rr, optin));
   RET(allow_big_smem(ctx, k_blockrot_prep, optin));
   RET(allow_big_smem(ctx, k_chol_inv, optin));

@@ -19,8 +19,9 @@
 #include "common.cuh"
 #include "small.cuh"
 
+#include <algorithm>
+
 #define HEEV_THREADS 512
-#define HEEV_SMEM_PR 100   // full Hz kept in shared memory up to this order
 
 struct HeevWork {
   cplx* A;        // per problem pr_max*pr_max (global path)
@@ -60,7 +61,8 @@ __device__ double warp_eig_index(const double* d, const double* e2, int n, int i
 }
 
 // Partially pivoted LU of (T − λI) and solves, on lane 0 of a warp.
-// Storage (6 arrays of n): u0 (diag), u1, u2 (superdiagonals), l (multipliers), piv.
+// Storage (6 arrays of n): u0 (reciprocal pivots), u1, u2 (superdiagonals), l
+// (multipliers), piv.
 __device__ void tri_lu(const double* d, const double* e, int n, double lam, double* u0, double* u1, double* u2,
                        double* l, double* piv, double tiny) {
   double a = d[0] - lam;
@@ -70,21 +72,23 @@ __device__ void tri_lu(const double* d, const double* e, int n, double lam, doub
     const double an = d[i + 1] - lam;           // next diagonal
     const double bn = (i + 1 < n - 1) ? e[i + 1] : 0.0;
     if (fabs(a) >= fabs(c)) {
-      double aa = (a == 0.0) ? tiny : a;
-      const double m = c / aa;
+      const double aa = (a == 0.0) ? tiny : a;
+      const double ia = 1.0 / aa;
+      const double m = c * ia;
       piv[i] = 0.0; l[i] = m;
-      u0[i] = aa; u1[i] = b; u2[i] = 0.0;
+      u0[i] = ia; u1[i] = b; u2[i] = 0.0;
       a = an - m * b;
       b = bn;
     } else {
-      const double m = a / c;
+      const double ic = 1.0 / c;
+      const double m = a * ic;
       piv[i] = 1.0; l[i] = m;
-      u0[i] = c; u1[i] = an; u2[i] = bn;
+      u0[i] = ic; u1[i] = an; u2[i] = bn;
       a = b - m * an;
       b = -m * bn;
     }
   }
-  u0[n - 1] = (a == 0.0) ? tiny : a;
+  u0[n - 1] = 1.0 / ((a == 0.0) ? tiny : a);
 }
 
 __device__ void tri_solve(int n, const double* u0, const double* u1, const double* u2, const double* l,
@@ -93,10 +97,18 @@ __device__ void tri_solve(int n, const double* u0, const double* u1, const doubl
     if (piv[i] != 0.0) { const double t = x[i]; x[i] = x[i + 1]; x[i + 1] = t; }
     x[i + 1] -= l[i] * x[i];
   }
-  x[n - 1] /= u0[n - 1];                         // U⁻¹ (three bands)
-  if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) / u0[n - 2];
-  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) / u0[i];
+  x[n - 1] *= u0[n - 1];                         // U⁻¹ (three bands, reciprocal pivots)
+  if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) * u0[n - 2];
+  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) * u0[i];
 }
+
+// Shared-memory plan of one launch, computed on the host (heev_plan).
+struct HeevPlan {
+  int lda;      // leading dimension of Hz in shared memory (≡ 4 mod 8), 0: Hz in global scratch
+  int nlu;      // warps whose tridiagonal LU factors live in shared memory (0: global scratch)
+  int gs_cap;   // eigenvectors kept in shared memory (0: worked on in Gout directly)
+  size_t bytes; // dynamic shared memory
+};
 
 __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const cplx* __restrict__ H1,
                                                           const cplx* __restrict__ H2, int ldh,
@@ -104,34 +116,38 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
                                                           const double* __restrict__ taus, double shift,
                                                           HeevWork work, int prmax, cplx* Gout, int ldg,
                                                           int64_t gstride, int* rr_out, double* lam_out,
-                                                          int* err) {
+                                                          int* err, HeevPlan plan, long long* clk) {
   extern __shared__ double dsm[];
   const int b = blockIdx.x;
   const int n = pr;
-  const bool in_smem = (n <= HEEV_SMEM_PR);
-  // shared layout: [A (n*n cplx, optional)] v w (n cplx) d e e2 lam (n doubles) tau (n cplx)
-  cplx* A = in_smem ? reinterpret_cast<cplx*>(dsm) : work.A + (int64_t)b * prmax * prmax;
-  cplx* v = reinterpret_cast<cplx*>(dsm) + (in_smem ? n * n : 0);
+  const int nlu = plan.nlu;
+  // shared layout: [A (n × lda cplx)] v w tau (n cplx) d e e2 lam (n doubles) LU (nlu·6n doubles) S (gs_cap·n cplx)
+  cplx* base = reinterpret_cast<cplx*>(dsm);
+  const int lda = plan.lda > 0 ? plan.lda : n;
+  cplx* A = plan.lda > 0 ? base : work.A + (int64_t)b * prmax * prmax;
+  cplx* v = base + (plan.lda > 0 ? (size_t)n * lda : 0);
   cplx* w = v + n;
   cplx* tau = w + n;
   double* d = reinterpret_cast<double*>(tau + n);
   double* e = d + n;
   double* e2 = e + n;
   double* lam = e2 + n;
+  double* lusm = lam + n;
+  cplx* Ssm = reinterpret_cast<cplx*>(lusm + (size_t)nlu * 6 * n);
   __shared__ double red[32];
-  __shared__ cplx s_tau, s_scal, s_alpha2;
+  __shared__ cplx s_tau;
+  __shared__ cplx ypart[32];
   __shared__ int s_rr;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int lda = n;
   const cplx z = zs[b];
   const double zz = z.x * z.x + z.y * z.y + shift;
   cplx* G = Gout + (int64_t)b * gstride;
 
-  // 1. Hz from the upper triangle, mirrored.
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 0] = clock64();
+  // 1. Hz from the upper triangle, mirrored (affine_conbine!, element (ii, jj), ii <= jj).
   for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
     const int i = q % n, j = q / n;
     const int ii = min(i, j), jj = max(i, j);
-    // affine_conbine! element (ii, jj): H1 − z H2 − z̄ conj(H2[jj, ii]) + zz·δ
     cplx h = H1[(int64_t)jj * ldh + ii];
     h = cfms(z, H2[(int64_t)jj * ldh + ii], h);
     h = cfms(cconj(z), cconj(H2[(int64_t)ii * ldh + jj]), h);
@@ -141,57 +157,65 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   __syncthreads();
 
   // 2. Householder tridiagonalisation (lower form): for column k reduce A[k+1:, k].
+  //    Three barriers per column: warp 0 forms the reflector; groups of 4 threads
+  //    form y_i = τ Σ_j conj(A[j,i]) v_j (column i of the Hermitian trailing block)
+  //    with per-warp partials of yᴴv; all threads apply A −= v wᴴ + w vᴴ with
+  //    w = y + α₂·v, α₂ = −½ τ (yᴴv), formed on the fly.
   for (int k = 0; k < n - 1; ++k) {
     const int m0 = k + 1;
-    double x2 = 0.0;
-    for (int i = m0 + 1 + threadIdx.x; i < n; i += blockDim.x) x2 += cabs2(A[k * lda + i]);
-    x2 = block_sum(x2, red);
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
+      double x2 = 0.0;
+      for (int i = m0 + 1 + lane; i < n; i += 32) x2 += cabs2(A[k * lda + i]);
+      x2 = warp_sum(x2);
       double beta; cplx t, sc;
       householder_coeffs(A[k * lda + m0], x2, &beta, &t, &sc);
-      s_tau = t; s_scal = sc;
-      tau[k] = t;
-      e[k] = beta;
-      d[k] = A[k * lda + k].x;
+      for (int i = m0 + lane; i < n; i += 32) {
+        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : cmul(A[k * lda + i], sc);
+        v[i] = vi;
+        if (i > m0) A[k * lda + i] = vi;      // reflector tail kept for the back-transformation
+      }
+      if (lane == 0) {
+        s_tau = t;
+        tau[k] = t;
+        e[k] = beta;
+        d[k] = A[k * lda + k].x;
+      }
     }
     __syncthreads();
-    const cplx t = s_tau, sc = s_scal;
-    // v = [1; x*scal], stored in A[m0:, k] (A[m0, k] keeps 1 during the update)
-    for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) {
-      const cplx vi = (i == m0) ? cmk(1.0, 0.0) : cmul(A[k * lda + i], sc);
-      v[i] = vi;
-      if (i > m0) A[k * lda + i] = vi;
-    }
-    __syncthreads();
+    const cplx t = s_tau;
     if (t.x != 0.0 || t.y != 0.0) {
-      // y = tau * A[m0:, m0:] v  — row i via column i (Hermitian): y_i = Σ_j conj(A[j,i]) v_j
-      for (int i = m0 + warp; i < n; i += nw) {
-        cplx s = czero();
-        for (int j = m0 + lane; j < n; j += 32) s = cfmac(A[i * lda + j], v[j], s);
-        s = warp_sum(s);
-        if (lane == 0) w[i] = cmul(t, s);
-      }
-      __syncthreads();
-      // alpha2 = -1/2 tau (yᴴ v)
-      cplx yv = czero();
-      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) yv = cfmac(w[i], v[i], yv);
-      {
-        __shared__ cplx cred[32];
-        yv = block_sum(yv, cred);
-      }
-      if (threadIdx.x == 0) s_alpha2 = cscale(cmul(t, yv), -0.5);
-      __syncthreads();
-      const cplx a2 = s_alpha2;
-      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) w[i] = cfma(a2, v[i], w[i]);
-      __syncthreads();
-      // A -= v wᴴ + w vᴴ on the trailing block
       const int mm = n - m0;
+      const int nq = ((mm * 4 + 31) / 32) * 32;
+      cplx yv_part = czero();
+      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const bool valid = q < mm * 4;
+        const int i = m0 + q / 4, part = q & 3;
+        cplx sum = czero();
+        if (valid)
+          for (int j = m0 + part; j < n; j += 4) sum = cfmac(A[i * lda + j], v[j], sum);
+        sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
+        sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
+        sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 2);
+        sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 2);
+        if (valid && part == 0) {
+          const cplx yi = cmul(t, sum);
+          w[i] = yi;
+          yv_part = cfmac(yi, v[i], yv_part);  // Σ conj(y_i) v_i
+        }
+      }
+      yv_part = warp_sum(yv_part);
+      if (lane == 0) ypart[warp] = yv_part;
+      __syncthreads();
+      cplx yv = czero();
+      for (int q = 0; q < nw; ++q) yv = cadd(yv, ypart[q]);
+      const cplx a2 = cscale(cmul(t, yv), -0.5);
       for (int q = threadIdx.x; q < mm * mm; q += blockDim.x) {
         const int i = m0 + q % mm, j = m0 + q / mm;
-        cplx a = A[j * lda + i];
-        a = csub(a, cmul(v[i], cconj(w[j])));
-        a = csub(a, cmul(w[i], cconj(v[j])));
-        A[j * lda + i] = a;
+        const cplx wi = cfma(a2, v[i], w[i]), wj = cfma(a2, v[j], w[j]);
+        cplx aij = A[j * lda + i];
+        aij = csub(aij, cmul(v[i], cconj(wj)));
+        aij = csub(aij, cmul(wi, cconj(v[j])));
+        A[j * lda + i] = aij;
       }
       __syncthreads();
     }
@@ -220,21 +244,25 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   const double gl = s_gl, gu = s_gu, pivmin = s_piv;
   const double atol = 1e-14 * fmax(fabs(gl), fabs(gu));
 
-  // 3. λ_max and the smallest eigenvalues with the gap rule of find_rr_dim!.
-  if (warp == 0) {
-    const double lmax = warp_eig_index(d, e2, n, n - 1, gl, gu, pivmin, atol);
-    if (lane == 0) lam[n - 1] = lmax;
+  // 3. λ_max and the smallest eigenvalues with the gap rule of find_rr_dim!.  The last
+  //    warp computes λ_max while the others compute λ_0, λ_1, ... in the same pass.
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 1] = clock64();
+  {
+    const int idx = (warp == nw - 1) ? n - 1 : warp;
+    if (warp == nw - 1 || idx < n - 1) {
+      const double li = warp_eig_index(d, e2, n, idx, gl, gu, pivmin, atol);
+      if (lane == 0) lam[idx] = li;
+    }
   }
   __syncthreads();
   const double gap = lam[n - 1] / taus[b] * 2.220446049250313e-16;
   const int n_init = min(2 * r, n);
   int n_last = n_init;                      // largest n of the sequence 2r, 4r, ... <= n
   while (n_last + 2 * r <= n) n_last += 2 * r;
-  int computed = 0;                         // eigenvalues 0..computed-1 known
+  int computed = min(n - 1, nw - 1);        // eigenvalues 0..computed-1 known
   int rr = 0;
   int ncheck = n_init;
   while (true) {
-    // make sure λ_0 .. λ_{ncheck-1} are known (passes of nw eigenvalues)
     while (computed < ncheck) {
       const int idx = computed + warp;
       if (idx < ncheck && idx < n - 1) {
@@ -256,7 +284,6 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
     ncheck += 2 * r;
   }
   rr = (rr > 0) ? max(rr, r) : n;
-  // λ for all indices < rr (needed for the eigenvectors)
   while (computed < rr) {
     const int idx = computed + warp;
     if (idx < rr && idx < n - 1) {
@@ -267,92 +294,114 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
     __syncthreads();
   }
 
-  // 4. Inverse iteration, one warp per eigenvector; s_j (real) goes to G[:, j].
+  // 4. Inverse iteration, one warp per eigenvector, into S (shared when rr fits).
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 2] = clock64();
+  const bool s_shared = rr <= plan.gs_cap;
+  cplx* S = s_shared ? Ssm : G;
+  const int lds = s_shared ? n : ldg;
   {
     const double tnorm = fmax(fabs(gl), fabs(gu));
     const double tiny = 2.220446049250313e-16 * tnorm + 1e-300;
-    for (int j = warp; j < rr; j += nw) {
-      double* lu = work.lu + ((int64_t)b * 16 + warp) * 6 * prmax;
-      double *u0 = lu, *u1 = lu + prmax, *u2 = lu + 2 * prmax, *l = lu + 3 * prmax, *pv = lu + 4 * prmax,
-             *x = lu + 5 * prmax;
-      // shift perturbed slightly away from the computed eigenvalue so the factor is nonsingular
+    const int nwk = (nlu > 0) ? min(nlu, nw) : nw;
+    for (int j = warp; j < rr && warp < nwk; j += nwk) {
+      const int ldl = (nlu > 0) ? n : prmax;
+      double* lu = (nlu > 0) ? lusm + (int64_t)warp * 6 * n : work.lu + ((int64_t)b * 16 + warp) * 6 * prmax;
+      double *u0 = lu, *u1 = lu + ldl, *u2 = lu + 2 * ldl, *l = lu + 3 * ldl, *pv = lu + 4 * ldl,
+             *x = lu + 5 * ldl;
       const double lamj = lam[j] + tiny * ((j & 1) ? 1.0 : -1.0);
       if (lane == 0) tri_lu(d, e, n, lamj, u0, u1, u2, l, pv, tiny);
-      // deterministic start vector
-      for (int i = lane; i < n; i += 32) {
+      for (int i = lane; i < n; i += 32) {       // deterministic start vector
         uint32_t h = (uint32_t)(i * 2654435761u) ^ (uint32_t)((j + 1) * 2246822519u);
         h ^= h >> 15; h *= 2654435761u; h ^= h >> 13;
         x[i] = 0.5 + (double)(h & 0xffff) / 65536.0;
       }
       __syncwarp();
-      for (int it = 0; it < 3; ++it) {
+      for (int it = 0; it < 2; ++it) {
         if (lane == 0) tri_solve(n, u0, u1, u2, l, pv, x);
         __syncwarp();
-        double s = 0.0;
-        for (int i = lane; i < n; i += 32) s += x[i] * x[i];
-        s = warp_sum(s);
-        const double inv = (s > 0.0 && isfinite(s)) ? 1.0 / sqrt(s) : 0.0;
+        double ss = 0.0;
+        for (int i = lane; i < n; i += 32) ss += x[i] * x[i];
+        ss = warp_sum(ss);
+        const double inv = (ss > 0.0 && isfinite(ss)) ? 1.0 / sqrt(ss) : 0.0;
         for (int i = lane; i < n; i += 32) x[i] *= inv;
         __syncwarp();
       }
-      for (int i = lane; i < n; i += 32) G[(int64_t)j * ldg + i] = cmk(x[i], 0.0);
+      for (int i = lane; i < n; i += 32) S[(int64_t)j * lds + i] = cmk(x[i], 0.0);
     }
   }
   __syncthreads();
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 3] = clock64();
   // Block-wide classical Gram–Schmidt with one re-orthogonalisation (CGS2) over the rr
   // real vectors, in index order.  v (no longer needed) holds the coefficients.
   {
     double* coef = reinterpret_cast<double*>(v);
     __shared__ double s_nrm;
     for (int j = 0; j < rr; ++j) {
-      double* gj = reinterpret_cast<double*>(G + (int64_t)j * ldg);   // stride-2 real parts
+      double* gj = reinterpret_cast<double*>(S + (int64_t)j * lds);   // stride-2 real parts
       for (int pass = 0; pass < 2 && j > 0; ++pass) {
         for (int q = warp; q < j; q += nw) {
-          const double* gq = reinterpret_cast<const double*>(G + (int64_t)q * ldg);
-          double s = 0.0;
-          for (int i = lane; i < n; i += 32) s += gq[2 * i] * gj[2 * i];
-          s = warp_sum(s);
-          if (lane == 0) coef[q] = s;
+          const double* gq = reinterpret_cast<const double*>(S + (int64_t)q * lds);
+          double sq = 0.0;
+          for (int i = lane; i < n; i += 32) sq += gq[2 * i] * gj[2 * i];
+          sq = warp_sum(sq);
+          if (lane == 0) coef[q] = sq;
         }
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
           double acc = 0.0;
-          for (int q = 0; q < j; ++q) acc += coef[q] * reinterpret_cast<const double*>(G + (int64_t)q * ldg)[2 * i];
+          for (int q = 0; q < j; ++q) acc += coef[q] * reinterpret_cast<const double*>(S + (int64_t)q * lds)[2 * i];
           gj[2 * i] -= acc;
         }
         __syncthreads();
       }
-      double s = 0.0;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) s += gj[2 * i] * gj[2 * i];
-      s = block_sum(s, red);
-      if (threadIdx.x == 0) s_nrm = (s > 0.0) ? 1.0 / sqrt(s) : 0.0;
+      double sq = 0.0;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) sq += gj[2 * i] * gj[2 * i];
+      sq = block_sum(sq, red);
+      if (threadIdx.x == 0) s_nrm = (sq > 0.0) ? 1.0 / sqrt(sq) : 0.0;
       __syncthreads();
       const double inv = s_nrm;
       for (int i = threadIdx.x; i < n; i += blockDim.x) gj[2 * i] *= inv;
       __syncthreads();
     }
   }
-  // 5. Back-transformation G = H_0 H_1 ... H_{n-2} S: apply H_{n-2} first.
-  for (int k = n - 2; k >= 0; --k) {
-    const int m0 = k + 1;
-    const cplx t = tau[k];
-    if (t.x == 0.0 && t.y == 0.0) continue;
-    for (int j = warp; j < rr; j += nw) {
-      cplx s = czero();
-      for (int i = m0 + lane; i < n; i += 32) {
-        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
-        s = cfmac(vi, G[(int64_t)j * ldg + i], s);
-      }
-      s = warp_sum(s);
-      const cplx f = cmul(t, s);
-      for (int i = m0 + lane; i < n; i += 32) {
-        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
-        G[(int64_t)j * ldg + i] = cfms(vi, f, G[(int64_t)j * ldg + i]);
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 4] = clock64();
+  // 5. Back-transformation G = H_0 H_1 ... H_{n-2} S (apply H_{n-2} first).  A group of
+  //    16 lanes owns one vector: dot product, 4-level reduction, update, no barrier.
+  {
+    const int half = threadIdx.x >> 4, hl = threadIdx.x & 15, nh = blockDim.x >> 4;
+    for (int j0 = 0; j0 < rr; j0 += nh) {
+      const int j = j0 + half;
+      const bool act = j < rr;
+      cplx* sj = S + (int64_t)(act ? j : 0) * lds;
+      for (int k = n - 2; k >= 0; --k) {
+        const int m0 = k + 1;
+        const cplx t = tau[k];
+        if (t.x == 0.0 && t.y == 0.0) continue;
+        cplx sum = czero();
+        if (act)
+          for (int i = m0 + hl; i < n; i += 16) {
+            const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
+            sum = cfmac(vi, sj[i], sum);
+          }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+          sum.x += __shfl_xor_sync(0xffffffffu, sum.x, o);
+          sum.y += __shfl_xor_sync(0xffffffffu, sum.y, o);
+        }
+        const cplx f = cmul(t, sum);
+        if (act)
+          for (int i = m0 + hl; i < n; i += 16) {
+            const cplx vi = (i == m0) ? cmk(1.0, 0.0) : A[k * lda + i];
+            sj[i] = cfms(vi, f, sj[i]);
+          }
+        __syncwarp();
       }
     }
-    // no barrier needed: each warp owns its columns and A is read-only here
   }
   __syncthreads();
+  if (s_shared)
+    for (int q = threadIdx.x; q < rr * n; q += blockDim.x) G[(int64_t)(q / n) * ldg + (q % n)] = S[q];
+  if (clk && threadIdx.x == 0) clk[(int64_t)b * 8 + 5] = clock64();
   if (threadIdx.x == 0) {
     rr_out[b] = rr;
     bool bad = !isfinite(lam[n - 1]);
@@ -365,8 +414,26 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   }
 }
 
-inline size_t heev_smem_bytes(int pr) {
-  size_t s = (size_t)3 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
-  if (pr <= HEEV_SMEM_PR) s += (size_t)pr * pr * sizeof(cplx);
-  return s;
+// Shared-memory plan for order pr within `avail` bytes: Hz in shared memory when it
+// fits next to the vectors, then up to 8 LU warps, then as many eigenvectors (<= 32)
+// as fit.
+inline HeevPlan heev_plan(int pr, size_t avail) {
+  HeevPlan p{};
+  const size_t vec = (size_t)3 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
+  int lda = pr + ((4 - pr % 8) + 8) % 8;                    // ≡ 4 (mod 8)
+  size_t need = vec + (size_t)pr * lda * sizeof(cplx);
+  const size_t lu1 = (size_t)6 * pr * sizeof(double);
+  const size_t s1 = (size_t)pr * sizeof(cplx);
+  if (need + 2 * lu1 + 6 * s1 <= avail) {
+    p.lda = lda;
+  } else {
+    p.lda = 0;
+    need = vec;
+  }
+  p.nlu = (int)std::min<size_t>(8, (avail - need) / lu1);
+  need += (size_t)p.nlu * lu1;
+  p.gs_cap = (int)std::min<size_t>(32, (avail - need) / s1);
+  need += (size_t)p.gs_cap * s1;
+  p.bytes = need;
+  return p;
 }

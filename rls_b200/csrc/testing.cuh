@@ -120,7 +120,7 @@ extern "C" int rls_test_svd_rr(rls_ctx* ctx, int nS, int r, int sideL, int lq, c
 
 // find_rr_dim on Hz built from H1, H2 (pr×pr, column-major); G gets pr × rr.
 extern "C" int rls_test_heev_rr(rls_ctx* ctx, int pr, int r, const rls_c64* H1, const rls_c64* H2, rls_c64 z,
-                                double shift, double tau, int* rr, double* lam, rls_c64* G) {
+                                double shift, double tau, int* rr, double* lam, rls_c64* G, long long* clk) {
   RET(need_space(ctx));
   if (pr < 1 || pr > ctx->pr_max || r < 1 || !H1 || !H2 || !rr || !G) return RLS_ERR_ARG;
   DevTmp t(ctx);
@@ -132,14 +132,17 @@ extern "C" int rls_test_heev_rr(rls_ctx* ctx, int pr, int r, const rls_c64* H1, 
   cplx zz = cmk(z.re, z.im);
   CK(cudaMemcpyAsync(ctx->zdev, &zz, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->taudev, &tau, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  k_heev_rr<<<1, HEEV_THREADS, heev_smem_bytes(pr), ctx->stream>>>(
+  const HeevPlan plan = heev_plan(pr, ctx->heev_smem_avail);
+  long long* dclk = clk ? t.alloc<long long>(8) : nullptr;
+  k_heev_rr<<<1, HEEV_THREADS, plan.bytes, ctx->stream>>>(
       pr, r, d1, d2, pr, ctx->zdev, ctx->taudev, shift, ctx->heev, ctx->pr_max, ctx->Gheev, ctx->pr_max,
-      (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev, ctx->derr);
+      (int64_t)ctx->pr_max * ctx->pr_max, ctx->rr_dev, ctx->lam_dev, ctx->derr, plan, dclk);
   RET(check_launch(ctx, "k_heev_rr"));
   RET(d2h(ctx, rr, ctx->rr_dev, 1));
   if (lam) CK(cudaMemcpyAsync(lam, ctx->lam_dev, sizeof(double) * pr, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpy2DAsync(G, pr * sizeof(cplx), ctx->Gheev, ctx->pr_max * sizeof(cplx), pr * sizeof(cplx), *rr,
                        cudaMemcpyDeviceToHost, ctx->stream));
+  if (clk) CK(cudaMemcpyAsync(clk, dclk, sizeof(long long) * 6, cudaMemcpyDeviceToHost, ctx->stream));
   return sync_and_check(ctx);
 }
 

@@ -134,8 +134,12 @@ def test_heev_rr_matches_zheevr(eng_T, pr, r, tau):
     rr = C.c_int(0)
     lam = np.zeros(pr)
     G = np.zeros((pr, pr), dtype=np.complex128, order="F")
+    clk = np.zeros(6, dtype=np.int64)
     check(lib().rls_test_heev_rr(e._h, pr, r, ptr(H1), ptr(H2), c64(z.real, z.imag), shift, tau, C.byref(rr),
-                                 ptr(lam), ptr(G)), e._h)
+                                 ptr(lam), ptr(G), ptr(clk)), e._h)
+    ph = np.diff(clk)
+    print(f"heev pr={pr}: cycles build+tridiag {ph[0]}, eigenvalues {ph[1]}, inverse iteration {ph[2]}, "
+          f"orthogonalisation {ph[3]}, back-transform {ph[4]}")
     Hz = affine_combine(z, H1, H2, H2.conj().T, np.eye(pr), shift=shift)
     Hz = np.triu(Hz) + np.triu(Hz, 1).conj().T
     Hz[np.diag_indices(pr)] = Hz.diagonal().real

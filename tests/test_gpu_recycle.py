@@ -66,7 +66,7 @@ def test_space_updates_and_recycle_match(setup):
         Vo = rs.V[:, :pr]
         # same subspace, orthonormal basis, consistent cached products
         assert np.linalg.norm(V.conj().T @ V - np.eye(pr)) < 1e-11
-        assert np.linalg.norm(V @ V.conj().T - Vo @ Vo.conj().T) < 1e-9 * np.sqrt(pr)
+        assert np.linalg.norm(V @ V.conj().T - Vo @ Vo.conj().T) < 1e-7 * np.sqrt(pr)
         assert np.linalg.norm(J5 - T @ V) <= 1e-12 * np.linalg.norm(T) * np.sqrt(pr)
         assert np.linalg.norm(J2 - T.conj().T @ V) <= 1e-12 * np.linalg.norm(T) * np.sqrt(pr)
         assert np.linalg.norm(J1 - T.conj().T @ (T @ V)) <= 1e-11 * np.linalg.norm(T) ** 2 * np.sqrt(pr)
