@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=1, help="steps timed on the unbatched per-point path")
+    ap.add_argument("--ncu-window", default=None,
+                    help="WARM,COUNT: run WARM points, then COUNT points inside cudaProfilerStart/Stop, and exit "
+                         "(for ncu --profile-from-start off); no timing output")
     return ap.parse_args()
 
 
@@ -233,6 +237,27 @@ def run_ours(args):
     if need > len(sub.Z):
         raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds the {len(sub.Z)} points of this rank")
 
+    # plain per-point drop-in (no speculative batching) on one step, for comparison
+    plain = None
+    if args.plain_steps > 0:
+        engp = Engine(local)
+        engp.set_batch(1)
+        engp.set_schur(T)
+        sigp = np.full(len(sub.Z), np.nan)
+        stp = PsTriRecyStats.alloc(len(sub.Z))
+        cstp = engp.stats_struct(stp)
+        for w in range(args.warmup):
+            engp.pstrirecy_range(sub, ctl, w * s, (w + 1) * s, sigp, stp, cstp, X0=X0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.plain_steps):
+            a = (args.warmup + k) * s
+            engp.pstrirecy_range(sub, ctl, a, a + s, sigp, stp, cstp)
+        torch.cuda.synchronize()
+        plain = {"value": args.plain_steps * s / (time.perf_counter() - t0), "unit": "pts/s",
+                 "steps": args.plain_steps, "mode": "one recycle step per launch sequence (set_batch(1))"}
+        engp.close()
+
     eng = Engine(local)
     eng.set_schur(T)
     sigma = np.full(len(sub.Z), np.nan)
@@ -337,6 +362,11 @@ def run_ours(args):
                                            args.cpu_sample_s)
     if e2e is not None:
         out["e2e"] = e2e
+    if plain is not None:
+        out["plain_per_point"] = plain
+        same = np.allclose(sigp[timed.start:timed.start + args.plain_steps * s],
+                           sigma[timed.start:timed.start + args.plain_steps * s], rtol=0, atol=1e-10)
+        out["plain_per_point"]["matches_batched"] = bool(same)
     if rank == 0:
         print(json.dumps(out), flush=True)
     eng.close()
@@ -344,8 +374,36 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ncu_window(args):
+    import torch
+    import rls_b200 as R
+    from rls_b200.solvers import Engine, PsTriRecyControl, PsTriRecyStats
+    warm, count = (int(x) for x in args.ncu_window.split(","))
+    _, T, _ = build_inputs(args.n)
+    rec = R.recursion_grid(*GRID)
+    ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
+    rng = np.random.default_rng(1)
+    X0 = rng.random((args.n, 6)) + 1j * rng.random((args.n, 6))
+    eng = Engine(0)
+    eng.set_schur(T)
+    sig = np.full(len(rec.Z), np.nan)
+    st = PsTriRecyStats.alloc(len(rec.Z))
+    cst = eng.stats_struct(st)
+    eng.pstrirecy_range(rec, ctl, 0, warm, sig, st, cst, X0=X0)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    eng.pstrirecy_range(rec, ctl, warm, warm + count, sig, st, cst)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(f"profiled points {warm}..{warm + count - 1}: {int(np.sum(st.refine_it[warm:warm + count] > 0))} refines",
+          flush=True)
+
+
 def main():
     args = parse()
+    if args.ncu_window:
+        run_ncu_window(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -118,6 +118,13 @@ int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verbose);
 void* rls_ctx_stream(rls_ctx* ctx);
 /* Number of kernel launches this context has issued so far.  No reference counterpart. */
 int64_t rls_ctx_launches(const rls_ctx* ctx);
+/* Speculative batching of recycle steps: up to max_points consecutive grid points
+ * (1..32) run their recycle step together against the current recycled space;
+ * points up to the first rejection are accepted exactly as the sequential loop
+ * would accept them (an accepted point does not change the space), the first
+ * rejected point is refined from its own recycle output.  1 = one point at a time
+ * (the plain per-point drop-in).  Default 16.  No reference counterpart. */
+int rls_ctx_set_batch(rls_ctx* ctx, int max_points);
 /* Ritz basis of the recycle step when the Ritz dimension equals the space size
  * (r_ == p·r): 1 (default) forms X = V·G1·G2 as for r_ < p·r; 0 keeps the
  * reference's X = V·G2 (fastRaylRitz.jl:199-202), whose result depends on the

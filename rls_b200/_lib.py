@@ -71,6 +71,7 @@ SIGNATURES = {
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_ctx_launches": (C.c_int64, [P]),
     "rls_ctx_set_ritz_basis": (C.c_int, [P, C.c_int]),
+    "rls_ctx_set_batch": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_profile": (C.c_int, [P, C.c_int]),
     "rls_ctx_profile_get": (C.c_int, [P, C.c_int, P, P, P]),
     # kernel-level test entry points (include/rls_b200_testing.h)

@@ -17,9 +17,10 @@ __host__ __device__ __forceinline__ int64_t tile_index(int I, int J) {
 }
 
 // ------------------------------------------------------------------------------------
-// Gram: C (k1×k2) = alpha·AᴴB + beta·C.  Phase 1: grid (chunks, ceil(k1/8)); warp w
-// owns column (blockIdx.y*8+w) of A and sums over the chunk's rows; k2 <= 32.
+// Gram: C (k1×k2) = alpha·AᴴB + beta·C.  Phase 1: grid (row chunks, ceil(k1/8)); warp w
+// owns column (blockIdx.y*8+w) of A and sums over the chunk's rows; k2 <= K2MAX.
 // ------------------------------------------------------------------------------------
+template <int K2MAX>
 __global__ void __launch_bounds__(256) k_gram_partial(int64_t nrows, int64_t chunk,
                                                       const cplx* __restrict__ A, int64_t lda, int k1,
                                                       const cplx* __restrict__ B, int64_t ldb, int k2,
@@ -28,20 +29,20 @@ __global__ void __launch_bounds__(256) k_gram_partial(int64_t nrows, int64_t chu
   const int col = blockIdx.y * 8 + w;
   const int64_t r0 = (int64_t)blockIdx.x * chunk;
   const int64_t r1 = min(nrows, r0 + chunk);
-  cplx acc[32];
+  cplx acc[K2MAX];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) acc[j] = czero();
+  for (int j = 0; j < K2MAX; ++j) acc[j] = czero();
   if (col < k1) {
     const cplx* a = A + (int64_t)col * lda;
     for (int64_t row = r0 + lane; row < r1; row += 32) {
       const cplx av = a[row];
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
+      for (int j = 0; j < K2MAX; ++j)
         if (j < k2) acc[j] = cfmac(av, __ldg(&B[(int64_t)j * ldb + row]), acc[j]);
     }
   }
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
+  for (int j = 0; j < K2MAX; ++j) {
     if (j < k2) {
       cplx s = warp_sum(acc[j]);
       if (lane == 0 && col < k1) part[((int64_t)blockIdx.x * k1 + col) * k2 + j] = s;
@@ -168,19 +169,21 @@ __device__ __forceinline__ void load_tile(cplx* sT, const cplx* __restrict__ tp,
   }
 }
 
-// acc[c] += (adj ? Tᴴ : T)[row, inner-range] · sX[inner-range, c], inner range of group grp.
-template <int KMAX>
+// acc[c] += (adj ? Tᴴ : T)[row, inner-range] · sX[inner-range, c]; the inner dimension is
+// split into NG ranges of TILE/NG, range `grp` here.
+template <int KMAX, int NG = 4>
 __device__ __forceinline__ void tile_apply(const cplx* sT, const cplx* sX, int k, int adj, int row, int grp,
                                            cplx* acc) {
+  constexpr int W = TILE / NG;
   if (!adj) {
-    for (int jj = grp * 16; jj < grp * 16 + 16; ++jj) {
+    for (int jj = grp * W; jj < grp * W + W; ++jj) {
       const cplx tv = sT[jj * TILE_LDS + row];
 #pragma unroll
       for (int c = 0; c < KMAX; ++c)
         if (c < k) acc[c] = cfma(tv, sX[c * TILE + jj], acc[c]);
     }
   } else {
-    for (int ii = grp * 16; ii < grp * 16 + 16; ++ii) {
+    for (int ii = grp * W; ii < grp * W + W; ++ii) {
       const cplx tv = sT[ii * TILE_LDS + row];   // T[ii, row]
 #pragma unroll
       for (int c = 0; c < KMAX; ++c)
@@ -290,6 +293,36 @@ __global__ void __launch_bounds__(256) k_diag_inv(int nb, int64_t n, const cplx*
   if (bad) atomicOr(err, DEVERR_NONFINITE);
 }
 
+// E tiles for the last step of the dataflow solve, per shift:
+//   adj = 0: E_b = D_b⁻¹ T(b, b+1)        (b < nb-1)
+//   adj = 1: E_b = D_b⁻ᴴ T(b-1, b)ᴴ       (b > 0)
+// so that X_b = D_b⁻¹ acc − E_b X_{b±1} needs one tile product after the last wait.
+// grid (nb, 2); one CTA computes one 64×64×64 complex product from shared memory.
+__global__ void __launch_bounds__(256) k_trsm_etiles(int nb, const cplx* __restrict__ T,
+                                                     const cplx* __restrict__ Dinv, cplx* __restrict__ E) {
+  extern __shared__ cplx sm[];
+  cplx* sD = sm;                  // TILE*TILE (column-major)
+  cplx* sT = sm + TILE * TILE;    // TILE*TILE
+  const int b = blockIdx.x, adj = blockIdx.y;
+  cplx* out = E + ((int64_t)adj * nb + b) * TILE * TILE;
+  if ((!adj && b == nb - 1) || (adj && b == 0)) return;
+  const cplx* dp = Dinv + (int64_t)b * TILE * TILE;
+  const cplx* tp = adj ? T + tile_index(b - 1, b) * (TILE * TILE) : T + tile_index(b, b + 1) * (TILE * TILE);
+  for (int q = threadIdx.x; q < TILE * TILE; q += blockDim.x) { sD[q] = dp[q]; sT[q] = tp[q]; }
+  __syncthreads();
+  // thread: row i = tid % 64, columns c = tid/64 + 4·m
+  const int i = threadIdx.x & 63, c0 = threadIdx.x >> 6;
+  for (int c = c0; c < TILE; c += 4) {
+    cplx s = czero();
+    if (!adj) {
+      for (int l = 0; l < TILE; ++l) s = cfma(sD[l * TILE + i], sT[c * TILE + l], s);          // D⁻¹[i,l]·T[l,c]
+    } else {
+      for (int l = 0; l < TILE; ++l) s = cfma(cconj(sD[i * TILE + l]), cconj(sT[l * TILE + c]), s);  // D⁻ᴴ[i,l]·Tᴴ[l,c]
+    }
+    out[c * TILE + i] = s;
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Dataflow triangular solve with the shifted Schur factor R = T − zI.
 //   adj = 0: R X = B   (back substitution, tiles of block row I, J > I)
@@ -309,89 +342,116 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-template <int KMAX>
-__global__ void __launch_bounds__(256) k_trsm_dataflow(int nb, const cplx* __restrict__ T,
-                                                       const cplx* __restrict__ Dinv, const cplx* B,
-                                                       cplx* X, int64_t ldx, int k, int adj,
-                                                       int* __restrict__ ticket, int* flags, int epoch,
-                                                       int* err) {
+// Shared memory: 2·TILE·TILE_LDS (tile, diagonal inverse) + (2 + NG)·TILE·k cplx.
+// All dependencies but the last are subtracted from the right-hand side as they
+// arrive; y = D_b⁻¹·acc is then formed before waiting for the last one, which enters
+// through the precomputed E_b (k_trsm_etiles): X_b = y − E_b·X_last.  E_b is stored
+// like a tile of T with adj = 0 semantics, so it is loaded untransposed.
+template <int KMAX, int NG>
+__global__ void __launch_bounds__(64 * NG) k_trsm_dataflow(int nb, const cplx* __restrict__ T,
+                                                          const cplx* __restrict__ Dinv,
+                                                          const cplx* __restrict__ E, const cplx* B,
+                                                          cplx* X, int64_t ldx, int k, int adj,
+                                                          int* __restrict__ ticket, int* flags, int epoch,
+                                                          int* err) {
   extern __shared__ cplx sm[];
   cplx* sT = sm;                         // TILE*TILE_LDS
-  cplx* sX = sT + TILE * TILE_LDS;       // TILE*k (dependency block)
+  cplx* sD = sT + TILE * TILE_LDS;       // TILE*TILE_LDS: this block's diagonal inverse
+  cplx* sX = sD + TILE * TILE_LDS;       // TILE*k (dependency block)
   cplx* sAcc = sX + TILE * k;            // TILE*k (running right-hand side)
-  cplx* sPart = sAcc + TILE * k;         // 4 × TILE*k partial products
+  cplx* sPart = sAcc + TILE * k;         // NG × TILE*k partial products
   __shared__ int sblk;
   if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
   __syncthreads();
   const int t = sblk;
   const int b = adj ? t : (nb - 1 - t);
   const int row = threadIdx.x & (TILE - 1), grp = threadIdx.x >> 6;
+  load_tile(sD, Dinv + (int64_t)b * TILE * TILE, adj);
   for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
     const int rr = q % TILE, c = q / TILE;
     sAcc[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
   }
-  const int ndep = adj ? b : (nb - 1 - b);
-  for (int d = 0; d < ndep; ++d) {
-    const int dep = adj ? d : (nb - 1 - d);
-    const cplx* tp = adj ? T + tile_index(dep, b) * (TILE * TILE) : T + tile_index(b, dep) * (TILE * TILE);
-    __syncthreads();
-    load_tile(sT, tp, adj);   // independent of X: issued before the wait
+  auto wait_flag = [&](int dep) {
     if (threadIdx.x == 0) {
       int spins = 0;
       while (ld_acquire(&flags[dep]) != epoch) {
         if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
-        __nanosleep(64);
+        if (spins > 64) __nanosleep(32);
       }
     }
     __syncthreads();
+  };
+  auto load_x = [&](int dep) {
     for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
       const int rr = q % TILE, c = q / TILE;
       sX[c * TILE + rr] = __ldcg(&X[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
     }
     __syncthreads();
+  };
+  // sPart ← products of the tile in `tile` (op per `op_adj`) with `vec`
+  auto product = [&](const cplx* tile, const cplx* vec, int op_adj) {
     cplx acc[KMAX];
 #pragma unroll
     for (int c = 0; c < KMAX; ++c) acc[c] = czero();
-    tile_apply<KMAX>(sT, sX, k, adj, row, grp, acc);
+    tile_apply<KMAX, NG>(tile, vec, k, op_adj, row, grp, acc);
 #pragma unroll
     for (int c = 0; c < KMAX; ++c)
       if (c < k) sPart[(grp * k + c) * TILE + row] = acc[c];
     __syncthreads();
+  };
+  const int ndep = adj ? b : (nb - 1 - b);
+  for (int d = 0; d + 1 < ndep; ++d) {
+    const int dep = adj ? d : (nb - 1 - d);
+    const cplx* tp = adj ? T + tile_index(dep, b) * (TILE * TILE) : T + tile_index(b, dep) * (TILE * TILE);
+    __syncthreads();
+    load_tile(sT, tp, adj);   // independent of X: issued before the wait
+    wait_flag(dep);
+    load_x(dep);
+    product(sT, sX, adj);
     for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
       const int rr = q % TILE, c = q / TILE;
       cplx v = sAcc[c * TILE + rr];
-      v = csub(v, sPart[(0 * k + c) * TILE + rr]);
-      v = csub(v, sPart[(1 * k + c) * TILE + rr]);
-      v = csub(v, sPart[(2 * k + c) * TILE + rr]);
-      v = csub(v, sPart[(3 * k + c) * TILE + rr]);
+#pragma unroll
+      for (int gq = 0; gq < NG; ++gq) v = csub(v, sPart[(gq * k + c) * TILE + rr]);
       sAcc[c * TILE + rr] = v;
     }
   }
-  // X_b = Dinv_b · acc  (adj: Dinv_bᴴ · acc)
+  // y = D_b⁻¹ acc (adj: D_b⁻ᴴ acc), kept in sAcc
   __syncthreads();
-  load_tile(sT, Dinv + (int64_t)b * TILE * TILE, adj);
-  __syncthreads();
-  {
-    cplx acc[KMAX];
+  product(sD, sAcc, adj);
+  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+    const int rr = q % TILE, c = q / TILE;
+    cplx v = sPart[(0 * k + c) * TILE + rr];
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c) acc[c] = czero();
-    tile_apply<KMAX>(sT, sAcc, k, adj, row, grp, acc);
+    for (int gq = 1; gq < NG; ++gq) v = cadd(v, sPart[(gq * k + c) * TILE + rr]);
+    sAcc[c * TILE + rr] = v;
+  }
+  if (ndep > 0) {
+    const int dep = adj ? b - 1 : b + 1;
+    load_tile(sT, E + ((int64_t)adj * nb + b) * TILE * TILE, 0);
+    wait_flag(dep);
+    load_x(dep);
+    product(sT, sX, 0);
+    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+      const int rr = q % TILE, c = q / TILE;
+      cplx v = sAcc[c * TILE + rr];
 #pragma unroll
-    for (int c = 0; c < KMAX; ++c)
-      if (c < k) sPart[(grp * k + c) * TILE + row] = acc[c];
+      for (int gq = 0; gq < NG; ++gq) v = csub(v, sPart[(gq * k + c) * TILE + rr]);
+      sAcc[c * TILE + rr] = v;
+    }
   }
   __syncthreads();
   for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
     const int rr = q % TILE, c = q / TILE;
-    cplx v = sPart[(0 * k + c) * TILE + rr];
-    v = cadd(v, sPart[(1 * k + c) * TILE + rr]);
-    v = cadd(v, sPart[(2 * k + c) * TILE + rr]);
-    v = cadd(v, sPart[(3 * k + c) * TILE + rr]);
-    X[(int64_t)c * ldx + (int64_t)b * TILE + rr] = v;
+    X[(int64_t)c * ldx + (int64_t)b * TILE + rr] = sAcc[c * TILE + rr];
   }
-  __threadfence();
+  // bar.sync orders every thread's stores before thread 0's release (cumulative).
   __syncthreads();
   if (threadIdx.x == 0) st_release(&flags[b], epoch);
+}
+
+inline size_t trsm_smem_bytes(int k, int ng) {
+  return ((size_t)2 * TILE * TILE_LDS + (size_t)(2 + ng) * TILE * k) * sizeof(cplx);
 }
 
 // Y[:, 0:k] = lam[j] * Y[:, j] - X[:, j]  (side 'L') or Y - X*lam (side 'S');

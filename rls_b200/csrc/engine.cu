@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/rls_b200.h"
+#include "batch.cuh"
 #include "blas.cuh"
 #include "heev.cuh"
 #include "rotate.cuh"
@@ -44,6 +45,7 @@ struct rls_ctx {
   int nb = 0;
   cplx* T = nullptr;        // tiles
   cplx* Dinv = nullptr;     // nb tiles
+  cplx* Etiles = nullptr;   // 2·nb tiles (k_trsm_etiles)
   cplx z_dinv = cmk(NAN, NAN);
   int* flags = nullptr;     // nb
   int* ticket = nullptr;    // 1
@@ -112,6 +114,13 @@ struct rls_ctx {
   int64_t launches = 0;            // kernel launches issued by this context
   int ritz_g1_always = 1;          // r_ == pr: use G1·G2 (1) or the reference's G2 alone (0)
   size_t heev_smem_avail = 0;      // dynamic shared memory k_heev_rr may use
+  // speculative batched recycle (rls_ctx_set_batch)
+  int spec_max = 16, spec_cur = 8;
+  cplx *bz = nullptr, *bG = nullptr, *bheevA = nullptr, *bczx = nullptr, *bstack0 = nullptr, *bstack1 = nullptr;
+  cplx *bRb = nullptr, *bG2 = nullptr, *bGtot = nullptr, *bXW = nullptr;
+  double *btau = nullptr, *bheevLU = nullptr, *bsig = nullptr, *bcolpart = nullptr, *bw0 = nullptr;
+  int* brr = nullptr;
+  int64_t bstack_stride = 0;
   struct KProf {
     std::vector<cudaEvent_t> ev;   // start/stop pairs not yet resolved
     int64_t count = 0;
@@ -260,7 +269,7 @@ int d2h(rls_ctx* ctx, T* h, const T* d, size_t count) {
 int gram(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k1, const cplx* B, int64_t ldb, int k2,
          cplx* C, int64_t ldc, cplx alpha = cmk(1, 0), cplx beta = cmk(0, 0)) {
   if (k1 <= 0 || k2 <= 0) return RLS_OK;
-  const int64_t chunk = 512;
+  const int64_t chunk = 64;   // 2 rows per lane: many CTAs, short dependency chains
   const int nchunks = (int)((nrows + chunk - 1) / chunk);
   for (int j0 = 0; j0 < k2; j0 += 32) {
     const int kk2 = std::min(32, k2 - j0);
@@ -269,8 +278,12 @@ int gram(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k1, const 
       return RLS_ERR_DIM;
     }
     dim3 grid(nchunks, (k1 + 7) / 8);
-    k_gram_partial<<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
-                                                  ctx->gram_part);
+    if (kk2 <= 8)
+      k_gram_partial<8><<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
+                                                       ctx->gram_part);
+    else
+      k_gram_partial<32><<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
+                                                        ctx->gram_part);
     RET(check_launch(ctx, "k_gram_partial"));
     const int tot = k1 * kk2;
     k_gram_reduce<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(nchunks, k1, kk2, ctx->gram_part, alpha, beta,
@@ -345,6 +358,32 @@ int small_gemm(rls_ctx* ctx, int m, int n, int kk, cplx alpha, const cplx* A, in
 // R (k×k, ld k) of the QR factorisation of A (nrows × k) by TSQR (k <= 64), else
 // by one CTA in global memory (A is then copied to tall_tmp first).
 int tsqr_r(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k, cplx* R) {
+  if (k <= 8) {  // warp leaves of 64 rows, reduced level by level
+    const cplx* src = A;
+    int64_t m = nrows, ld = lda;
+    int which = 0;
+    while (true) {
+      const int64_t nleaf = (m + 63) / 64;
+      cplx* dst = (nleaf == 1) ? R : ctx->tsqr_stack[which];
+      const int64_t ldd = (nleaf == 1) ? k : nleaf * k;
+      if (nleaf > 1 && (size_t)nleaf * k * k > ctx->tsqr_stack_elems) {
+        set_err(ctx, "tsqr workspace too small");
+        return RLS_ERR_DIM;
+      }
+      const unsigned nblk = (unsigned)((nleaf + 7) / 8);
+      if (k <= 4)
+        k_tsqr_warp<4><<<nblk, 256, 0, ctx->stream>>>(m, k, src, ld, dst, ldd, nleaf);
+      else
+        k_tsqr_warp<8><<<nblk, 256, 0, ctx->stream>>>(m, k, src, ld, dst, ldd, nleaf);
+      RET(check_launch(ctx, "k_tsqr_warp"));
+      if (nleaf == 1) break;
+      src = dst;
+      m = nleaf * k;
+      ld = m;
+      which ^= 1;
+    }
+    return RLS_OK;
+  }
   if (k <= 64) {
     // mb >= 2k guarantees every level shrinks the stack (m' = ceil(m/mb)·k < m for m > mb).
     int mb = std::max(2 * k, std::min(256, (int)(196608 / (k * (int)sizeof(cplx)))));
@@ -466,16 +505,18 @@ int ensure_dinv(rls_ctx* ctx, cplx z) {
   const size_t smem = 2 * TILE * TILE * sizeof(cplx);
   k_diag_inv<<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->n, ctx->T, z, ctx->Dinv, ctx->derr);
   RET(check_launch(ctx, "k_diag_inv"));
+  k_trsm_etiles<<<dim3(ctx->nb, 2), 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, ctx->Etiles);
+  RET(check_launch(ctx, "k_trsm_etiles"));
   ctx->z_dinv = z;
   return RLS_OK;
 }
 
-// X = R⁻¹ B (adj=0) or R⁻ᴴ B (adj=1), R = T − zI; X may alias B; k <= 24.
+// X = R⁻¹ B (adj=0) or R⁻ᴴ B (adj=1), R = T − zI; X may alias B.
 int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int k) {
   RET(ensure_dinv(ctx, z));
-  if (k > 24) {
-    for (int c0 = 0; c0 < k; c0 += 24)
-      RET(trsm(ctx, z, adj, B + (int64_t)c0 * ld, X + (int64_t)c0 * ld, ld, std::min(24, k - c0)));
+  if (k > 8) {   // column chunks of 8 (the kernel's register/shared-memory budget)
+    for (int c0 = 0; c0 < k; c0 += 8)
+      RET(trsm(ctx, z, adj, B + (int64_t)c0 * ld, X + (int64_t)c0 * ld, ld, std::min(8, k - c0)));
     return RLS_OK;
   }
   ctx->epoch += 1;
@@ -484,15 +525,10 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
     CK(cudaMemsetAsync(ctx->flags, 0, sizeof(int) * ctx->nb, ctx->stream));
   }
   CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(int), ctx->stream));
-  const size_t smem = ((size_t)TILE * TILE_LDS + 6 * (size_t)TILE * k) * sizeof(cplx);
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_TRSM, &e0);
-  if (k <= 8)
-    k_trsm_dataflow<8><<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
-                                                            ctx->flags, ctx->epoch, ctx->derr);
-  else
-    k_trsm_dataflow<24><<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, B, X, ld, k, adj, ctx->ticket,
-                                                             ctx->flags, ctx->epoch, ctx->derr);
+  k_trsm_dataflow<8, 8><<<ctx->nb, 512, trsm_smem_bytes(k, 8), ctx->stream>>>(
+      ctx->nb, ctx->T, ctx->Dinv, ctx->Etiles, B, X, ld, k, adj, ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);
   // algorithmic bytes: the upper triangle of T once (n²/2 complex) + B read + X written
   prof_end(ctx, KP_TRSM, e0, 16.0 * ((double)ctx->n * (ctx->n + 1) / 2 + 2.0 * (double)ctx->n * k));
   return check_launch(ctx, "k_trsm_dataflow");
@@ -526,12 +562,16 @@ void release_space(rls_ctx* ctx) {
   cplx** bufs[] = {&ctx->V, &ctx->J1, &ctx->J2, &ctx->J5, &ctx->shift_tmp, &ctx->L, &ctx->H1, &ctx->H2, &ctx->Hs,
                    &ctx->Ulist, &ctx->heev.A, &ctx->Gheev, &ctx->CzX, &ctx->Gtot, &ctx->S, &ctx->CS, &ctx->Gk,
                    &ctx->Rk, &ctx->tall_tmp, &ctx->gram_part, &ctx->tsqr_stack[0], &ctx->tsqr_stack[1],
-                   &ctx->house_tau, &ctx->zdev, &ctx->owW, &ctx->owR, &ctx->svdA, &ctx->svdV, &ctx->gemm_tmp};
+                   &ctx->house_tau, &ctx->zdev, &ctx->owW, &ctx->owR, &ctx->svdA, &ctx->svdV, &ctx->gemm_tmp, &ctx->bz, &ctx->bG, &ctx->bheevA,
+                   &ctx->bczx, &ctx->bstack0, &ctx->bstack1, &ctx->bRb, &ctx->bG2, &ctx->bGtot, &ctx->bXW};
   for (cplx** b : bufs) { dfree(ctx, *b); *b = nullptr; }
-  double** dbufs[] = {&ctx->heev.lu, &ctx->lam_dev, &ctx->taudev, &ctx->sig_rec, &ctx->sig, &ctx->lam};
+  double** dbufs[] = {&ctx->heev.lu, &ctx->lam_dev, &ctx->taudev, &ctx->sig_rec, &ctx->sig, &ctx->lam,
+                      &ctx->btau, &ctx->bheevLU, &ctx->bsig, &ctx->bcolpart, &ctx->bw0};
   for (double** b : dbufs) { dfree(ctx, *b); *b = nullptr; }
   dfree(ctx, ctx->rr_dev);
   ctx->rr_dev = nullptr;
+  dfree(ctx, ctx->brr);
+  ctx->brr = nullptr;
   for (int i = 0; i < 8; ++i) { dfree(ctx, ctx->small[i]); ctx->small[i] = nullptr; }
   ctx->r = 0;
   ctx->p_max = 0;
@@ -581,7 +621,7 @@ int setup_space(rls_ctx* ctx, int r, int p_max) {
   ctx->tall_tmp_cols = std::max(prm, 2 * r);
   RET(dalloc_t(ctx, &ctx->tall_tmp, (size_t)np * ctx->tall_tmp_cols));
   const int kmax = std::max(prm, 3 * r);
-  ctx->gram_part_elems = (size_t)((np + 511) / 512) * kmax * 32;
+  ctx->gram_part_elems = (size_t)((np + 63) / 64) * kmax * 32;
   RET(dalloc_t(ctx, &ctx->gram_part, ctx->gram_part_elems));
   ctx->tsqr_stack_elems = (size_t)((np + 63) / 64 + 2) * 64 * 64;
   RET(dalloc_t(ctx, &ctx->tsqr_stack[0], ctx->tsqr_stack_elems));
@@ -595,6 +635,27 @@ int setup_space(rls_ctx* ctx, int r, int p_max) {
   RET(dalloc_t(ctx, &ctx->svdV, (size_t)prm * prm));
   ctx->gemm_tmp_cols = 64;
   RET(dalloc_t(ctx, &ctx->gemm_tmp, (size_t)np * 64));
+  {  // speculative batch workspaces (BATCH_MAX points)
+    const size_t BM = BATCH_MAX;
+    RET(dalloc_t(ctx, &ctx->bz, BM));
+    RET(dalloc_t(ctx, &ctx->btau, BM));
+    RET(dalloc_t(ctx, &ctx->brr, BM));
+    RET(dalloc_t(ctx, &ctx->bG, BM * prm * prm));
+    RET(dalloc_t(ctx, &ctx->bheevA, BM * prm * prm));
+    RET(dalloc_t(ctx, &ctx->bheevLU, BM * 16 * 6 * prm));
+    RET(dalloc_t(ctx, &ctx->bczx, BM * np * BATCH_KMAX));
+    const int64_t nleaf0 = (np + 255) / 256;
+    ctx->bstack_stride = (nleaf0 + 1) * BATCH_KMAX * BATCH_KMAX;
+    RET(dalloc_t(ctx, &ctx->bstack0, BM * ctx->bstack_stride));
+    RET(dalloc_t(ctx, &ctx->bstack1, BM * ctx->bstack_stride));
+    RET(dalloc_t(ctx, &ctx->bRb, BM * BATCH_KMAX * BATCH_KMAX));
+    RET(dalloc_t(ctx, &ctx->bG2, BM * BATCH_KMAX * BATCH_KMAX));
+    RET(dalloc_t(ctx, &ctx->bsig, BM * BATCH_KMAX));
+    RET(dalloc_t(ctx, &ctx->bGtot, BM * prm * r));
+    RET(dalloc_t(ctx, &ctx->bXW, BM * 2 * np * r));
+    RET(dalloc_t(ctx, &ctx->bcolpart, BM * (np / 32 + 1)));
+    RET(dalloc_t(ctx, &ctx->bw0, BM));
+  }
   return RLS_OK;
 }
 
@@ -759,19 +820,31 @@ int add_blocks(rls_ctx* ctx, const cplx* Xin, cplx z) {  // _add_blocks! (recySp
   return RLS_OK;
 }
 
-int block_unitary_update(rls_ctx* ctx) {  // _block_unitary_update! (recySpace.jl:226-286)
+// _block_unitary_update! (recySpace.jl:226-286).  The reference interleaves, per
+// rotation, rmul!(·, U_iᴴ) and lmul!(U_i, ·) on H1/H2; left and right products commute,
+// so all right products run first (row-parallel) and all left products after
+// (column-parallel).  J6 = V and J3 = S'J5 = J5 follow V and J5.
+int block_unitary_update(rls_ctx* ctx) {
   const int p = ctx->p, r = ctx->r;
   if (p <= 1) return RLS_OK;
-  const int pr = p * r;
-  const size_t smem = ((size_t)2 * r * r + 8 * (size_t)r * r + r + 2 * (size_t)r * pr) * sizeof(cplx);
-  k_blockrot_prep<<<1, 256, smem, ctx->stream>>>(p, r, ctx->L, ctx->H1, ctx->H2, ctx->pr_max, ctx->Ulist);
-  RET(check_launch(ctx, "k_blockrot_prep"));
+  const int pr = p * r, r2 = 2 * r;
+  const size_t smc = ((size_t)pr * r + 2 * (size_t)r * r + 4 * (size_t)r * r + r) * sizeof(cplx);
+  k_blockrot_coeffs<<<1, 32, smc, ctx->stream>>>(p, r, ctx->L, ctx->pr_max, ctx->Ulist);
+  RET(check_launch(ctx, "k_blockrot_coeffs"));
   RotArrays arr{};
-  arr.a[0] = ctx->V; arr.a[1] = ctx->J1; arr.a[2] = ctx->J2; arr.a[3] = ctx->J5;
-  dim3 grid((unsigned)((ctx->n_pad + 31) / 32), 4);
-  const size_t smem2 = ((size_t)32 * 2 * r + 4 * (size_t)r * r) * sizeof(cplx);
-  k_blockrot_apply<<<grid, 32 * 2 * r, smem2, ctx->stream>>>(ctx->n_pad, p, r, arr, ctx->n_pad, ctx->Ulist);
-  return check_launch(ctx, "k_blockrot_apply");
+  cplx* tall[4] = {ctx->V, ctx->J1, ctx->J2, ctx->J5};
+  for (int q = 0; q < 4; ++q) { arr.a[q] = tall[q]; arr.nrows[q] = ctx->n_pad; arr.ld[q] = ctx->n_pad; }
+  arr.a[4] = ctx->H1; arr.nrows[4] = pr; arr.ld[4] = ctx->pr_max;
+  arr.a[5] = ctx->H2; arr.nrows[5] = pr; arr.ld[5] = ctx->pr_max;
+  const size_t sm = ((size_t)32 * r2 + (size_t)r2 * r2) * sizeof(cplx);
+  dim3 grid((unsigned)((ctx->n_pad + 31) / 32), 6);
+  k_blockrot_apply<<<grid, 32 * r2, sm, ctx->stream>>>(p, r, arr, ctx->Ulist);
+  RET(check_launch(ctx, "k_blockrot_apply"));
+  RotMats mats{};
+  mats.m[0] = ctx->L; mats.m[1] = ctx->H1; mats.m[2] = ctx->H2;
+  dim3 grid2((unsigned)((pr + 31) / 32), 3);
+  k_blockrot_left<<<grid2, 32 * r2, sm, ctx->stream>>>(p, r, mats, ctx->pr_max, ctx->Ulist);
+  return check_launch(ctx, "k_blockrot_left");
 }
 
 int update_recycled_space(rls_ctx* ctx, cplx z, const cplx* X, double tau, bool force_add, int p_min) {
@@ -894,6 +967,84 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   return RLS_OK;
 }
 
+// Recycle step of B consecutive points against the current space (batch.cuh).  On
+// return rr[b] (0 when the batch path skipped the point: Ritz dimension > BATCH_KMAX),
+// sig0[b] and w0[b] = |W_b[:,1]| for b < B; X_b, W_b stay in ctx->bXW.
+int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, double shift, int* rr, double* sig0,
+                  double* w0) {
+  const int r = ctx->r, pr = ctx->p * r;
+  const int64_t np = ctx->n_pad;
+  CK(cudaMemcpyAsync(ctx->bz, zs, sizeof(cplx) * B, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->btau, taus, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->stream));
+  const HeevPlan plan = heev_plan(pr, ctx->heev_smem_avail);
+  HeevWork hw{ctx->bheevA, ctx->bheevLU};
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_HEEV, &e0);
+  k_heev_rr<<<B, HEEV_THREADS, plan.bytes, ctx->stream>>>(pr, r, ctx->H1, ctx->H2, ctx->pr_max, ctx->bz, ctx->btau,
+                                                          shift, hw, ctx->pr_max, ctx->bG, ctx->pr_max,
+                                                          (int64_t)ctx->pr_max * ctx->pr_max, ctx->brr, nullptr,
+                                                          ctx->derr, plan, nullptr);
+  prof_end(ctx, KP_HEEV, e0, B * 16.0 / 3.0 * (double)pr * pr * pr);
+  RET(check_launch(ctx, "k_heev_rr(batch)"));
+  BatchDesc d{};
+  d.B = B; d.pr = pr; d.r = r; d.ldh = ctx->pr_max; d.np = np;
+  d.J1 = ctx->J1; d.J2 = ctx->J2; d.J5 = ctx->J5; d.V = ctx->V;
+  d.zs = ctx->bz; d.rr = ctx->brr;
+  d.G1 = ctx->bG; d.g1_stride = (int64_t)ctx->pr_max * ctx->pr_max; d.ldg1 = ctx->pr_max;
+  d.czx = ctx->bczx;
+  d.stack[0] = ctx->bstack0; d.stack[1] = ctx->bstack1; d.stack_stride = ctx->bstack_stride;
+  d.Rb = ctx->bRb; d.sig = ctx->bsig; d.G2 = ctx->bG2;
+  d.Gtot = ctx->bGtot; d.gtot_stride = (int64_t)ctx->pr_max * r;
+  d.XW = ctx->bXW; d.colpart = ctx->bcolpart; d.ntiles = (int)((np + 31) / 32); d.w0sq = ctx->bw0;
+  d.g1_always = ctx->ritz_g1_always;
+  const dim3 tiles((unsigned)d.ntiles, (unsigned)B);
+  cudaEvent_t e1 = nullptr;
+  prof_begin(ctx, KP_RECYCLE_GEMM, &e1);
+  k_batch_czx<<<tiles, 256, (size_t)8 * BATCH_KMAX * 32 * sizeof(cplx), ctx->stream>>>(d);
+  RET(check_launch(ctx, "k_batch_czx"));
+  // TSQR levels sized for BATCH_KMAX columns
+  {
+    const int mb = 256;
+    int64_t m = np;
+    int level = 0;
+    int64_t ld_in = np;
+    while (true) {
+      const int64_t nleaf = (m + mb - 1) / mb;
+      const bool fin = (nleaf == 1);
+      const int64_t ld_out = nleaf * BATCH_KMAX;
+      k_batch_tsqr<<<dim3((unsigned)nleaf, (unsigned)B), 256, ((size_t)mb * BATCH_KMAX + 2 * BATCH_KMAX) * sizeof(cplx),
+                     ctx->stream>>>(d, level, mb, ld_in, ld_out, fin ? 1 : 0);
+      RET(check_launch(ctx, "k_batch_tsqr"));
+      if (fin) break;
+      if (ld_out > ctx->bstack_stride / BATCH_KMAX) {
+        set_err(ctx, "batched TSQR stack too small");
+        return RLS_ERR_DIM;
+      }
+      m = nleaf * BATCH_KMAX;
+      ld_in = ld_out;
+      ++level;
+    }
+  }
+  k_batch_svd_gtot<<<B, 256, 0, ctx->stream>>>(d);
+  RET(check_launch(ctx, "k_batch_svd_gtot"));
+  k_batch_xw<<<tiles, 256, (size_t)2 * 8 * 8 * 32 * sizeof(cplx), ctx->stream>>>(d);
+  RET(check_launch(ctx, "k_batch_xw"));
+  prof_end(ctx, KP_RECYCLE_GEMM, e1, B * 16.0 * ((double)ctx->n * pr * 6 + 2.0 * ctx->n * r));
+  k_batch_w0<<<B, 256, 0, ctx->stream>>>(d);
+  RET(check_launch(ctx, "k_batch_w0"));
+  std::vector<double> hs((size_t)B * BATCH_KMAX), hw0(B);
+  CK(cudaMemcpyAsync(rr, ctx->brr, sizeof(int) * B, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(hs.data(), ctx->bsig, sizeof(double) * B * BATCH_KMAX, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(hw0.data(), ctx->bw0, sizeof(double) * B, cudaMemcpyDeviceToHost, ctx->stream));
+  RET(sync_and_check(ctx));
+  for (int b = 0; b < B; ++b) {
+    if (rr[b] < 1 || rr[b] > BATCH_KMAX) rr[b] = 0;
+    sig0[b] = hs[(size_t)b * BATCH_KMAX];
+    w0[b] = hw0[b] >= 0 ? std::sqrt(hw0[b]) : INFINITY;
+  }
+  return RLS_OK;
+}
+
 void emit_log(rls_ctx* ctx, const char* fmt, ...) {
   if (!ctx->log_fn) return;
   char buf[512];
@@ -950,14 +1101,17 @@ int allow_big_smem(rls_ctx* ctx, K kernel, int optin) {
 int set_kernel_attrs(rls_ctx* ctx) {
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  RET(allow_big_smem(ctx, k_trsm_dataflow<8>, optin));
-  RET(allow_big_smem(ctx, k_trsm_dataflow<24>, optin));
+  RET(allow_big_smem(ctx, k_trsm_dataflow<8, 8>, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<8>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<8>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<16>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<32>, optin));
+  RET(allow_big_smem(ctx, k_batch_czx, optin));
+  RET(allow_big_smem(ctx, k_batch_xw, optin));
+  RET(allow_big_smem(ctx, k_batch_tsqr, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<16>, optin));
   RET(allow_big_smem(ctx, k_diag_inv, optin));
+  RET(allow_big_smem(ctx, k_trsm_etiles, optin));
   RET(allow_big_smem(ctx, k_tsqr_leaf, optin));
   RET(allow_big_smem(ctx, k_heev_rr, optin));
   {
@@ -966,7 +1120,7 @@ int set_kernel_attrs(rls_ctx* ctx) {
     ctx->heev_smem_avail = (size_t)(optin - (int)fa.sharedSizeBytes);
   }
   RET(allow_big_smem(ctx, k_svd_rr, optin));
-  RET(allow_big_smem(ctx, k_blockrot_prep, optin));
+  RET(allow_big_smem(ctx, k_blockrot_coeffs, optin));
   RET(allow_big_smem(ctx, k_chol_inv, optin));
   RET(allow_big_smem(ctx, k_trtri, optin));
   return RLS_OK;
@@ -1054,7 +1208,7 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   // drop an old operator and space
-  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
+  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->Etiles, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
                   (void*)ctx->colpart, (void*)ctx->trmm_uO[0], (void*)ctx->trmm_us[0], (void*)ctx->trmm_Ofirst[0],
                   (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
                   (void*)ctx->trmm_Ofirst[1], (void*)ctx->trmm_Ocount[1]})
@@ -1082,6 +1236,7 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   RET(dalloc_t(ctx, &ctx->T, h.size()));
   CK(cudaMemcpyAsync(ctx->T, h.data(), h.size() * sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
+  RET(dalloc_t(ctx, &ctx->Etiles, (size_t)2 * nb * TILE * TILE));
   RET(dalloc_t(ctx, &ctx->flags, (size_t)nb));
   RET(dalloc_t(ctx, &ctx->ticket, 1));
   ctx->z_dinv = cmk(NAN, NAN);
@@ -1202,6 +1357,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     }
     run.active = true;
     run.next = 0;
+    ctx->spec_cur = std::min(8, ctx->spec_max);
     run.nZ = nZ;
     run.remaining = 0;
     run.have_failed = false;
@@ -1215,40 +1371,22 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     return RLS_ERR_STATE;
   }
   const double lob_tol = ctl->lobpcg_tol_scale * ctl->tol;
-  for (int64_t i = i_begin; i < i_end; ++i) {
+  auto thresh_ok = [&](double w0, double s0) {   // _residual_norm_ok (psTriRecy.jl:237-245)
+    return w0 < ctl->normC * std::max(s0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps);
+  };
+  auto accept = [&](int64_t i, double s0, int r_svdrr) {
+    sigma_min[i] = s0;
+    if (st->M_vec_apps) st->M_vec_apps[i] = 0;
+    if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = 0;
+    if (st->R_vec_apps) st->R_vec_apps[i] = 0;
+    if (ctx->verbose >= 1)
+      emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
+               (long long)(i + 1), (long long)nZ, Z[i].re, Z[i].im, "recycled", ctx->p, r_svdrr, s0);
+  };
+  // Refine point i (X0 = keep.S[:, 1:r] as left by its recycle step, or the previous
+  // run state) and update the space (psTriRecy.jl:795-855).
+  auto refine = [&](int64_t i, int r_svdrr) -> int {
     const cplx z = cmk(Z[i].re, Z[i].im);
-    if (st->p_count) st->p_count[i] = ctx->p;
-    if (st->r_recy) st->r_recy[i] = 0;
-    if (st->refine_it) st->refine_it[i] = 0;
-    int64_t m_apps = 0, r_apps = 0;
-    int r_svdrr = 0;
-    if (ctx->p > 0) {
-      const uint64_t t0 = now_ns();
-      const double gtau = run.remaining > 0 ? ctl->gap_tau * ctl->gap_tau_scale : ctl->gap_tau;
-      RecycleResult rres{};
-      RET(recycle_step(ctx, z, ctl->shift, gtau, &rres));
-      run.remaining = run.remaining > 0 ? run.remaining - 1 : 0;
-      st->recycle_time_ns += now_ns() - t0;
-      r_svdrr = rres.rr;
-      if (st->r_recy) st->r_recy[i] = r_svdrr;
-      // _residual_norm_ok (psTriRecy.jl:237-245)
-      const bool ok = rres.w0norm < ctl->normC * std::max(rres.sigma0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps);
-      if (ok) {
-        sigma_min[i] = rres.sigma0;
-        if (st->M_vec_apps) st->M_vec_apps[i] = 0;
-        if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = 0;
-        if (st->R_vec_apps) st->R_vec_apps[i] = 0;
-        if (ctx->verbose >= 1)
-          emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
-                   (long long)(i + 1), (long long)nZ, z.x, z.y, "recycled", ctx->p, r_svdrr, sigma_min[i]);
-        run.next = i + 1;
-        continue;
-      }
-      if (ctx->verbose >= 2)
-        emit_log(ctx, "  recycle rejected: |W[:,1]|=%.3e threshold=%.3e σ_recy=%.6e r_svdrr=%d pr=%d", rres.w0norm,
-                 ctl->normC * std::max(rres.sigma0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps), rres.sigma0,
-                 r_svdrr, ctx->p * r);
-    }
     const uint64_t t1 = now_ns();
     LobpcgResult lres{};
     RET(lobpcg_invtri(ctx, z, r, 2000, lob_tol, true, &lres));
@@ -1256,6 +1394,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     RET(d2h(ctx, &s0, ctx->sig, 1));
     sigma_min[i] = s0;  // keep.σ[1] (psTriRecy.jl:809)
     const int64_t it = lres.it;
+    int64_t m_apps = 0, r_apps = 0;
     if (st->refine_it) st->refine_it[i] = it;
     if (it > 0) r_apps += 2 * r + it * r + (it - 1) * r;
     st->refine_time_ns += now_ns() - t1;
@@ -1283,7 +1422,100 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
       emit_log(ctx, "[%4lld/%4lld] z=%9.4f%+9.4fim | main: state=%-12s p=%3d r_svdrr=%3d σ=%9.3e",
                (long long)(i + 1), (long long)nZ, z.x, z.y, state, ctx->p, r_svdrr, sigma_min[i]);
     }
-    run.next = i + 1;
+    return RLS_OK;
+  };
+  auto gap_tau_at = [&](int rem) { return rem > 0 ? ctl->gap_tau * ctl->gap_tau_scale : ctl->gap_tau; };
+
+  int64_t i = i_begin;
+  while (i < i_end) {
+    if (st->refine_it) st->refine_it[i] = 0;
+    if (st->r_recy) st->r_recy[i] = 0;
+    if (st->p_count) st->p_count[i] = ctx->p;
+    if (ctx->p == 0) {
+      RET(refine(i, 0));
+      run.next = ++i;
+      continue;
+    }
+    const int B = (int)std::min<int64_t>(std::min(ctx->spec_cur, ctx->spec_max), i_end - i);
+    if (B >= 2 && ctx->spec_max >= 2) {
+      // Speculative batch: the recycle steps of points i..i+B-1 against the current space.
+      // Accepted points leave the space unchanged, so the results up to the first
+      // rejection are exactly those of the sequential loop.
+      cplx zs[BATCH_MAX];
+      double taus[BATCH_MAX], sig0[BATCH_MAX], w0[BATCH_MAX];
+      int rr[BATCH_MAX];
+      for (int b = 0; b < B; ++b) {
+        zs[b] = cmk(Z[i + b].re, Z[i + b].im);
+        taus[b] = gap_tau_at(std::max(run.remaining - b, 0));
+      }
+      const uint64_t t0 = now_ns();
+      RET(recycle_batch(ctx, B, zs, taus, ctl->shift, rr, sig0, w0));
+      st->recycle_time_ns += now_ns() - t0;
+      int b = 0;
+      bool failed = false;
+      for (; b < B; ++b) {
+        if (rr[b] == 0) break;  // Ritz dimension beyond the batch path: per-point below
+        if (st->p_count) st->p_count[i + b] = ctx->p;
+        if (st->r_recy) st->r_recy[i + b] = rr[b];
+        if (st->refine_it) st->refine_it[i + b] = 0;
+        if (thresh_ok(w0[b], sig0[b])) {
+          accept(i + b, sig0[b], rr[b]);
+          continue;
+        }
+        failed = true;
+        break;
+      }
+      if (failed) {
+        // recycle steps consumed: b + 1 (the rejected point ran one too)
+        run.remaining = std::max(run.remaining - (b + 1), 0);
+        const cplx* xw = ctx->bXW + (int64_t)b * 2 * ctx->n_pad * r;
+        CK(cudaMemcpyAsync(ctx->S, xw, sizeof(cplx) * 2 * ctx->n_pad * r, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (ctx->verbose >= 2)
+          emit_log(ctx, "  recycle rejected: |W[:,1]|=%.3e σ_recy=%.6e r_svdrr=%d pr=%d (batch %d/%d)", w0[b],
+                   sig0[b], rr[b], ctx->p * r, b + 1, B);
+        RET(refine(i + b, rr[b]));
+        i += b + 1;
+        ctx->spec_cur = std::max(4, std::min(ctx->spec_max, b + 4));
+      } else {
+        run.remaining = std::max(run.remaining - b, 0);
+        i += b;
+        if (b == B) ctx->spec_cur = std::min(ctx->spec_max, 2 * ctx->spec_cur);
+        else {  // point i (= old i + b) needs the per-point path (large Ritz dimension)
+          const cplx z = cmk(Z[i].re, Z[i].im);
+          if (st->p_count) st->p_count[i] = ctx->p;
+          const uint64_t t1 = now_ns();
+          RecycleResult rres{};
+          RET(recycle_step(ctx, z, ctl->shift, gap_tau_at(run.remaining), &rres));
+          run.remaining = run.remaining > 0 ? run.remaining - 1 : 0;
+          st->recycle_time_ns += now_ns() - t1;
+          if (st->r_recy) st->r_recy[i] = rres.rr;
+          if (thresh_ok(rres.w0norm, rres.sigma0)) accept(i, rres.sigma0, rres.rr);
+          else RET(refine(i, rres.rr));
+          ++i;
+        }
+      }
+      run.next = i;
+      continue;
+    }
+    // per-point recycle step
+    {
+      const cplx z = cmk(Z[i].re, Z[i].im);
+      const uint64_t t0 = now_ns();
+      RecycleResult rres{};
+      RET(recycle_step(ctx, z, ctl->shift, gap_tau_at(run.remaining), &rres));
+      run.remaining = run.remaining > 0 ? run.remaining - 1 : 0;
+      st->recycle_time_ns += now_ns() - t0;
+      if (st->r_recy) st->r_recy[i] = rres.rr;
+      if (thresh_ok(rres.w0norm, rres.sigma0)) {
+        accept(i, rres.sigma0, rres.rr);
+      } else {
+        if (ctx->verbose >= 2)
+          emit_log(ctx, "  recycle rejected: |W[:,1]|=%.3e σ_recy=%.6e r_svdrr=%d pr=%d", rres.w0norm, rres.sigma0,
+                   rres.rr, ctx->p * r);
+        RET(refine(i, rres.rr));
+      }
+      run.next = ++i;
+    }
   }
   if (i_end == nZ) run.active = false;
   return sync_and_check(ctx);
@@ -1298,6 +1530,13 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
 extern "C" void* rls_ctx_stream(rls_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 extern "C" int64_t rls_ctx_launches(const rls_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int rls_ctx_set_batch(rls_ctx* ctx, int max_points) {
+  if (!ctx || max_points < 1 || max_points > BATCH_MAX) return RLS_ERR_ARG;
+  ctx->spec_max = max_points;
+  ctx->spec_cur = std::min(8, max_points);
+  return RLS_OK;
+}
 
 extern "C" int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always) {
   if (!ctx) return RLS_ERR_ARG;

@@ -28,33 +28,52 @@ struct HeevWork {
   double* lu;     // per problem 16 warps × 6 × pr_max doubles
 };
 
-__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
-  int cnt = 0;
-  double q = d[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  cnt += (q < 0.0);
-  for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    cnt += (q < 0.0);
-  }
-  return cnt;
+// 1/q by the hardware reciprocal estimate refined with two Newton–Raphson steps
+// (r ← r + r(1 − q r)); the relative error is far below what a Sturm count needs.
+__device__ __forceinline__ double recip_nr(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  double e = fma(-q, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-q, r, 1.0);
+  return fma(r, e, r);
 }
 
-// Eigenvalue with 0-based index `idx` (ascending) by 32-way multisection, one warp.
+// Numbers of eigenvalues of the tridiagonal (d, e²) below x1 and below x2 (two
+// interleaved Sturm sequences).
+__device__ __forceinline__ void sturm_count2(const double* d, const double* e2, int n, double x1, double x2,
+                                             double pivmin, int* c1, int* c2) {
+  double q1 = d[0] - x1, q2 = d[0] - x2;
+  if (fabs(q1) < pivmin) q1 = -pivmin;
+  if (fabs(q2) < pivmin) q2 = -pivmin;
+  int n1 = (q1 < 0.0), n2 = (q2 < 0.0);
+  for (int i = 1; i < n; ++i) {
+    const double di = d[i], ei = e2[i - 1];
+    q1 = di - x1 - ei * recip_nr(q1);
+    q2 = di - x2 - ei * recip_nr(q2);
+    if (fabs(q1) < pivmin) q1 = -pivmin;
+    if (fabs(q2) < pivmin) q2 = -pivmin;
+    n1 += (q1 < 0.0);
+    n2 += (q2 < 0.0);
+  }
+  *c1 = n1;
+  *c2 = n2;
+}
+
+// Eigenvalue with 0-based index `idx` (ascending) by 65-way multisection, one warp:
+// lane l evaluates the counts at the interior points 2l+1 and 2l+2 of 65 intervals.
 __device__ double warp_eig_index(const double* d, const double* e2, int n, int idx, double gl, double gu,
                                  double pivmin, double atol) {
   const int lane = threadIdx.x & 31;
   double lo = gl, hi = gu;
-  for (int round = 0; round < 14 && (hi - lo) > atol; ++round) {
-    const double h = (hi - lo) / 33.0;
-    const double x = lo + h * (lane + 1);
-    const int c = sturm_count(d, e2, n, x, pivmin);     // # eigenvalues < x
-    // largest lane whose count <= idx gives a new lower bound; smallest with count > idx an upper bound
-    const unsigned le = __ballot_sync(0xffffffffu, c <= idx);
-    const int nle = __popc(le);                          // counts are monotone in lane
-    const double nlo = (nle > 0) ? lo + h * nle : lo;
-    const double nhi = (nle < 32) ? lo + h * (nle + 1) : hi;
+  for (int round = 0; round < 12 && (hi - lo) > atol; ++round) {
+    const double h = (hi - lo) / 65.0;
+    int c1, c2;
+    sturm_count2(d, e2, n, lo + h * (2 * lane + 1), lo + h * (2 * lane + 2), pivmin, &c1, &c2);
+    // counts are monotone in the point index: number of points with count <= idx
+    const int nle = __popc(__ballot_sync(0xffffffffu, c1 <= idx)) + __popc(__ballot_sync(0xffffffffu, c2 <= idx));
+    const double nlo = lo + h * nle;
+    const double nhi = (nle < 64) ? lo + h * (nle + 1) : hi;
     lo = nlo; hi = nhi;
   }
   return 0.5 * (lo + hi);
@@ -157,10 +176,9 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   __syncthreads();
 
   // 2. Householder tridiagonalisation (lower form): for column k reduce A[k+1:, k].
-  //    Three barriers per column: warp 0 forms the reflector; groups of 4 threads
-  //    form y_i = τ Σ_j conj(A[j,i]) v_j (column i of the Hermitian trailing block)
-  //    with per-warp partials of yᴴv; all threads apply A −= v wᴴ + w vᴴ with
-  //    w = y + α₂·v, α₂ = −½ τ (yᴴv), formed on the fly.
+  //    Four barriers per column: warp 0 forms the reflector; groups of 4 threads
+  //    form y = τ·A·v from the lower triangle with per-warp partials of yᴴv;
+  //    w = y + α₂·v, α₂ = −½ τ (yᴴv); the lower triangle takes A −= v wᴴ + w vᴴ.
   for (int k = 0; k < n - 1; ++k) {
     const int m0 = k + 1;
     if (warp == 0) {
@@ -184,6 +202,8 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
     __syncthreads();
     const cplx t = s_tau;
     if (t.x != 0.0 || t.y != 0.0) {
+      // y_i = τ Σ_j Ã[i,j] v_j over the trailing block, Ã from the lower triangle:
+      // Ã[i,j] = A[i,j] (i >= j), conj(A[j,i]) (i < j).
       const int mm = n - m0;
       const int nq = ((mm * 4 + 31) / 32) * 32;
       cplx yv_part = czero();
@@ -191,8 +211,11 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
         const bool valid = q < mm * 4;
         const int i = m0 + q / 4, part = q & 3;
         cplx sum = czero();
-        if (valid)
-          for (int j = m0 + part; j < n; j += 4) sum = cfmac(A[i * lda + j], v[j], sum);
+        if (valid) {
+          int j = m0 + part;
+          for (; j < i; j += 4) sum = cfma(A[j * lda + i], v[j], sum);        // row i, j < i
+          for (; j < n; j += 4) sum = cfmac(A[i * lda + j], v[j], sum);       // column i, j >= i
+        }
         sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
         sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
         sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 2);
@@ -209,12 +232,15 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
       cplx yv = czero();
       for (int q = 0; q < nw; ++q) yv = cadd(yv, ypart[q]);
       const cplx a2 = cscale(cmul(t, yv), -0.5);
+      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) w[i] = cfma(a2, v[i], w[i]);
+      __syncthreads();
+      // lower triangle (and diagonal) of A −= v wᴴ + w vᴴ
       for (int q = threadIdx.x; q < mm * mm; q += blockDim.x) {
         const int i = m0 + q % mm, j = m0 + q / mm;
-        const cplx wi = cfma(a2, v[i], w[i]), wj = cfma(a2, v[j], w[j]);
+        if (i < j) continue;
         cplx aij = A[j * lda + i];
-        aij = csub(aij, cmul(v[i], cconj(wj)));
-        aij = csub(aij, cmul(wi, cconj(v[j])));
+        aij = csub(aij, cmul(v[i], cconj(w[j])));
+        aij = csub(aij, cmul(w[i], cconj(v[j])));
         A[j * lda + i] = aij;
       }
       __syncthreads();

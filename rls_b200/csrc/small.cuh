@@ -100,6 +100,66 @@ __global__ void __launch_bounds__(256) k_tsqr_leaf(int64_t m, int k, int mb, con
   }
 }
 
+// ------------------------------------------------------------------------------------
+// One-warp TSQR leaf for narrow blocks (k <= 8): warp w of the CTA factors rows
+// [leaf*64, leaf*64 + 64) of A (m × k), leaf = blockIdx.x*8 + w, each lane holding two
+// rows in registers; reductions are warp shuffles only.  R (k × k, zeros below the
+// diagonal) goes to rows [leaf*k, leaf*k + k) of `stack` (ld = lds).
+// ------------------------------------------------------------------------------------
+template <int KW>
+__global__ void __launch_bounds__(256) k_tsqr_warp(int64_t m, int k, const cplx* __restrict__ A, int64_t lda,
+                                                   cplx* __restrict__ stack, int64_t lds, int64_t nleaf) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t leaf = (int64_t)blockIdx.x * 8 + w;
+  if (leaf >= nleaf) return;
+  const int64_t r0 = leaf * 64;
+  cplx a0[KW], a1[KW];   // rows r0 + lane and r0 + 32 + lane
+#pragma unroll
+  for (int c = 0; c < KW; ++c) {
+    const int64_t i0 = r0 + lane, i1 = r0 + 32 + lane;
+    a0[c] = (c < k && i0 < m) ? A[(int64_t)c * lda + i0] : czero();
+    a1[c] = (c < k && i1 < m) ? A[(int64_t)c * lda + i1] : czero();
+  }
+  // R row j lives in lane j's register rj[] after step j (k <= 8 < 32)
+  cplx rrow[KW];
+#pragma unroll
+  for (int c = 0; c < KW; ++c) rrow[c] = czero();
+#pragma unroll
+  for (int j = 0; j < KW; ++j) {
+    if (j < k) {
+      // pivot row j: held by lane j (row j < 32 of the leaf) in a0
+      const cplx alpha = cmk(__shfl_sync(0xffffffffu, a0[j].x, j), __shfl_sync(0xffffffffu, a0[j].y, j));
+      double x2 = (lane > j ? cabs2(a0[j]) : 0.0) + cabs2(a1[j]);
+      x2 = warp_sum(x2);
+      double beta; cplx t, sc;
+      householder_coeffs(alpha, x2, &beta, &t, &sc);
+      // v: v_j = 1 (lane j, a0), v_i = x_i * sc below; rows above j are 0
+      const cplx v0 = (lane == j) ? cmk(1.0, 0.0) : ((lane > j) ? cmul(a0[j], sc) : czero());
+      const cplx v1 = cmul(a1[j], sc);
+      const cplx tc = cconj(t);
+      // columns c > j: s_c = vᴴ a_c, a_c −= conj(τ) v s_c
+#pragma unroll
+      for (int c = 0; c < KW; ++c) {
+        if (c > j && c < k) {
+          cplx sdot = cfmac(v1, a1[c], cfmac(v0, a0[c], czero()));
+          sdot = warp_sum(sdot);
+          const cplx f = cmul(tc, sdot);
+          a0[c] = cfms(v0, f, a0[c]);
+          a1[c] = cfms(v1, f, a1[c]);
+        }
+      }
+      // column j becomes [.., beta at row j, 0 below]
+      if (lane == j) a0[j] = cmk(beta, 0.0);
+      else if (lane > j) a0[j] = czero();
+      a1[j] = czero();
+    }
+  }
+  // R = upper k×k of the leaf (rows 0..k-1 are lanes 0..k-1 of a0)
+#pragma unroll
+  for (int c = 0; c < KW; ++c)
+    if (c < k && lane < k) stack[(int64_t)c * lds + leaf * k + lane] = (lane <= c) ? a0[c] : czero();
+}
+
 // Generic in-global Householder QR factor R of an m×k matrix by one CTA (slow path for
 // wide k).  A is overwritten.  R (k×k, ldr) gets the upper triangle, zeros below.
 __global__ void __launch_bounds__(512) k_house_r_global(int m, int k, cplx* A, int lda, cplx* tau,

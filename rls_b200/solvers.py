@@ -233,6 +233,10 @@ class Engine:
         for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
             setattr(st, f, int(getattr(cst, f)))
 
+    def set_batch(self, max_points: int):
+        """Speculative recycle batch size (1 = plain per-point path)."""
+        check(lib().rls_ctx_set_batch(self._h, int(max_points)), self._h)
+
     def stream_ptr(self) -> int:
         return int(lib().rls_ctx_stream(self._h) or 0)
 

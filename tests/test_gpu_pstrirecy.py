@@ -101,3 +101,28 @@ def test_pstrirecy_laser_small(cuda_device):
     sig, st = R.psTriRecy(R.SchurFactor(T), rec, ctl, verbose=0, X0=X0)
     truth = np.array([dense_sigma_min(C, z) for z in rec.Z])
     assert np.max(np.abs(sig - truth)) <= 1e-4
+
+
+def test_batched_recycle_matches_per_point(sprand_case):
+    """Speculative batches give the sequential loop's results: same σ, same decisions."""
+    C, T, normC, grid = sprand_case
+    n, r = T.shape[0], 6
+    X0 = _x0(n, r, seed=21)
+    grid2 = (0.45, 0.55, 0.0, 0.1, 16, 12, 6)
+    rec = R.recursion_grid(*grid2)
+    ctl = R.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=20, r=r, recy_tau=1.6)
+    out = {}
+    for B in (1, 4, 16):
+        eng = R.Engine(0)
+        eng.set_batch(B)
+        eng.set_schur(T)
+        out[B] = eng.pstrirecy(rec, ctl, X0=X0)
+        eng.close()
+    s1, st1 = out[1]
+    assert np.sum(st1.refine_it == 0) > 0.5 * len(s1)   # the grid exercises recycling
+    for B in (4, 16):
+        sB, stB = out[B]
+        assert np.max(np.abs(sB - s1)) <= 1e-8 * normC
+        assert np.array_equal(stB.refine_it > 0, st1.refine_it > 0)
+        assert np.array_equal(stB.p_count, st1.p_count)
+        assert np.array_equal(stB.r_recy, st1.r_recy)
