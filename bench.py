@@ -46,6 +46,7 @@ METRIC = "σ_min grid pts/s (psTriRecy, sprand N=4000, 200×200 grid, k=20, tol 
 GRID = (0.45, 0.55, 0.0, 0.1, 200, 200, 20)
 N_MAT = 4000
 NORMC = 3.2
+NCU_TRSM_TRAFFIC = 132.53e6 + 3.88e6   # bytes per k_trsm_dataflow launch (ncu, n = 4000)
 
 
 def parse():
@@ -136,6 +137,27 @@ class ClockSampler:
                 "power_w_max": max((num(r[3]) or 0.0) for r in self.rows)}
 
 
+def strip_offset(rank, world, nZ, strip):
+    """First traversal index of this rank's share: the grid's nZ // strip serpentine strips
+    (strip = n_x · k points each) are split into `world` contiguous runs, and rank i starts
+    its own traversal, with its own recycled space, at the first strip of run i."""
+    nstrips = nZ // strip
+    if world > nstrips:
+        raise SystemExit(f"{world} ranks for {nstrips} strips of the grid")
+    return (rank * nstrips // world) * strip
+
+
+def max_over_ranks(x, world, device):
+    """The largest of the ranks' values of x (a time), on every rank."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_baseline(T, rec, ctl, X0, budget_s, min_pts=2):
     """The oracle (CPU restatement) from the start of the traversal, bounded by time."""
     from oracle.pstrirecy import PsTriRecyRun
@@ -223,10 +245,7 @@ def run_ours(args):
         del buf
 
     rec = R.recursion_grid(*GRID)
-    nZ = len(rec.Z)
-    strip = GRID[4] * GRID[6]
-    nstrips = nZ // strip
-    off = (rank * nstrips // world) * strip
+    off = strip_offset(rank, world, len(rec.Z), GRID[4] * GRID[6])
     sub = R.Recursion(*GRID)
     sub.Z = np.ascontiguousarray(rec.Z[off:])
     ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
@@ -288,11 +307,7 @@ def run_ours(args):
     clk.stop()
     if world > 1:
         dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
     timed = slice(args.warmup * s, (args.warmup + args.steps) * s)
     refines = int(np.sum(st.refine_it[timed] > 0))
     prof = {k: eng.profile(k) for k in range(4)}
@@ -309,11 +324,7 @@ def run_ours(args):
         eng2.set_schur(T)
         for k in range(args.warmup + args.steps):
             eng2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sigma2, st2, cst2, X0=X0)
-        el = time.perf_counter() - t0
-        te = torch.tensor([el], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        el = float(te.item())
+        el = max_over_ranks(time.perf_counter() - t0, world, "cuda")
         nsteps = args.warmup + args.steps
         T_bytes = args.n * args.n * 16
         e2e = {"value": world * nsteps * s / el, "unit": "pts/s",
@@ -346,8 +357,11 @@ def run_ours(args):
     top = max((k for k in prof if k != 1), key=lambda k: shares[k])
     cnt, tot_ms, work = prof[top]
     achieved = (work / cnt) / (tot_ms / cnt / 1e3) / 1e9 if cnt else 0.0
+    # DRAM bytes per launch of the TRSM from one ncu capture of this workload (n = 4000, k = 6):
+    # dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_trsm_dataflow_sprand4000.md
+    traffic = NCU_TRSM_TRAFFIC if (top == 0 and args.n == N_MAT) else None
     out["roofline"] = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": hbm_peak,
-                       "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                       "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "launches": cnt, "avg_us": tot_ms / max(cnt, 1) * 1e3}
     out["kernel_time_ms"] = {names[k]: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}

@@ -1,0 +1,64 @@
+"""Host logic of the multi-rank benchmark, on CPU with two `gloo` ranks.
+
+Each rank runs its own traversal of the grid from the first strip of its share, with no
+collective on the data path; the only exchange is the max over ranks of the timings.
+"""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import bench
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from datetime import timedelta
+    from rls_b200.grid import recursion_grid
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        rec = recursion_grid(*bench.GRID)
+        strip = bench.GRID[4] * bench.GRID[6]
+        off = bench.strip_offset(rank, world, len(rec.Z), strip)
+        t = bench.max_over_ranks(10.0 * (rank + 1), world, "cpu")
+        first = rec.Z[off]
+        with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+            json.dump({"off": off, "t": t, "first": [first.real, first.imag]}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2])
+def test_strip_shares_and_max_over_ranks(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
+    strip = bench.GRID[4] * bench.GRID[6]
+    offs = [r["off"] for r in res]
+    assert offs[0] == 0
+    assert all(o % strip == 0 for o in offs)
+    assert offs == sorted(set(offs))                      # distinct, increasing shares
+    assert all(r["t"] == 10.0 * world for r in res)       # every rank sees the slowest rank's time
+    # every rank starts at the corner of its first strip: an x edge of the grid, on the
+    # strip's first row of y
+    x_st, x_ed, y_st, y_ed, n_x, n_y, k = bench.GRID
+    dy = (y_ed - y_st) / (n_y - 1)
+    for r in res:
+        s = r["off"] // strip
+        assert np.isclose(r["first"][0], x_st if s % 2 == 0 else x_ed)
+        assert np.isclose(r["first"][1], y_st + s * k * dy)
+
+
+def test_strip_offset_rejects_more_ranks_than_strips():
+    with pytest.raises(SystemExit):
+        bench.strip_offset(0, 11, 200 * 200, 200 * 20)
