@@ -199,6 +199,33 @@ int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
                           const rls_lobpcg_control* control, rls_c64* X_out,
                           double* sigma_r, double* sigma, int64_t* it);
 
+/* ---- allocation-free utility ---------------------------------------------------- */
+
+/* R (k × k, upper triangular, leading dimension k) of the QR factorisation of the
+ * device block A (m × k, leading dimension lda), by the engine's warp TSQR kernel.
+ * No counterpart in the reference: it exists for callers that must not have this
+ * library allocate device memory — applications whose own pool allocator already
+ * holds the device's free memory, or that call it inside a hot loop where a
+ * cudaMalloc/cudaFree would synchronise the device.  It takes no context and
+ * allocates nothing: its reduction tree lives in a fixed 2.25 MiB device array
+ * inside the library, one per device, reserved when the library's device code
+ * is loaded.
+ *   - Limits: 1 <= m <= 131072, 1 <= k <= 8, lda >= m; anything larger returns
+ *     RLS_ERR_DIM and rls_last_error(NULL) says which limit was hit.
+ *   - A and R are device pointers on the current device.  Unlike the other
+ *     calls, this one only enqueues work on `stream` (a cudaStream_t; NULL is
+ *     the legacy default stream) and returns; R is ready when the stream has
+ *     reached that point.
+ *   - The first call on a device, with that device current, looks up the
+ *     array's address there (cudaGetSymbolAddress); make that first call before
+ *     any stream capture begins on the device.
+ *   - All calls on a device share the one array, and it keeps the last call's
+ *     contents (nothing in it needs to start at zero).  Calls whose work
+ *     overlaps on the GPU — issued on different streams, or from several host
+ *     threads on one stream without ordering — race on it and give wrong
+ *     results; calls in order on one stream are safe. */
+int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int k, rls_c64* R, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

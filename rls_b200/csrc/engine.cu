@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1563,6 +1564,120 @@ extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, dou
   if (count) *count = ctx->kprof[kernel].count;
   if (total_ms) *total_ms = ctx->kprof[kernel].ms;
   if (work) *work = ctx->kprof[kernel].bytes;
+  return RLS_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Allocation-free R factor of a tall, narrow block.
+//
+// Some callers cannot let this library allocate device memory: an application whose own
+// pool allocator (PyTorch's caching allocator, CUDA.jl's memory pool) already holds the
+// free device memory, or one that orthogonalises a block inside a hot loop, where
+// cudaMalloc/cudaFree would synchronise the device and stall its other streams.  For
+// them the reduction tree of the warp TSQR lives in the file-scope array below, a
+// fixed 2.25 MiB of device memory reserved when the library's device code is loaded.
+// No context is involved, so nothing else is allocated either.
+//
+// Every call on a device shares this one array, and it keeps what the last call wrote.
+// Nothing in it has to start at zero: each level of the tree writes every element that
+// the next level reads.  Two calls whose work overlaps on the GPU (different streams
+// of one device, or the same stream used from two host threads without ordering) race
+// on the array and return wrong R factors; calls in order on one stream are safe.
+// ------------------------------------------------------------------------------------
+#define RLS_NOALLOC_MAX_ROWS 131072
+#define RLS_NOALLOC_MAX_COLS 8
+#define RLS_NOALLOC_MAX_DEVICES 64
+// Level 0 of the tree holds one k×k R per 64-row leaf: ceil(m/64)·k² ≤ MAX_ROWS elements
+// (k ≤ 8, MAX_ROWS a multiple of 64).  Level 1 reduces those ceil(m/64)·k ≤ MAX_ROWS/8
+// rows the same way into ≤ MAX_ROWS/8 elements; deeper levels alternate between the two
+// halves and are smaller still.  Total 147456 complex values = 2.25 MiB.
+#define RLS_NOALLOC_STACK0 ((size_t)RLS_NOALLOC_MAX_ROWS)
+#define RLS_NOALLOC_STACK1 ((size_t)RLS_NOALLOC_MAX_ROWS / 8)
+
+static __device__ __align__(256) cplx g_noalloc_tsqr_scratch[RLS_NOALLOC_STACK0 + RLS_NOALLOC_STACK1];
+
+namespace {
+std::mutex g_noalloc_mu;
+cplx* g_noalloc_ptr[RLS_NOALLOC_MAX_DEVICES] = {};
+
+void noalloc_fail(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_create_err = buf;
+}
+}  // namespace
+
+extern "C" int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int k, rls_c64* R, void* stream) {
+  if (!A || !R) {
+    noalloc_fail("rls_tsqr_r_noalloc: A and R must be device pointers, got NULL");
+    return RLS_ERR_ARG;
+  }
+  if (m < 1 || m > RLS_NOALLOC_MAX_ROWS || k < 1 || k > RLS_NOALLOC_MAX_COLS) {
+    noalloc_fail("rls_tsqr_r_noalloc: %lld x %d block exceeds the fixed scratch (1 <= m <= %d rows, "
+                 "1 <= k <= %d columns)",
+                 (long long)m, k, RLS_NOALLOC_MAX_ROWS, RLS_NOALLOC_MAX_COLS);
+    return RLS_ERR_DIM;
+  }
+  if (lda < m) {
+    noalloc_fail("rls_tsqr_r_noalloc: lda = %lld is smaller than m = %lld", (long long)lda, (long long)m);
+    return RLS_ERR_DIM;
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= RLS_NOALLOC_MAX_DEVICES) {
+    noalloc_fail("rls_tsqr_r_noalloc: no usable current device (%s)", cudaGetErrorString(e));
+    return RLS_ERR_CUDA;
+  }
+  cplx* scratch;
+  {
+    // set-up, once per device, with that device current: the scratch array's address
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_tsqr_scratch);
+      if (e != cudaSuccess || !p) {
+        noalloc_fail("rls_tsqr_r_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                     cudaGetErrorString(e));
+        return RLS_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = static_cast<cplx*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cplx* stack[2] = {scratch, scratch + RLS_NOALLOC_STACK0};
+  const size_t cap[2] = {RLS_NOALLOC_STACK0, RLS_NOALLOC_STACK1};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const cplx* src = reinterpret_cast<const cplx*>(A);
+  int64_t rows = m, ld = lda;
+  int which = 0;
+  while (true) {
+    const int64_t nleaf = (rows + 63) / 64;
+    const bool last = nleaf == 1;
+    cplx* dst = last ? reinterpret_cast<cplx*>(R) : stack[which];
+    const int64_t ldd = last ? k : nleaf * k;
+    if (!last && (size_t)nleaf * k * k > cap[which]) {  // unreachable within the limits above
+      noalloc_fail("rls_tsqr_r_noalloc: reduction level of %lld rows does not fit the scratch", (long long)rows);
+      return RLS_ERR_DIM;
+    }
+    const unsigned nblk = (unsigned)((nleaf + 7) / 8);
+    if (k <= 4)
+      k_tsqr_warp<4><<<nblk, 256, 0, st>>>(rows, k, src, ld, dst, ldd, nleaf);
+    else
+      k_tsqr_warp<8><<<nblk, 256, 0, st>>>(rows, k, src, ld, dst, ldd, nleaf);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      noalloc_fail("rls_tsqr_r_noalloc: launch failed: %s", cudaGetErrorString(e));
+      return RLS_ERR_CUDA;
+    }
+    if (last) break;
+    src = dst;
+    rows = nleaf * k;
+    ld = rows;
+    which ^= 1;
+  }
   return RLS_OK;
 }
 
