@@ -311,6 +311,7 @@ def run_ours(args):
     timed = slice(args.warmup * s, (args.warmup + args.steps) * s)
     refines = int(np.sum(st.refine_it[timed] > 0))
     prof = {k: eng.profile(k) for k in range(4)}
+    waits = eng.profile(4)
 
     # end to end through the public C ABI on a fresh context, host buffers in and out
     e2e = None
@@ -365,6 +366,7 @@ def run_ours(args):
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "launches": cnt, "avg_us": tot_ms / max(cnt, 1) * 1e3}
     out["kernel_time_ms"] = {names[k]: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}
+    out["host_waits"] = {"count": waits[0], "ms": waits[1], "per_step": waits[0] / args.steps}
     if prof[1][0]:
         c1, t1, f1 = prof[1]
         out["heev_fp64"] = {"gflops": f1 / (t1 / 1e3) / 1e9, "launches": c1, "avg_us": t1 / c1 * 1e3}

@@ -7,8 +7,9 @@
  *   - complex values are rls_c64 {re, im} (layout of Julia ComplexF64 and of
  *     C99 double complex); matrices are column-major with a leading dimension;
  *   - grid indices and permutations are 1-based, as in the Julia API;
- *   - calls are synchronous; no exceptions cross the ABI; a negative return is
- *     an rls_status and rls_last_error() gives the message;
+ *   - calls are synchronous (rls_tsqr_r_noalloc only enqueues; see there); no
+ *     exceptions cross the ABI; a negative return is an rls_status and
+ *     rls_last_error() gives the message;
  *   - the library never frees or retains caller memory.
  */
 #ifndef RLS_B200_H
@@ -133,8 +134,10 @@ int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always);
 /* Per-kernel CUDA-event timing: kernel 0 = triangular solve, 1 = projected
  * eigensolve, 2 = recycle-step streaming product, 3 = triangular multiply.
  * set_profile resets the counters; profile_get returns launches, total device
- * milliseconds and algorithmic work (bytes; flops for kernel 1).  No reference
- * counterpart (the reference times phases with time_ns, psTriRecy.jl:306-309). */
+ * milliseconds and algorithmic work (bytes; flops for kernel 1).  kernel 4
+ * returns the host's blocking waits on the stream instead: their number and
+ * total wall milliseconds (work = 0).  No reference counterpart (the reference
+ * times phases with time_ns, psTriRecy.jl:306-309). */
 int rls_ctx_set_profile(rls_ctx* ctx, int on);
 int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work);
 

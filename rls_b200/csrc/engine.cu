@@ -110,6 +110,13 @@ struct rls_ctx {
     double thresh = 0.0;
   } run;
 
+  // pinned host staging for device→host reads (one stream synchronisation per read batch)
+  unsigned char* hstage = nullptr;
+  int* hstage_err = nullptr;
+  // blocking host waits on the stream, counted while profiling
+  int64_t host_waits = 0;
+  double host_wait_ms = 0.0;
+
   // optional per-kernel event timing (rls_ctx_set_profile)
   bool profile = false;
   int64_t launches = 0;            // kernel launches issued by this context
@@ -232,13 +239,20 @@ void prof_resolve(rls_ctx* ctx) {
   }
 }
 
+// Waits for the stream and reads the device error word through the pinned staging area
+// (one round trip).  Every device→host read of the engine ends here.
 int sync_and_check(rls_ctx* ctx) {
+  const auto t0 = std::chrono::steady_clock::now();
+  CK(cudaMemcpyAsync(ctx->hstage_err, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (ctx->profile) prof_resolve(ctx);
-  int h = 0;
-  CK(cudaMemcpy(&h, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (ctx->profile) {
+    ctx->host_waits += 1;
+    ctx->host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    prof_resolve(ctx);
+  }
+  const int h = *ctx->hstage_err;
   if (h) {
-    CK(cudaMemset(ctx->derr, 0, sizeof(int)));
+    CK(cudaMemsetAsync(ctx->derr, 0, sizeof(int), ctx->stream));
     if (h & DEVERR_SPIN_TIMEOUT) {
       set_err(ctx, "a bounded device wait expired in the triangular solve");
       return RLS_ERR_TIMEOUT;
@@ -256,10 +270,49 @@ int sync_and_check(rls_ctx* ctx) {
   return RLS_OK;
 }
 
+constexpr size_t kStageBytes = 64 * 1024;   // pinned staging area (plus the error word)
+
+// Up to a few device→host reads gathered into one round trip through the pinned staging
+// area; reads that do not fit go straight to their pageable destination.
+struct D2HBatch {
+  rls_ctx* ctx;
+  size_t used = 0;
+  struct Item { void* h; size_t off, bytes; };
+  Item items[8];
+  int n = 0;
+  explicit D2HBatch(rls_ctx* c) : ctx(c) {}
+  template <class T>
+  int add(T* h, const T* d, size_t count) {
+    const size_t bytes = count * sizeof(T);
+    if (n < 8 && used + bytes <= kStageBytes) {
+      CK(cudaMemcpyAsync(ctx->hstage + used, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      items[n++] = {h, used, bytes};
+      used += (bytes + 15) & ~size_t(15);
+    } else {
+      CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    return RLS_OK;
+  }
+  int finish() {
+    RET(sync_and_check(ctx));
+    for (int i = 0; i < n; ++i) std::memcpy(items[i].h, ctx->hstage + items[i].off, items[i].bytes);
+    return RLS_OK;
+  }
+};
+
 template <class T>
 int d2h(rls_ctx* ctx, T* h, const T* d, size_t count) {
-  CK(cudaMemcpyAsync(h, d, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
-  return sync_and_check(ctx);
+  D2HBatch b(ctx);
+  RET(b.add(h, d, count));
+  return b.finish();
+}
+
+template <class T, class U>
+int d2h2(rls_ctx* ctx, T* h1, const T* d1, size_t n1, U* h2, const U* d2, size_t n2) {
+  D2HBatch b(ctx);
+  RET(b.add(h1, d1, n1));
+  RET(b.add(h2, d2, n2));
+  return b.finish();
 }
 
 // ---------------------------------------------------------------------------------
@@ -718,9 +771,8 @@ int lobpcg_invtri(rls_ctx* ctx, cplx z, int r, int64_t maxit, double tol, bool s
     double w0 = 0.0;
     RET(residual(W, &w0));
     double hs[2];
-    RET(d2h(ctx, hs, ctx->dscal, 1));
     double s0;
-    RET(d2h(ctx, &s0, ctx->sig, 1));
+    RET(d2h2(ctx, hs, ctx->dscal, 1, &s0, ctx->sig, 1));
     const double wn = std::sqrt(hs[0]);
     // check_conv_svd, side 'L' (lobpcgSvd.jl:329-331): |W[:,1]| < tol
     if (wn < tol) {
@@ -860,8 +912,7 @@ int update_recycled_space(rls_ctx* ctx, cplx z, const cplx* X, double tau, bool 
     RET(copy_cols(ctx, X, x, 1));
     RET(orth_robust(ctx, np, ctx->V, np, pr, x, np, 1, ctx->owW, ctx->owR));
     std::vector<cplx> c((size_t)pr + 1);
-    RET(d2h(ctx, c.data(), ctx->owW, (size_t)pr));
-    RET(d2h(ctx, c.data() + pr, ctx->owR, 1));
+    RET(d2h2(ctx, c.data(), ctx->owW, (size_t)pr, c.data() + pr, ctx->owR, 1));
     const double rho2 = c[pr].x * c[pr].x + c[pr].y * c[pr].y;
     const double res0 = std::sqrt(rho2);
     int l = 0;
@@ -960,8 +1011,7 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   k_sum<<<1, 256, 0, ctx->stream>>>(ctx->colpart, nparts, ctx->dscal);
   RET(check_launch(ctx, "k_sum"));
   double w2 = 0.0, s0 = 0.0;
-  RET(d2h(ctx, &w2, ctx->dscal, 1));
-  RET(d2h(ctx, &s0, ctx->sig_rec, 1));
+  RET(d2h2(ctx, &w2, ctx->dscal, 1, &s0, ctx->sig_rec, 1));
   out->rr = rr;
   out->sigma0 = s0;
   out->w0norm = std::sqrt(w2);
@@ -1034,10 +1084,13 @@ int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, doubl
   k_batch_w0<<<B, 256, 0, ctx->stream>>>(d);
   RET(check_launch(ctx, "k_batch_w0"));
   std::vector<double> hs((size_t)B * BATCH_KMAX), hw0(B);
-  CK(cudaMemcpyAsync(rr, ctx->brr, sizeof(int) * B, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(hs.data(), ctx->bsig, sizeof(double) * B * BATCH_KMAX, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(hw0.data(), ctx->bw0, sizeof(double) * B, cudaMemcpyDeviceToHost, ctx->stream));
-  RET(sync_and_check(ctx));
+  {
+    D2HBatch rd(ctx);
+    RET(rd.add(rr, ctx->brr, (size_t)B));
+    RET(rd.add(hs.data(), ctx->bsig, (size_t)B * BATCH_KMAX));
+    RET(rd.add(hw0.data(), ctx->bw0, (size_t)B));
+    RET(rd.finish());
+  }
   for (int b = 0; b < B; ++b) {
     if (rr[b] < 1 || rr[b] > BATCH_KMAX) rr[b] = 0;
     sig0[b] = hs[(size_t)b * BATCH_KMAX];
@@ -1165,6 +1218,12 @@ extern "C" int rls_ctx_create(rls_ctx** out, int device) {
     return RLS_ERR_CUDA;
   }
   int st = set_kernel_attrs(ctx);
+  if (st == RLS_OK && cudaHostAlloc((void**)&ctx->hstage, kStageBytes + 64, cudaHostAllocDefault) != cudaSuccess) {
+    ctx->hstage = nullptr;
+    set_err(ctx, "pinned host staging allocation failed");
+    st = RLS_ERR_NOMEM;
+  }
+  if (st == RLS_OK) ctx->hstage_err = reinterpret_cast<int*>(ctx->hstage + kStageBytes);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->derr, 4);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->dscal, 256);
   if (st != RLS_OK) {
@@ -1183,6 +1242,7 @@ extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
   for (auto& b : ctx->owned) cudaFree(b.p);
   ctx->owned.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->hstage) cudaFreeHost(ctx->hstage);
   delete ctx;
 }
 
@@ -1549,6 +1609,8 @@ extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
   if (!ctx) return RLS_ERR_ARG;
   RET(sync_and_check(ctx));
   ctx->profile = on != 0;
+  ctx->host_waits = 0;
+  ctx->host_wait_ms = 0.0;
   for (auto& k : ctx->kprof) {
     k.count = 0;
     k.ms = 0.0;
@@ -1558,9 +1620,15 @@ extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
 }
 
 extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work) {
-  if (!ctx || kernel < 0 || kernel > 3) return RLS_ERR_ARG;
+  if (!ctx || kernel < 0 || kernel > 4) return RLS_ERR_ARG;
   RET(sync_and_check(ctx));
   prof_resolve(ctx);
+  if (kernel == 4) {
+    if (count) *count = ctx->host_waits;
+    if (total_ms) *total_ms = ctx->host_wait_ms;
+    if (work) *work = 0.0;
+    return RLS_OK;
+  }
   if (count) *count = ctx->kprof[kernel].count;
   if (total_ms) *total_ms = ctx->kprof[kernel].ms;
   if (work) *work = ctx->kprof[kernel].bytes;
