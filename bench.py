@@ -46,7 +46,7 @@ METRIC = "σ_min grid pts/s (psTriRecy, sprand N=4000, 200×200 grid, k=20, tol 
 GRID = (0.45, 0.55, 0.0, 0.1, 200, 200, 20)
 N_MAT = 4000
 NORMC = 3.2
-NCU_TRSM_TRAFFIC = 132.53e6 + 3.88e6   # bytes per k_trsm_dataflow launch (ncu, n = 4000)
+NCU_TRSM_TRAFFIC = None   # bytes per k_trsm_half launch from an ncu capture (n = 4000); None until captured
 
 
 def parse():
@@ -346,7 +346,7 @@ def run_ours(args):
     out["gpu_launches"] = int(l1 - l0)
     out["clocks"] = clk.summary()
     # roofline of the dominant profiled kernel
-    names = {0: "k_trsm_dataflow (R⁻¹/R⁻ᴴ on T−zI)", 1: "k_heev_rr (projected eigensolve)",
+    names = {0: "k_trsm_half (R⁻¹/R⁻ᴴ on T−zI, block-row scaled factor)", 1: "k_heev_rr (projected eigensolve)",
              2: "k_gemm_rows (recycle X/W product)", 3: "k_trmm_partial+reduce (T·V, Tᴴ·[J5 V])"}
     peaks = {}
     try:
@@ -359,7 +359,7 @@ def run_ours(args):
     cnt, tot_ms, work = prof[top]
     achieved = (work / cnt) / (tot_ms / cnt / 1e3) / 1e9 if cnt else 0.0
     # DRAM bytes per launch of the TRSM from one ncu capture of this workload (n = 4000, k = 6):
-    # dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_trsm_dataflow_sprand4000.md
+    # dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_trsm_half_sprand4000.md
     traffic = NCU_TRSM_TRAFFIC if (top == 0 and args.n == N_MAT) else None
     out["roofline"] = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": hbm_peak,
                        "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,

@@ -163,10 +163,11 @@ __global__ void __launch_bounds__(256) k_gemm_rows(int64_t nrows, CombSrc src, i
 __device__ __forceinline__ void load_tile(cplx* sT, const cplx* __restrict__ tp, int adj) {
   for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
     const int rr = t % TILE, cc = t / TILE;
-    const cplx v = tp[t];
-    if (!adj) sT[cc * TILE_LDS + rr] = v;   // element (rr, cc) at column cc
-    else sT[rr * TILE_LDS + cc] = v;        // element (rr, cc) at "column" rr
+    cp_async16(adj ? &sT[rr * TILE_LDS + cc]     // element (rr, cc) at "column" rr
+                   : &sT[cc * TILE_LDS + rr],    // element (rr, cc) at column cc
+               &tp[t]);
   }
+  cp_async_wait_all();
 }
 
 // acc[c] += (adj ? Tᴴ : T)[row, inner-range] · sX[inner-range, c]; the inner dimension is
@@ -250,16 +251,17 @@ __global__ void k_trmm_reduce(int nb, int k, const int* __restrict__ O_first, co
   }
 }
 
-// ------------------------------------------------------------------------------------
-// Inverse of each shifted diagonal tile D_I = T_II − z·I (upper triangular), rows
-// beyond n set to the identity.  One CTA (256 threads) per tile; right-looking
-// back substitution on all 64 right-hand sides at once.
-// ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_diag_inv(int nb, int64_t n, const cplx* __restrict__ T, cplx z,
+// Inverses D_b⁻¹ of the diagonal tiles of R = T − zI, one CTA per tile (512 threads).
+// Warp w solves U y = e_j for the columns j ∈ {w, 31−w, 32+w, 63−w} (equal work per
+// warp) by column-oriented back substitution: lane i holds rows i and i+32 of the
+// right-hand side, y_l is broadcast by shuffle and every lane updates its rows < l.
+// Pad rows (global row ≥ n) get 1 on the diagonal, so the pad stays inert.
+// Dynamic shared memory: TILE·TILE_LDS cplx.
+__global__ void __launch_bounds__(512) k_diag_inv(int nb, int64_t n, const cplx* __restrict__ T, cplx z,
                                                   cplx* __restrict__ Dinv, int* err) {
   extern __shared__ cplx sm[];
-  cplx* sU = sm;                    // TILE*TILE
-  cplx* sY = sm + TILE * TILE;      // TILE*TILE
+  cplx* sU = sm;                    // U[r][c] at sU[c*TILE_LDS + r], zero below the diagonal
+  __shared__ cplx sdi[TILE];        // 1 / U[i][i]
   const int I = blockIdx.x;
   const cplx* tp = T + tile_index(I, I) * (TILE * TILE);
   for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
@@ -267,71 +269,119 @@ __global__ void __launch_bounds__(256) k_diag_inv(int nb, int64_t n, const cplx*
     const int64_t g = (int64_t)I * TILE + rr;
     cplx u = tp[t];
     if (rr == cc) u = (g < n) ? csub(u, z) : cmk(1.0, 0.0);
-    sU[t] = (rr <= cc) ? u : czero();
-    sY[t] = (rr == cc) ? cmk(1.0, 0.0) : czero();
+    sU[cc * TILE_LDS + rr] = (rr <= cc) ? u : czero();
   }
   __syncthreads();
-  for (int i = TILE - 1; i >= 0; --i) {
-    const cplx dinv = cinv(sU[i * TILE + i]);
-    // row i of Y: columns c >= i
-    for (int c = i + threadIdx.x; c < TILE; c += blockDim.x) sY[c * TILE + i] = cmul(sY[c * TILE + i], dinv);
-    __syncthreads();
-    // rows l < i: Y[l, c] -= U[l, i] * Y[i, c]  (c >= i)
-    const int nl = i, ncol = TILE - i;
-    for (int t = threadIdx.x; t < nl * ncol; t += blockDim.x) {
-      const int l = t % nl, c = i + t / nl;
-      sY[c * TILE + l] = cfms(sU[i * TILE + l], sY[c * TILE + i], sY[c * TILE + l]);
-    }
-    __syncthreads();
-  }
+  if (threadIdx.x < TILE) sdi[threadIdx.x] = cinv(sU[threadIdx.x * TILE_LDS + threadIdx.x]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   bool bad = false;
-  for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
-    const cplx y = sY[t];
-    if (!isfinite(y.x) || !isfinite(y.y)) bad = true;
-    Dinv[(int64_t)I * TILE * TILE + t] = y;
+  const int cols[4] = {w, 31 - w, 32 + w, 63 - w};
+  cplx* out = Dinv + (int64_t)I * TILE * TILE;
+  for (int q = 0; q < 4; ++q) {
+    const int j = cols[q];
+    cplx y0 = (lane == j) ? cmk(1.0, 0.0) : czero();        // row lane
+    cplx y1 = (lane + 32 == j) ? cmk(1.0, 0.0) : czero();   // row lane + 32
+    for (int l = j; l >= 0; --l) {
+      const int src = l & 31;
+      const cplx mine = (l >= 32) ? y1 : y0;
+      const cplx rl = cmk(__shfl_sync(0xffffffffu, mine.x, src), __shfl_sync(0xffffffffu, mine.y, src));
+      const cplx yl = cmul(rl, sdi[l]);
+      if (lane == src) {
+        if (l >= 32) y1 = yl;
+        else y0 = yl;
+      }
+      if (lane < l) y0 = cfms(sU[l * TILE_LDS + lane], yl, y0);
+      if (lane + 32 < l) y1 = cfms(sU[l * TILE_LDS + lane + 32], yl, y1);
+    }
+    if (!isfinite(y0.x) || !isfinite(y0.y) || !isfinite(y1.x) || !isfinite(y1.y)) bad = true;
+    out[j * TILE + lane] = y0;
+    out[j * TILE + lane + 32] = y1;
   }
   if (bad) atomicOr(err, DEVERR_NONFINITE);
 }
 
-// E tiles for the last step of the dataflow solve, per shift:
-//   adj = 0: E_b = D_b⁻¹ T(b, b+1)        (b < nb-1)
-//   adj = 1: E_b = D_b⁻ᴴ T(b-1, b)ᴴ       (b > 0)
-// so that X_b = D_b⁻¹ acc − E_b X_{b±1} needs one tile product after the last wait.
-// grid (nb, 2); one CTA computes one 64×64×64 complex product from shared memory.
-__global__ void __launch_bounds__(256) k_trsm_etiles(int nb, const cplx* __restrict__ T,
-                                                     const cplx* __restrict__ Dinv, cplx* __restrict__ E) {
+// Block-row scaled factor of the shifted solve: G(I, J) = D_I⁻¹ · T(I, J) for every tile
+// J > I, stored in the packed tile layout of T (diagonal slots unused).  With
+// R = D·(I + G) the solves need no D⁻¹ product on their dependency chain:
+//   R x = b   ⇔  x_b = D_b⁻¹ b_b − Σ_{J>b} G(b,J) x_J
+//   Rᴴ x = b  ⇔  u_b = b_b − Σ_{J<b} G(J,b)ᴴ u_J,  x_b = D_b⁻ᴴ u_b.
+// Grid: two CTAs per tile slot (nb(nb+1)/2 slots), CTA h computing output rows
+// [32h, 32h+32); 256 threads.  Warp w owns the four rows 4w..4w+3 (A values broadcast),
+// lane the columns lane and lane+32.  D_I⁻¹ is upper triangular, so warp w sums only
+// l ≥ 32h + 4w (a warp-uniform start).  The result is staged in shared memory and
+// written out coalesced.
+// Dynamic shared memory (scale_smem_bytes): 64×33 + 64×65 cplx, two CTAs per SM.
+#define SC_ALD 33
+__global__ void __launch_bounds__(256) k_trsm_scale(const cplx* __restrict__ T, const cplx* __restrict__ Dinv,
+                                                    cplx* __restrict__ G) {
   extern __shared__ cplx sm[];
-  cplx* sD = sm;                  // TILE*TILE (column-major)
-  cplx* sT = sm + TILE * TILE;    // TILE*TILE
-  const int b = blockIdx.x, adj = blockIdx.y;
-  cplx* out = E + ((int64_t)adj * nb + b) * TILE * TILE;
-  if ((!adj && b == nb - 1) || (adj && b == 0)) return;
-  const cplx* dp = Dinv + (int64_t)b * TILE * TILE;
-  const cplx* tp = adj ? T + tile_index(b - 1, b) * (TILE * TILE) : T + tile_index(b, b + 1) * (TILE * TILE);
-  for (int q = threadIdx.x; q < TILE * TILE; q += blockDim.x) { sD[q] = dp[q]; sT[q] = tp[q]; }
+  cplx* sA = sm;                      // D⁻¹[32h + i][l] at sA[l*SC_ALD + i]
+  cplx* sB = sm + TILE * SC_ALD;      // T[l][c] at sB[c*TILE_LDS + l]; output staging afterwards
+  const int64_t idx = blockIdx.x >> 1;
+  const int h = blockIdx.x & 1;
+  int J = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+  while ((int64_t)J * (J + 1) / 2 > idx) --J;
+  while ((int64_t)(J + 1) * (J + 2) / 2 <= idx) ++J;
+  const int I = (int)(idx - (int64_t)J * (J + 1) / 2);
+  if (I >= J) return;
+  const cplx* dp = Dinv + (int64_t)I * TILE * TILE;
+  const cplx* tp = T + idx * (TILE * TILE);
+  for (int q = threadIdx.x; q < 32 * TILE; q += blockDim.x) {
+    const int r = q % 32, l = q / 32;
+    cp_async16(&sA[l * SC_ALD + r], &dp[l * TILE + h * 32 + r]);
+  }
+  for (int q = threadIdx.x; q < TILE * TILE; q += blockDim.x) {
+    const int r = q % TILE, c = q / TILE;
+    cp_async16(&sB[c * TILE_LDS + r], &tp[q]);
+  }
+  cp_async_wait_all();
   __syncthreads();
-  // thread: row i = tid % 64, columns c = tid/64 + 4·m
-  const int i = threadIdx.x & 63, c0 = threadIdx.x >> 6;
-  for (int c = c0; c < TILE; c += 4) {
-    cplx s = czero();
-    if (!adj) {
-      for (int l = 0; l < TILE; ++l) s = cfma(sD[l * TILE + i], sT[c * TILE + l], s);          // D⁻¹[i,l]·T[l,c]
-    } else {
-      for (int l = 0; l < TILE; ++l) s = cfma(cconj(sD[i * TILE + l]), cconj(sT[l * TILE + c]), s);  // D⁻ᴴ[i,l]·Tᴴ[l,c]
-    }
-    out[c * TILE + i] = s;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  cplx acc[4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) { acc[a][0] = czero(); acc[a][1] = czero(); }
+  for (int l = 32 * h + 4 * w; l < TILE; ++l) {
+    cplx av[4], bv[2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) av[a] = sA[l * SC_ALD + 4 * w + a];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) bv[c] = sB[(lane + 32 * c) * TILE_LDS + l];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) acc[a][c] = cfma(av[a], bv[c], acc[a][c]);
+  }
+  __syncthreads();   // sB is reused for the output block (32 rows × 64 columns, ld 33)
+  cplx* sO = sB;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) sO[(lane + 32 * c) * SC_ALD + 4 * w + a] = acc[a][c];
+  __syncthreads();
+  cplx* out = G + idx * (TILE * TILE);
+  for (int q = threadIdx.x; q < 32 * TILE; q += blockDim.x) {
+    const int r = q % 32, c = q / 32;
+    out[c * TILE + h * 32 + r] = sO[c * SC_ALD + r];
   }
 }
 
+inline size_t scale_smem_bytes() { return ((size_t)TILE * SC_ALD + (size_t)TILE * TILE_LDS) * sizeof(cplx); }
+
 // ------------------------------------------------------------------------------------
-// Dataflow triangular solve with the shifted Schur factor R = T − zI.
-//   adj = 0: R X = B   (back substitution, tiles of block row I, J > I)
-//   adj = 1: Rᴴ X = B  (forward substitution, tiles of block column J, I < J)
-// One CTA per tile row; CTAs take row blocks by ticket in dependency order, so a
-// CTA only ever waits on blocks owned by CTAs that started before it.  Each wait
-// is bounded by RLS_SPIN_LIMIT polls; on expiry the CTA records DEVERR_SPIN_TIMEOUT
-// and finishes with whatever it has, so the launch always terminates.
-// X may alias B.  k <= 24.
+// Dataflow triangular solve on the scaled factor (k_trsm_scale), half block rows.
+//   adj = 0: R x = b   → x_b = D_b⁻¹ b_b − Σ_{J>b} G(b,J) x_J, written to X;
+//   adj = 1: Rᴴ x = b  → u_b = b_b − Σ_{J<b} G(J,b)ᴴ u_J, written to U; k_trsm_finish
+//            then forms X = D⁻ᴴ U block by block.
+// Two CTAs per 64-row block, each owning 32 rows (grid 2·nb, 256 threads), taken by
+// ticket in dependency order: a CTA only waits on the two halves of blocks owned by
+// CTAs that started before it, so every wait ends even when not all CTAs are resident.
+// Waits are bounded by RLS_SPIN_LIMIT polls; on expiry the CTA records
+// DEVERR_SPIN_TIMEOUT and carries on, so the launch always terminates.  Each
+// dependency costs one 32×64×k product; the next tile is prefetched into registers
+// while the current dependency is awaited and applied.  Published halves carry an
+// epoch in flags[2·block + half] (st.release / ld.acquire at gpu scope).  X must not
+// alias B.  K (the number of columns, 1..8) is a template parameter.
 // ------------------------------------------------------------------------------------
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -342,116 +392,160 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Shared memory: 2·TILE·TILE_LDS (tile, diagonal inverse) + (2 + NG)·TILE·k cplx.
-// All dependencies but the last are subtracted from the right-hand side as they
-// arrive; y = D_b⁻¹·acc is then formed before waiting for the last one, which enters
-// through the precomputed E_b (k_trsm_etiles): X_b = y − E_b·X_last.  E_b is stored
-// like a tile of T with adj = 0 semantics, so it is loaded untransposed.
-template <int KMAX, int NG>
-__global__ void __launch_bounds__(64 * NG) k_trsm_dataflow(int nb, const cplx* __restrict__ T,
-                                                          const cplx* __restrict__ Dinv,
-                                                          const cplx* __restrict__ E, const cplx* B,
-                                                          cplx* X, int64_t ldx, int k, int adj,
-                                                          int* __restrict__ ticket, int* flags, int epoch,
-                                                          int* err) {
+#define HT_LDS 33   // shared-memory leading dimension of a 32-row half tile
+
+// Prefetch of a 32×64 half tile into registers (8 values per thread of 256):
+//   trans = 0: A[r][jj] = M[h*32 + r][jj]          (M column-major 64×64)
+//   trans = 1: A[r][jj] = conj(M[jj][h*32 + r])
+struct HalfTile {
+  cplx v[8];
+  __device__ __forceinline__ void load(const cplx* __restrict__ M, int h, int trans) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = i * 256 + threadIdx.x;
+      v[i] = trans ? M[(h * 32 + idx / 64) * TILE + (idx % 64)] : M[(idx / 32) * TILE + h * 32 + (idx % 32)];
+    }
+  }
+  __device__ __forceinline__ void store(cplx* sA, int trans) const {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = i * 256 + threadIdx.x;
+      if (trans) sA[(idx % 64) * HT_LDS + idx / 64] = cconj(v[i]);
+      else sA[(idx / 32) * HT_LDS + (idx % 32)] = v[i];
+    }
+  }
+};
+
+// sAcc[c][r] (op)= Σ_jj A[r][jj]·sX[c][jj] for the 32×64 half tile in sA and exactly K
+// columns: warp w sums jj ∈ [8w, 8w+8) for row = lane, and the eight partial sums are
+// combined through sPart.  op: 0 set, 1 subtract.  Starts and ends with the block
+// synchronised.
+template <int K>
+__device__ __forceinline__ void half_product(const cplx* sA, const cplx* sX, cplx* sPart, cplx* sAcc, int op) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  cplx acc[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) acc[c] = czero();
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int jj = w * 8 + q;
+    const cplx a = sA[jj * HT_LDS + lane];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = cfma(a, sX[c * TILE + jj], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < K; ++c) sPart[(w * K + c) * 32 + lane] = acc[c];
+  __syncthreads();
+  if (threadIdx.x < 32 * K) {
+    const int r = threadIdx.x & 31, c = threadIdx.x >> 5;
+    cplx v = sPart[c * 32 + r];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) v = cadd(v, sPart[(q * K + c) * 32 + r]);
+    sAcc[c * 32 + r] = op ? csub(sAcc[c * 32 + r], v) : v;
+  }
+  __syncthreads();
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_trsm_half(int nb, const cplx* __restrict__ G, const cplx* __restrict__ Dinv,
+                                                   const cplx* __restrict__ B, cplx* __restrict__ X, cplx* U,
+                                                   int64_t ldx, int adj, int* __restrict__ ticket, int* flags,
+                                                   int epoch, int* err) {
   extern __shared__ cplx sm[];
-  cplx* sT = sm;                         // TILE*TILE_LDS
-  cplx* sD = sT + TILE * TILE_LDS;       // TILE*TILE_LDS: this block's diagonal inverse
-  cplx* sX = sD + TILE * TILE_LDS;       // TILE*k (dependency block)
-  cplx* sAcc = sX + TILE * k;            // TILE*k (running right-hand side)
-  cplx* sPart = sAcc + TILE * k;         // NG × TILE*k partial products
+  cplx* sA = sm;                       // TILE·HT_LDS
+  cplx* sX = sA + TILE * HT_LDS;       // TILE·K
+  cplx* sAcc = sX + TILE * K;          // 32·K
+  cplx* sPart = sAcc + 32 * K;         // 8·K·32
   __shared__ int sblk;
   if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
   __syncthreads();
-  const int t = sblk;
-  const int b = adj ? t : (nb - 1 - t);
-  const int row = threadIdx.x & (TILE - 1), grp = threadIdx.x >> 6;
-  load_tile(sD, Dinv + (int64_t)b * TILE * TILE, adj);
-  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
-    const int rr = q % TILE, c = q / TILE;
-    sAcc[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
+  const int pos = sblk >> 1, h = sblk & 1;
+  const int b = adj ? pos : (nb - 1 - pos);
+  const int64_t r0 = (int64_t)b * TILE + h * 32;   // first row of this half
+  cplx* out = adj ? U : X;                          // where the chain's values live
+  const int ndep = adj ? b : (nb - 1 - b);
+  HalfTile pf;
+  auto dep_of = [&](int d) { return adj ? d : (nb - 1 - d); };
+  auto tile_of = [&](int dep) {
+    return adj ? G + tile_index(dep, b) * (TILE * TILE) : G + tile_index(b, dep) * (TILE * TILE);
+  };
+  if (ndep > 0) pf.load(tile_of(dep_of(0)), h, adj);
+  // start value: D_b⁻¹ b_b (forward) or b_b (adjoint) on this half's rows
+  if (!adj) {
+    HalfTile dt;
+    dt.load(Dinv + (int64_t)b * TILE * TILE, h, 0);
+    for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
+      const int rr = q % TILE, c = q / TILE;
+      sX[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
+    }
+    dt.store(sA, 0);
+    __syncthreads();
+    half_product<K>(sA, sX, sPart, sAcc, 0);
+  } else {
+    for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
+      const int rr = q % 32, c = q / 32;
+      sAcc[c * 32 + rr] = B[(int64_t)c * ldx + r0 + rr];
+    }
+    __syncthreads();
   }
-  auto wait_flag = [&](int dep) {
-    if (threadIdx.x == 0) {
+  for (int d = 0; d < ndep; ++d) {
+    const int dep = dep_of(d);
+    pf.store(sA, adj);
+    if (d + 1 < ndep) pf.load(tile_of(dep_of(d + 1)), h, adj);   // in flight during the wait
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {             // threads 0 and 32: one half each
+      const int* f = &flags[2 * dep + (threadIdx.x >> 5)];
       int spins = 0;
-      while (ld_acquire(&flags[dep]) != epoch) {
+      while (ld_acquire(f) != epoch) {
         if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
         if (spins > 64) __nanosleep(32);
       }
     }
     __syncthreads();
-  };
-  auto load_x = [&](int dep) {
-    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
+    for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
       const int rr = q % TILE, c = q / TILE;
-      sX[c * TILE + rr] = __ldcg(&X[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
+      sX[c * TILE + rr] = __ldcg(&out[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
     }
     __syncthreads();
-  };
-  // sPart ← products of the tile in `tile` (op per `op_adj`) with `vec`
-  auto product = [&](const cplx* tile, const cplx* vec, int op_adj) {
-    cplx acc[KMAX];
-#pragma unroll
-    for (int c = 0; c < KMAX; ++c) acc[c] = czero();
-    tile_apply<KMAX, NG>(tile, vec, k, op_adj, row, grp, acc);
-#pragma unroll
-    for (int c = 0; c < KMAX; ++c)
-      if (c < k) sPart[(grp * k + c) * TILE + row] = acc[c];
-    __syncthreads();
-  };
-  const int ndep = adj ? b : (nb - 1 - b);
-  for (int d = 0; d + 1 < ndep; ++d) {
-    const int dep = adj ? d : (nb - 1 - d);
-    const cplx* tp = adj ? T + tile_index(dep, b) * (TILE * TILE) : T + tile_index(b, dep) * (TILE * TILE);
-    __syncthreads();
-    load_tile(sT, tp, adj);   // independent of X: issued before the wait
-    wait_flag(dep);
-    load_x(dep);
-    product(sT, sX, adj);
-    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
-      const int rr = q % TILE, c = q / TILE;
-      cplx v = sAcc[c * TILE + rr];
-#pragma unroll
-      for (int gq = 0; gq < NG; ++gq) v = csub(v, sPart[(gq * k + c) * TILE + rr]);
-      sAcc[c * TILE + rr] = v;
-    }
+    half_product<K>(sA, sX, sPart, sAcc, 1);
   }
-  // y = D_b⁻¹ acc (adj: D_b⁻ᴴ acc), kept in sAcc
-  __syncthreads();
-  product(sD, sAcc, adj);
-  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
-    const int rr = q % TILE, c = q / TILE;
-    cplx v = sPart[(0 * k + c) * TILE + rr];
-#pragma unroll
-    for (int gq = 1; gq < NG; ++gq) v = cadd(v, sPart[(gq * k + c) * TILE + rr]);
-    sAcc[c * TILE + rr] = v;
-  }
-  if (ndep > 0) {
-    const int dep = adj ? b - 1 : b + 1;
-    load_tile(sT, E + ((int64_t)adj * nb + b) * TILE * TILE, 0);
-    wait_flag(dep);
-    load_x(dep);
-    product(sT, sX, 0);
-    for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
-      const int rr = q % TILE, c = q / TILE;
-      cplx v = sAcc[c * TILE + rr];
-#pragma unroll
-      for (int gq = 0; gq < NG; ++gq) v = csub(v, sPart[(gq * k + c) * TILE + rr]);
-      sAcc[c * TILE + rr] = v;
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < TILE * k; q += blockDim.x) {
-    const int rr = q % TILE, c = q / TILE;
-    X[(int64_t)c * ldx + (int64_t)b * TILE + rr] = sAcc[c * TILE + rr];
+  for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
+    const int rr = q % 32, c = q / 32;
+    out[(int64_t)c * ldx + r0 + rr] = sAcc[c * 32 + rr];
   }
   // bar.sync orders every thread's stores before thread 0's release (cumulative).
   __syncthreads();
-  if (threadIdx.x == 0) st_release(&flags[b], epoch);
+  if (threadIdx.x == 0) st_release(&flags[2 * b + h], epoch);
 }
 
-inline size_t trsm_smem_bytes(int k, int ng) {
-  return ((size_t)2 * TILE * TILE_LDS + (size_t)(2 + ng) * TILE * k) * sizeof(cplx);
+// X_b = D_b⁻ᴴ U_b on each half block row (grid 2·nb, 256 threads): the last step of the
+// adjoint solve.
+template <int K>
+__global__ void __launch_bounds__(256) k_trsm_finish(const cplx* __restrict__ Dinv, const cplx* __restrict__ U,
+                                                     cplx* __restrict__ X, int64_t ldx) {
+  extern __shared__ cplx sm[];
+  cplx* sA = sm;                       // TILE·HT_LDS
+  cplx* sX = sA + TILE * HT_LDS;       // TILE·K
+  cplx* sAcc = sX + TILE * K;          // 32·K
+  cplx* sPart = sAcc + 32 * K;         // 8·K·32
+  const int b = blockIdx.x >> 1, h = blockIdx.x & 1;
+  HalfTile dt;
+  dt.load(Dinv + (int64_t)b * TILE * TILE, h, 1);
+  for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
+    const int rr = q % TILE, c = q / TILE;
+    sX[c * TILE + rr] = U[(int64_t)c * ldx + (int64_t)b * TILE + rr];
+  }
+  dt.store(sA, 1);
+  __syncthreads();
+  half_product<K>(sA, sX, sPart, sAcc, 0);
+  for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
+    const int rr = q % 32, c = q / 32;
+    X[(int64_t)c * ldx + (int64_t)b * TILE + h * 32 + rr] = sAcc[c * 32 + rr];
+  }
+}
+
+// Dynamic shared memory of k_trsm_half / k_trsm_finish for K columns.
+inline size_t trsm_half_smem_bytes(int K) {
+  return ((size_t)TILE * HT_LDS + (size_t)TILE * K + 32 * K + 8 * K * 32) * sizeof(cplx);
 }
 
 // Y[:, 0:k] = lam[j] * Y[:, j] - X[:, j]  (side 'L') or Y - X*lam (side 'S');

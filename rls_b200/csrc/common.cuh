@@ -52,6 +52,14 @@ RLS_HD cplx cdiv(cplx a, cplx b) {
 }
 RLS_HD cplx cinv(cplx b) { return cdiv(make_double2(1.0, 0.0), b); }
 
+// 16-byte global→shared copies issued without waiting (cp.async, L2 only); a thread's
+// copies are complete after cp_async_wait_all(), visible to the block after a barrier.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -46,9 +46,10 @@ struct rls_ctx {
   int nb = 0;
   cplx* T = nullptr;        // tiles
   cplx* Dinv = nullptr;     // nb tiles
-  cplx* Etiles = nullptr;   // 2·nb tiles (k_trsm_etiles)
+  cplx* G = nullptr;        // tiles of the block-row scaled factor D⁻¹T (k_trsm_scale)
+  cplx* trsm_u = nullptr;   // n_pad × 8: the adjoint solve's chain values
   cplx z_dinv = cmk(NAN, NAN);
-  int* flags = nullptr;     // nb
+  int* flags = nullptr;     // 2·nb (one per half block row)
   int* ticket = nullptr;    // 1
   int epoch = 0;
   int* trmm_uO[2] = {nullptr, nullptr};
@@ -556,11 +557,12 @@ int orth_robust(rls_ctx* ctx, int64_t nrows, const cplx* V, int64_t ldv, int nV,
 
 int ensure_dinv(rls_ctx* ctx, cplx z) {
   if (ctx->z_dinv.x == z.x && ctx->z_dinv.y == z.y) return RLS_OK;
-  const size_t smem = 2 * TILE * TILE * sizeof(cplx);
-  k_diag_inv<<<ctx->nb, 256, smem, ctx->stream>>>(ctx->nb, ctx->n, ctx->T, z, ctx->Dinv, ctx->derr);
+  k_diag_inv<<<ctx->nb, 512, TILE * TILE_LDS * sizeof(cplx), ctx->stream>>>(ctx->nb, ctx->n, ctx->T, z, ctx->Dinv,
+                                                                            ctx->derr);
   RET(check_launch(ctx, "k_diag_inv"));
-  k_trsm_etiles<<<dim3(ctx->nb, 2), 256, smem, ctx->stream>>>(ctx->nb, ctx->T, ctx->Dinv, ctx->Etiles);
-  RET(check_launch(ctx, "k_trsm_etiles"));
+  const unsigned nslots = (unsigned)((int64_t)ctx->nb * (ctx->nb + 1) / 2);
+  k_trsm_scale<<<2 * nslots, 256, scale_smem_bytes(), ctx->stream>>>(ctx->T, ctx->Dinv, ctx->G);
+  RET(check_launch(ctx, "k_trsm_scale"));
   ctx->z_dinv = z;
   return RLS_OK;
 }
@@ -573,19 +575,45 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
       RET(trsm(ctx, z, adj, B + (int64_t)c0 * ld, X + (int64_t)c0 * ld, ld, std::min(8, k - c0)));
     return RLS_OK;
   }
+  if (B == X || ld != ctx->n_pad) {
+    set_err(ctx, "trsm: output must not alias the right-hand side, and ld must be n_pad");
+    return RLS_ERR_ARG;
+  }
   ctx->epoch += 1;
   if (ctx->epoch > (1 << 30)) {
     ctx->epoch = 1;
-    CK(cudaMemsetAsync(ctx->flags, 0, sizeof(int) * ctx->nb, ctx->stream));
+    CK(cudaMemsetAsync(ctx->flags, 0, sizeof(int) * 2 * ctx->nb, ctx->stream));
   }
   CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(int), ctx->stream));
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_TRSM, &e0);
-  k_trsm_dataflow<8, 8><<<ctx->nb, 512, trsm_smem_bytes(k, 8), ctx->stream>>>(
-      ctx->nb, ctx->T, ctx->Dinv, ctx->Etiles, B, X, ld, k, adj, ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);
-  // algorithmic bytes: the upper triangle of T once (n²/2 complex) + B read + X written
+  const size_t smem = trsm_half_smem_bytes(k);
+  const unsigned grid = (unsigned)(2 * ctx->nb);
+#define RLS_TRSM_CASE(K)                                                                                         \
+  case K:                                                                                                        \
+    k_trsm_half<K><<<grid, 256, smem, ctx->stream>>>(ctx->nb, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, ld, adj,     \
+                                                     ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);           \
+    break;
+  switch (k) {
+    RLS_TRSM_CASE(1) RLS_TRSM_CASE(2) RLS_TRSM_CASE(3) RLS_TRSM_CASE(4)
+    RLS_TRSM_CASE(5) RLS_TRSM_CASE(6) RLS_TRSM_CASE(7) RLS_TRSM_CASE(8)
+    default: set_err(ctx, "trsm: %d columns", k); return RLS_ERR_ARG;
+  }
+#undef RLS_TRSM_CASE
+  // algorithmic bytes: the upper triangle of the factor once (n²/2 complex) + B read + X written
   prof_end(ctx, KP_TRSM, e0, 16.0 * ((double)ctx->n * (ctx->n + 1) / 2 + 2.0 * (double)ctx->n * k));
-  return check_launch(ctx, "k_trsm_dataflow");
+  RET(check_launch(ctx, "k_trsm_half"));
+  if (adj) {
+#define RLS_FIN_CASE(K) \
+  case K: k_trsm_finish<K><<<grid, 256, smem, ctx->stream>>>(ctx->Dinv, ctx->trsm_u, X, ld); break;
+    switch (k) {
+      RLS_FIN_CASE(1) RLS_FIN_CASE(2) RLS_FIN_CASE(3) RLS_FIN_CASE(4)
+      RLS_FIN_CASE(5) RLS_FIN_CASE(6) RLS_FIN_CASE(7) RLS_FIN_CASE(8)
+    }
+#undef RLS_FIN_CASE
+    RET(check_launch(ctx, "k_trsm_finish"));
+  }
+  return RLS_OK;
 }
 
 // Y = T X (adj=0) or Tᴴ X (adj=1); k <= 16.
@@ -1155,7 +1183,23 @@ int allow_big_smem(rls_ctx* ctx, K kernel, int optin) {
 int set_kernel_attrs(rls_ctx* ctx) {
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  RET(allow_big_smem(ctx, k_trsm_dataflow<8, 8>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<1>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<2>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<3>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<4>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<5>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<6>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<7>, optin));
+  RET(allow_big_smem(ctx, k_trsm_half<8>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<1>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<2>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<3>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<4>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<5>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<6>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<7>, optin));
+  RET(allow_big_smem(ctx, k_trsm_finish<8>, optin));
+  RET(allow_big_smem(ctx, k_trsm_scale, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<8>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<8>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<16>, optin));
@@ -1165,7 +1209,6 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_batch_tsqr, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<16>, optin));
   RET(allow_big_smem(ctx, k_diag_inv, optin));
-  RET(allow_big_smem(ctx, k_trsm_etiles, optin));
   RET(allow_big_smem(ctx, k_tsqr_leaf, optin));
   RET(allow_big_smem(ctx, k_heev_rr, optin));
   {
@@ -1269,7 +1312,7 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   // drop an old operator and space
-  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->Etiles, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
+  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
                   (void*)ctx->colpart, (void*)ctx->trmm_uO[0], (void*)ctx->trmm_us[0], (void*)ctx->trmm_Ofirst[0],
                   (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
                   (void*)ctx->trmm_Ofirst[1], (void*)ctx->trmm_Ocount[1]})
@@ -1297,8 +1340,9 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   RET(dalloc_t(ctx, &ctx->T, h.size()));
   CK(cudaMemcpyAsync(ctx->T, h.data(), h.size() * sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
-  RET(dalloc_t(ctx, &ctx->Etiles, (size_t)2 * nb * TILE * TILE));
-  RET(dalloc_t(ctx, &ctx->flags, (size_t)nb));
+  RET(dalloc_t(ctx, &ctx->G, h.size()));
+  RET(dalloc_t(ctx, &ctx->trsm_u, (size_t)ctx->n_pad * 8));
+  RET(dalloc_t(ctx, &ctx->flags, (size_t)2 * nb));
   RET(dalloc_t(ctx, &ctx->ticket, 1));
   ctx->z_dinv = cmk(NAN, NAN);
   ctx->epoch = 0;

@@ -47,11 +47,12 @@ extern "C" int rls_test_trsm(rls_ctx* ctx, rls_c64 z, int adj, int k, const rls_
   DevTmp t(ctx);
   const int64_t np = ctx->n_pad, n = ctx->n;
   cplx* d = t.alloc<cplx>((size_t)np * k);
-  if (!d) return RLS_ERR_NOMEM;
+  cplx* dx = t.alloc<cplx>((size_t)np * k);
+  if (!d || !dx) return RLS_ERR_NOMEM;
   CK(cudaMemcpy2DAsync(d, np * sizeof(cplx), B, n * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyHostToDevice,
                        ctx->stream));
-  RET(trsm(ctx, cmk(z.re, z.im), adj, d, d, np, k));
-  CK(cudaMemcpy2DAsync(X, n * sizeof(cplx), d, np * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyDeviceToHost,
+  RET(trsm(ctx, cmk(z.re, z.im), adj, d, dx, np, k));
+  CK(cudaMemcpy2DAsync(X, n * sizeof(cplx), dx, np * sizeof(cplx), n * sizeof(cplx), k, cudaMemcpyDeviceToHost,
                        ctx->stream));
   return sync_and_check(ctx);
 }
