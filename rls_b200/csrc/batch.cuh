@@ -40,42 +40,65 @@ __device__ __forceinline__ bool batch_ok(const BatchDesc& d, int b) {
   return k >= 1 && k <= BATCH_KMAX;
 }
 
-// CzX_b = (J5 − z_b V) G1_b  (np × rr_b): 32 rows per CTA, split-K over 8 warps.
-// Dynamic shared memory: 8 × BATCH_KMAX × 32 cplx.
+// CzX_b = (J5 − z_b V) G1_b  (np × rr_b).  CTA (tile, b): 64 rows, 256 threads, thread
+// (row = t % 64, column group g = t / 64) owning columns 4g..4g+3.  G1_b (pr × 16, zero
+// beyond rr_b) sits in shared memory for broadcast reads; y = J5 − z V is staged in
+// chunks of CZX_KC inner indices, so each value of J5 and V is read once per CTA.
+// Column groups beyond rr_b (a warp-uniform test) skip the arithmetic.
+// Dynamic shared memory: czx_smem_bytes(pr).
+#define CZX_KC 32
 __global__ void __launch_bounds__(256) k_batch_czx(BatchDesc d) {
-  extern __shared__ cplx redc[];
-  auto red = reinterpret_cast<cplx(*)[BATCH_KMAX][32]>(redc);
+  extern __shared__ cplx smc[];
   const int b = blockIdx.y;
   if (!batch_ok(d, b)) return;
-  const int k2 = d.rr[b];
+  const int k2 = d.rr[b], pr = d.pr;
+  cplx* sG = smc;                          // G1_b[kk][j] at sG[kk*BATCH_KMAX + j]
+  cplx* sY = sG + pr * BATCH_KMAX;         // y[kk][row] at sY[kk*64 + row]
   const cplx mz = cneg(d.zs[b]);
   const cplx* G = d.G1 + (int64_t)b * d.g1_stride;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * 32 + lane;
-  const int kc = (d.pr + 7) / 8, kb = w * kc, ke = min(d.pr, kb + kc);
-  cplx acc[BATCH_KMAX];
+  for (int q = threadIdx.x; q < pr * BATCH_KMAX; q += blockDim.x) {
+    const int kk = q / BATCH_KMAX, j = q % BATCH_KMAX;
+    sG[q] = (j < k2) ? G[(int64_t)j * d.ldg1 + kk] : czero();
+  }
+  const int row = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  const bool active = g * 4 < k2;
+  cplx acc[4];
 #pragma unroll
-  for (int j = 0; j < BATCH_KMAX; ++j) acc[j] = czero();
-  if (row < d.np) {
-    for (int kk = kb; kk < ke; ++kk) {
-      const int64_t off = (int64_t)kk * d.np + row;
-      const cplx y = cfma(mz, d.V[off], d.J5[off]);
+  for (int c = 0; c < 4; ++c) acc[c] = czero();
+  for (int k0 = 0; k0 < pr; k0 += CZX_KC) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < 64 * CZX_KC; q += blockDim.x) {
+      const int rr = q % 64, kk = q / 64;
+      const int64_t gr = r0 + rr;
+      cplx y = czero();
+      if (k0 + kk < pr && gr < d.np) {
+        const int64_t off = (int64_t)(k0 + kk) * d.np + gr;
+        y = cfma(mz, d.V[off], d.J5[off]);
+      }
+      sY[kk * 64 + rr] = y;
+    }
+    __syncthreads();
+    if (active) {
+      const int kmax = min(CZX_KC, pr - k0);
+#pragma unroll 4
+      for (int kk = 0; kk < kmax; ++kk) {
+        const cplx y = sY[kk * 64 + row];
+        const cplx* gk = sG + (k0 + kk) * BATCH_KMAX + g * 4;
 #pragma unroll
-      for (int j = 0; j < BATCH_KMAX; ++j)
-        if (j < k2) acc[j] = cfma(y, __ldg(&G[(int64_t)j * d.ldg1 + kk]), acc[j]);
+        for (int c = 0; c < 4; ++c) acc[c] = cfma(y, gk[c], acc[c]);
+      }
     }
   }
-#pragma unroll
-  for (int j = 0; j < BATCH_KMAX; ++j)
-    if (j < k2) red[w][j][lane] = acc[j];
-  __syncthreads();
   cplx* out = d.czx + (int64_t)b * d.np * BATCH_KMAX;
-  for (int j = w; j < k2; j += 8) {
-    cplx s = czero();
-    for (int q = 0; q < 8; ++q) s = cadd(s, red[q][j][lane]);
-    if (row < d.np) out[(int64_t)j * d.np + row] = s;
+  if (r0 + row < d.np) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (g * 4 + c < k2) out[(int64_t)(g * 4 + c) * d.np + r0 + row] = acc[c];
   }
 }
+
+inline size_t czx_smem_bytes(int pr) { return ((size_t)pr * BATCH_KMAX + 64 * CZX_KC) * sizeof(cplx); }
 
 // One TSQR level for every point: leaf CTA (blockIdx.x, b) factors rows
 // [leaf*mb, leaf*mb + mb) of the m_b × k_b input (level 0: CzX_b with m_b = np;
@@ -151,56 +174,58 @@ __global__ void __launch_bounds__(256) k_batch_svd_gtot(BatchDesc d) {
 }
 
 // X_b = V G_b, W_b = (J1 − z J2 − z̄ J5 + |z|² V) G_b − X_b Σ_b², partial |W_b[:,1]|².
-// Dynamic shared memory: 2 × 8 × 8 × 32 cplx.
-__global__ void __launch_bounds__(256) k_batch_xw(BatchDesc d) {
-  extern __shared__ cplx redx[];
-  auto red = reinterpret_cast<cplx(*)[8][8][32]>(redx);
+// CTA (tile, b): XW_ROWS rows, one thread per row with R columns of X and of W in
+// registers; G_b (pr × R) sits in shared memory for broadcast reads.  R = r exactly.
+// Dynamic shared memory: pr·R cplx.
+#define XW_ROWS 256
+template <int R>
+__global__ void __launch_bounds__(XW_ROWS) k_batch_xw(BatchDesc d) {
+  extern __shared__ cplx smx[];
   const int b = blockIdx.y;
   if (!batch_ok(d, b)) return;
-  const int r = d.r, pr = d.pr;
+  const int pr = d.pr;
   const cplx z = d.zs[b];
   const cplx mz = cneg(z), mzc = cneg(cconj(z));
   const double zz = z.x * z.x + z.y * z.y;
-  const cplx* G = d.Gtot + (int64_t)b * d.gtot_stride;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * 32 + lane;
-  const int kc = (pr + 7) / 8, kb = w * kc, ke = min(pr, kb + kc);
-  cplx acc[8], accx[8];
+  const cplx* G = d.Gtot + (int64_t)b * d.gtot_stride;   // column j at G + j*pr
+  for (int q = threadIdx.x; q < pr * R; q += blockDim.x) {
+    const int kk = q / R, j = q % R;
+    smx[q] = G[(int64_t)j * pr + kk];
+  }
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * XW_ROWS + threadIdx.x;
+  cplx ax[R], aw[R];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) { acc[j] = czero(); accx[j] = czero(); }
+  for (int j = 0; j < R; ++j) { ax[j] = czero(); aw[j] = czero(); }
   if (row < d.np) {
-    for (int kk = kb; kk < ke; ++kk) {
+#pragma unroll 2
+    for (int kk = 0; kk < pr; ++kk) {
       const int64_t off = (int64_t)kk * d.np + row;
       const cplx vv = d.V[off];
       cplx y = d.J1[off];
       y = cfma(mz, d.J2[off], y);
       y = cfma(mzc, d.J5[off], y);
       y = cadd(y, cscale(vv, zz));
+      const cplx* gk = smx + kk * R;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (j < r) {
-          const cplx g = __ldg(&G[(int64_t)j * pr + kk]);
-          acc[j] = cfma(y, g, acc[j]);
-          accx[j] = cfma(vv, g, accx[j]);
-        }
+      for (int j = 0; j < R; ++j) {
+        const cplx gv = gk[j];
+        ax[j] = cfma(vv, gv, ax[j]);
+        aw[j] = cfma(y, gv, aw[j]);
+      }
     }
   }
-#pragma unroll
-  for (int j = 0; j < 8; ++j)
-    if (j < r) { red[0][w][j][lane] = acc[j]; red[1][w][j][lane] = accx[j]; }
-  __syncthreads();
-  cplx* X = d.XW + (int64_t)b * 2 * d.np * r;
-  cplx* W = X + d.np * r;
+  cplx* X = d.XW + (int64_t)b * 2 * d.np * d.r;
+  cplx* W = X + d.np * d.r;
   const double* sg = d.sig + (int64_t)b * BATCH_KMAX;
   double c0 = 0.0;
-  for (int j = w; j < r; j += 8) {
-    cplx sa = czero(), sx = czero();
-    for (int q = 0; q < 8; ++q) { sa = cadd(sa, red[0][q][j][lane]); sx = cadd(sx, red[1][q][j][lane]); }
-    const cplx out = csub(sa, cscale(sx, sg[j] * sg[j]));
-    if (row < d.np) {
-      X[(int64_t)j * d.np + row] = sx;
-      W[(int64_t)j * d.np + row] = out;
-      if (j == 0) c0 = cabs2(out);
+  if (row < d.np) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const cplx o = csub(aw[j], cscale(ax[j], sg[j] * sg[j]));
+      X[(int64_t)j * d.np + row] = ax[j];
+      W[(int64_t)j * d.np + row] = o;
+      if (j == 0) c0 = cabs2(o);
     }
   }
   __shared__ double sred[32];

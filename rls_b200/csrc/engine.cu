@@ -1074,12 +1074,11 @@ int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, doubl
   d.stack[0] = ctx->bstack0; d.stack[1] = ctx->bstack1; d.stack_stride = ctx->bstack_stride;
   d.Rb = ctx->bRb; d.sig = ctx->bsig; d.G2 = ctx->bG2;
   d.Gtot = ctx->bGtot; d.gtot_stride = (int64_t)ctx->pr_max * r;
-  d.XW = ctx->bXW; d.colpart = ctx->bcolpart; d.ntiles = (int)((np + 31) / 32); d.w0sq = ctx->bw0;
+  d.XW = ctx->bXW; d.colpart = ctx->bcolpart; d.ntiles = (int)((np + XW_ROWS - 1) / XW_ROWS); d.w0sq = ctx->bw0;
   d.g1_always = ctx->ritz_g1_always;
-  const dim3 tiles((unsigned)d.ntiles, (unsigned)B);
   cudaEvent_t e1 = nullptr;
   prof_begin(ctx, KP_RECYCLE_GEMM, &e1);
-  k_batch_czx<<<tiles, 256, (size_t)8 * BATCH_KMAX * 32 * sizeof(cplx), ctx->stream>>>(d);
+  k_batch_czx<<<dim3((unsigned)((np + 63) / 64), (unsigned)B), 256, czx_smem_bytes(pr), ctx->stream>>>(d);
   RET(check_launch(ctx, "k_batch_czx"));
   // TSQR levels sized for BATCH_KMAX columns
   {
@@ -1106,7 +1105,21 @@ int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, doubl
   }
   k_batch_svd_gtot<<<B, 256, 0, ctx->stream>>>(d);
   RET(check_launch(ctx, "k_batch_svd_gtot"));
-  k_batch_xw<<<tiles, 256, (size_t)2 * 8 * 8 * 32 * sizeof(cplx), ctx->stream>>>(d);
+  {
+    const dim3 grid((unsigned)d.ntiles, (unsigned)B);
+    const size_t smem = (size_t)pr * r * sizeof(cplx);
+    switch (r) {
+      case 1: k_batch_xw<1><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 2: k_batch_xw<2><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 3: k_batch_xw<3><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 4: k_batch_xw<4><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 5: k_batch_xw<5><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 6: k_batch_xw<6><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 7: k_batch_xw<7><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      case 8: k_batch_xw<8><<<grid, XW_ROWS, smem, ctx->stream>>>(d); break;
+      default: set_err(ctx, "batched recycle step supports r <= 8, got %d", r); return RLS_ERR_ARG;
+    }
+  }
   RET(check_launch(ctx, "k_batch_xw"));
   prof_end(ctx, KP_RECYCLE_GEMM, e1, B * 16.0 * ((double)ctx->n * pr * 6 + 2.0 * ctx->n * r));
   k_batch_w0<<<B, 256, 0, ctx->stream>>>(d);
@@ -1205,7 +1218,6 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_gemm_rows<16>, optin));
   RET(allow_big_smem(ctx, k_gemm_rows<32>, optin));
   RET(allow_big_smem(ctx, k_batch_czx, optin));
-  RET(allow_big_smem(ctx, k_batch_xw, optin));
   RET(allow_big_smem(ctx, k_batch_tsqr, optin));
   RET(allow_big_smem(ctx, k_trmm_partial<16>, optin));
   RET(allow_big_smem(ctx, k_diag_inv, optin));

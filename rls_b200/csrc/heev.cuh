@@ -140,22 +140,23 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   const int b = blockIdx.x;
   const int n = pr;
   const int nlu = plan.nlu;
-  // shared layout: [A (n × lda cplx)] v w tau (n cplx) d e e2 lam (n doubles) LU (nlu·6n doubles) S (gs_cap·n cplx)
+  // shared layout: [A (n × lda cplx)] v v1 w tau (n cplx) yp (16n cplx) d e e2 lam (n doubles)
+  // LU (nlu·6n doubles) S (gs_cap·n cplx)
   cplx* base = reinterpret_cast<cplx*>(dsm);
   const int lda = plan.lda > 0 ? plan.lda : n;
   cplx* A = plan.lda > 0 ? base : work.A + (int64_t)b * prmax * prmax;
   cplx* v = base + (plan.lda > 0 ? (size_t)n * lda : 0);
-  cplx* w = v + n;
+  cplx* v1 = v + n;
+  cplx* w = v1 + n;
   cplx* tau = w + n;
-  double* d = reinterpret_cast<double*>(tau + n);
+  cplx* yp = tau + n;                     // 16 warps × n partial products of the reduction
+  double* d = reinterpret_cast<double*>(yp + (size_t)16 * n);
   double* e = d + n;
   double* e2 = e + n;
   double* lam = e2 + n;
   double* lusm = lam + n;
   cplx* Ssm = reinterpret_cast<cplx*>(lusm + (size_t)nlu * 6 * n);
   __shared__ double red[32];
-  __shared__ cplx s_tau;
-  __shared__ cplx ypart[32];
   __shared__ int s_rr;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const cplx z = zs[b];
@@ -175,76 +176,130 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   }
   __syncthreads();
 
-  // 2. Householder tridiagonalisation (lower form): for column k reduce A[k+1:, k].
-  //    Four barriers per column: warp 0 forms the reflector; groups of 4 threads
-  //    form y = τ·A·v from the lower triangle with per-warp partials of yᴴv;
-  //    w = y + α₂·v, α₂ = −½ τ (yᴴv); the lower triangle takes A −= v wᴴ + w vᴴ.
+  // 2. Householder tridiagonalisation: for column k reduce A[k+1:, k].  Both triangles of
+  //    the trailing block are kept, so y = τ·A·v is a plain column sweep.  Three barriers
+  //    per column:
+  //      B  warp w sums the columns j ≡ w (mod 16) of the trailing block for all rows
+  //         (lane = row), partial products to yp[w], partial yᴴv per warp;
+  //      R  y_i = Σ_w yp[w][i]; α₂ = −½ τ yᴴv;
+  //      D  A −= v wᴴ + w vᴴ on the trailing block, w = y + α₂·v, columns of warps 1..15;
+  //         warp 0 updates column k+1 and forms the next reflector meanwhile.
+  //    Reflectors alternate between two buffers.
+  auto make_reflector = [&](int k) {   // warp 0; column k (rows ≥ k+1) is final
+    const int m0 = k + 1;
+    cplx* vk = (k & 1) ? v1 : v;
+    double x2 = 0.0;
+    for (int i = m0 + 1 + lane; i < n; i += 32) x2 += cabs2(A[k * lda + i]);
+    x2 = warp_sum(x2);
+    // Householder coefficients in the convention of LAPACK's zlarfg (β real, τ complex);
+    // the divisions are reciprocals refined by Newton–Raphson (recip_nr).
+    const cplx alpha = A[k * lda + m0];
+    double beta;
+    cplx t, sc;
+    if (x2 == 0.0 && alpha.y == 0.0) {
+      beta = alpha.x; t = czero(); sc = czero();
+    } else {
+      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + x2);
+      beta = (alpha.x >= 0.0) ? -nrm : nrm;
+      const double ib = recip_nr(beta);
+      t = cmk((beta - alpha.x) * ib, -alpha.y * ib);
+      const double ar = alpha.x - beta, ai = alpha.y;             // sc = 1 / (α − β)
+      const double id = recip_nr(ar * ar + ai * ai);
+      sc = cmk(ar * id, -ai * id);
+    }
+    for (int i = m0 + lane; i < n; i += 32) {
+      const cplx vi = (i == m0) ? cmk(1.0, 0.0) : cmul(A[k * lda + i], sc);
+      vk[i] = vi;
+      if (i > m0) A[k * lda + i] = vi;      // reflector tail kept for the back-transformation
+    }
+    if (lane == 0) {
+      tau[k] = t;
+      e[k] = beta;
+      d[k] = A[k * lda + k].x;
+    }
+  };
+  __shared__ cplx yvp[16];
+  if (n > 1 && warp == 0) make_reflector(0);
+  __syncthreads();
   for (int k = 0; k < n - 1; ++k) {
     const int m0 = k + 1;
-    if (warp == 0) {
-      double x2 = 0.0;
-      for (int i = m0 + 1 + lane; i < n; i += 32) x2 += cabs2(A[k * lda + i]);
-      x2 = warp_sum(x2);
-      double beta; cplx t, sc;
-      householder_coeffs(A[k * lda + m0], x2, &beta, &t, &sc);
-      for (int i = m0 + lane; i < n; i += 32) {
-        const cplx vi = (i == m0) ? cmk(1.0, 0.0) : cmul(A[k * lda + i], sc);
-        v[i] = vi;
-        if (i > m0) A[k * lda + i] = vi;      // reflector tail kept for the back-transformation
+    const cplx t = tau[k];
+    const cplx* vk = (k & 1) ? v1 : v;
+    const bool active = (t.x != 0.0 || t.y != 0.0);
+    if (active) {   // B
+      cplx yv = czero();
+      for (int i0 = m0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        const bool ok = i < n;
+        cplx s0 = czero(), s1 = czero();
+        int j = m0 + warp;
+        for (; j + 16 < n; j += 32) {
+          if (ok) {
+            s0 = cfma(A[j * lda + i], vk[j], s0);
+            s1 = cfma(A[(j + 16) * lda + i], vk[j + 16], s1);
+          }
+        }
+        if (j < n && ok) s0 = cfma(A[j * lda + i], vk[j], s0);
+        if (ok) {
+          const cplx yi = cmul(t, cadd(s0, s1));
+          yp[warp * n + i] = yi;
+          yv = cfmac(yi, vk[i], yv);
+        }
       }
-      if (lane == 0) {
-        s_tau = t;
-        tau[k] = t;
-        e[k] = beta;
-        d[k] = A[k * lda + k].x;
+      yv = warp_sum(yv);
+      if (lane == 0) yvp[warp] = yv;
+    }
+    __syncthreads();
+    cplx a2 = czero();
+    if (active) {   // R
+      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) {
+        cplx y0 = yp[i], y1 = yp[n + i], y2 = yp[2 * n + i], y3 = yp[3 * n + i];
+#pragma unroll
+        for (int q = 4; q < 16; q += 4) {
+          y0 = cadd(y0, yp[q * n + i]);
+          y1 = cadd(y1, yp[(q + 1) * n + i]);
+          y2 = cadd(y2, yp[(q + 2) * n + i]);
+          y3 = cadd(y3, yp[(q + 3) * n + i]);
+        }
+        w[i] = cadd(cadd(y0, y1), cadd(y2, y3));
+      }
+      cplx s0 = cadd(yvp[0], yvp[1]), s1 = cadd(yvp[2], yvp[3]);
+#pragma unroll
+      for (int q = 4; q < 16; q += 4) {
+        s0 = cadd(s0, cadd(yvp[q], yvp[q + 1]));
+        s1 = cadd(s1, cadd(yvp[q + 2], yvp[q + 3]));
+      }
+      a2 = cscale(cmul(t, cadd(s0, s1)), -0.5);
+    }
+    __syncthreads();
+    if (warp == 0) {   // D, column m0 (all trailing rows), then the next reflector
+      if (active) {
+        const cplx vj = vk[m0], wj = cfma(a2, vj, w[m0]);
+        for (int i = m0 + lane; i < n; i += 32) {
+          const cplx vi = vk[i], wi = cfma(a2, vi, w[i]);
+          cplx aij = A[m0 * lda + i];
+          aij = csub(aij, cmulc(wj, vi));    // v_i conj(w_j)
+          aij = csub(aij, cmulc(vj, wi));    // w_i conj(v_j)
+          A[m0 * lda + i] = aij;
+        }
+        __syncwarp();
+      }
+      if (k + 1 < n - 1) make_reflector(k + 1);
+    } else if (active) {   // D, columns m0+1 .. n-1 (all trailing rows)
+      for (int i0 = m0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        if (i >= n) continue;
+        const cplx vi = vk[i], wi = cfma(a2, vi, w[i]);
+        for (int j = m0 + warp; j < n; j += nw - 1) {
+          const cplx vj = vk[j], wj = cfma(a2, vj, w[j]);
+          cplx aij = A[j * lda + i];
+          aij = csub(aij, cmulc(wj, vi));
+          aij = csub(aij, cmulc(vj, wi));
+          A[j * lda + i] = aij;
+        }
       }
     }
     __syncthreads();
-    const cplx t = s_tau;
-    if (t.x != 0.0 || t.y != 0.0) {
-      // y_i = τ Σ_j Ã[i,j] v_j over the trailing block, Ã from the lower triangle:
-      // Ã[i,j] = A[i,j] (i >= j), conj(A[j,i]) (i < j).
-      const int mm = n - m0;
-      const int nq = ((mm * 4 + 31) / 32) * 32;
-      cplx yv_part = czero();
-      for (int q = threadIdx.x; q < nq; q += blockDim.x) {
-        const bool valid = q < mm * 4;
-        const int i = m0 + q / 4, part = q & 3;
-        cplx sum = czero();
-        if (valid) {
-          int j = m0 + part;
-          for (; j < i; j += 4) sum = cfma(A[j * lda + i], v[j], sum);        // row i, j < i
-          for (; j < n; j += 4) sum = cfmac(A[i * lda + j], v[j], sum);       // column i, j >= i
-        }
-        sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
-        sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
-        sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 2);
-        sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 2);
-        if (valid && part == 0) {
-          const cplx yi = cmul(t, sum);
-          w[i] = yi;
-          yv_part = cfmac(yi, v[i], yv_part);  // Σ conj(y_i) v_i
-        }
-      }
-      yv_part = warp_sum(yv_part);
-      if (lane == 0) ypart[warp] = yv_part;
-      __syncthreads();
-      cplx yv = czero();
-      for (int q = 0; q < nw; ++q) yv = cadd(yv, ypart[q]);
-      const cplx a2 = cscale(cmul(t, yv), -0.5);
-      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) w[i] = cfma(a2, v[i], w[i]);
-      __syncthreads();
-      // lower triangle (and diagonal) of A −= v wᴴ + w vᴴ
-      for (int q = threadIdx.x; q < mm * mm; q += blockDim.x) {
-        const int i = m0 + q % mm, j = m0 + q / mm;
-        if (i < j) continue;
-        cplx aij = A[j * lda + i];
-        aij = csub(aij, cmul(v[i], cconj(w[j])));
-        aij = csub(aij, cmul(w[i], cconj(v[j])));
-        A[j * lda + i] = aij;
-      }
-      __syncthreads();
-    }
   }
   if (threadIdx.x == 0) d[n - 1] = A[(n - 1) * lda + (n - 1)].x;
   for (int i = threadIdx.x; i < n - 1; i += blockDim.x) e2[i] = e[i] * e[i];
@@ -445,7 +500,7 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
 // as fit.
 inline HeevPlan heev_plan(int pr, size_t avail) {
   HeevPlan p{};
-  const size_t vec = (size_t)3 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
+  const size_t vec = (size_t)(4 + 16) * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
   int lda = pr + ((4 - pr % 8) + 8) % 8;                    // ≡ 4 (mod 8)
   size_t need = vec + (size_t)pr * lda * sizeof(cplx);
   const size_t lu1 = (size_t)6 * pr * sizeof(double);
