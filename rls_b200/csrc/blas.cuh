@@ -17,49 +17,79 @@ __host__ __device__ __forceinline__ int64_t tile_index(int I, int J) {
 }
 
 // ------------------------------------------------------------------------------------
-// Gram: C (k1×k2) = alpha·AᴴB + beta·C.  Phase 1: grid (row chunks, ceil(k1/8)); warp w
-// owns column (blockIdx.y*8+w) of A and sums over the chunk's rows; k2 <= K2MAX.
+// Gram: C (k1×k2) = alpha·AᴴB + beta·C in one launch.  Grid (row chunks, ceil(k1/8)):
+// warp w of CTA (c, g) owns column g·8+w of A and sums conj(A)·B over chunk c's rows,
+// writing its partial to part[c][col][:].  The last CTA of column group g to finish
+// (atomic counter, after a fence) sums the partials of that group over the chunks in a
+// fixed order — four threads per output over chunks ≡ q (mod 4), then a fixed shuffle
+// tree — so the result does not depend on which CTA finishes last; it then resets the
+// counter.  K2 is the exact column count of B when EXACT, else an upper bound.
 // ------------------------------------------------------------------------------------
-template <int K2MAX>
-__global__ void __launch_bounds__(256) k_gram_partial(int64_t nrows, int64_t chunk,
-                                                      const cplx* __restrict__ A, int64_t lda, int k1,
-                                                      const cplx* __restrict__ B, int64_t ldb, int k2,
-                                                      cplx* __restrict__ part) {
+template <int K2, bool EXACT>
+__global__ void __launch_bounds__(256) k_gram(int64_t nrows, int64_t chunk, const cplx* __restrict__ A,
+                                              int64_t lda, int k1, const cplx* __restrict__ B, int64_t ldb,
+                                              int k2, cplx* part, int* counters, cplx alpha, cplx beta, cplx* C,
+                                              int64_t ldc) {
+  const int kk2 = EXACT ? K2 : k2;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int col = blockIdx.y * 8 + w;
   const int64_t r0 = (int64_t)blockIdx.x * chunk;
   const int64_t r1 = min(nrows, r0 + chunk);
-  cplx acc[K2MAX];
+  cplx acc[K2];
 #pragma unroll
-  for (int j = 0; j < K2MAX; ++j) acc[j] = czero();
+  for (int j = 0; j < K2; ++j) acc[j] = czero();
   if (col < k1) {
     const cplx* a = A + (int64_t)col * lda;
     for (int64_t row = r0 + lane; row < r1; row += 32) {
       const cplx av = a[row];
 #pragma unroll
-      for (int j = 0; j < K2MAX; ++j)
-        if (j < k2) acc[j] = cfmac(av, __ldg(&B[(int64_t)j * ldb + row]), acc[j]);
+      for (int j = 0; j < K2; ++j)
+        if (EXACT || j < k2) acc[j] = cfmac(av, __ldg(&B[(int64_t)j * ldb + row]), acc[j]);
     }
   }
 #pragma unroll
-  for (int j = 0; j < K2MAX; ++j) {
-    if (j < k2) {
-      cplx s = warp_sum(acc[j]);
-      if (lane == 0 && col < k1) part[((int64_t)blockIdx.x * k1 + col) * k2 + j] = s;
+  for (int j = 0; j < K2; ++j) {
+    if (EXACT || j < k2) {
+      const cplx s = warp_sum(acc[j]);
+      if (lane == 0 && col < k1) part[((int64_t)blockIdx.x * k1 + col) * kk2 + j] = s;
     }
   }
-}
-
-__global__ void k_gram_reduce(int nchunks, int k1, int k2, const cplx* __restrict__ part, cplx alpha,
-                              cplx beta, cplx* C, int64_t ldc) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= k1 * k2) return;
-  const int i = t / k2, j = t % k2;
-  cplx s = czero();
-  for (int c = 0; c < nchunks; ++c) s = cadd(s, part[((int64_t)c * k1 + i) * k2 + j]);
-  cplx out = cmul(alpha, s);
-  if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + i], out);
-  C[(int64_t)j * ldc + i] = out;
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = (atomicAdd(&counters[blockIdx.y], 1) == (int)gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int i0 = blockIdx.y * 8, ni = min(8, k1 - i0), nout = ni * kk2, nc = (int)gridDim.x;
+  const int q = threadIdx.x & 3;
+  for (int base = 0; base < nout; base += (int)blockDim.x / 4) {
+    const int o = base + (int)threadIdx.x / 4;
+    const bool valid = o < nout;
+    const int i = i0 + (valid ? o / kk2 : 0), j = valid ? o % kk2 : 0;
+    cplx s0 = czero(), s1 = czero();
+    if (valid) {
+      int c = q;
+      for (; c + 4 < nc; c += 8) {
+        s0 = cadd(s0, __ldcg(&part[((int64_t)c * k1 + i) * kk2 + j]));
+        s1 = cadd(s1, __ldcg(&part[((int64_t)(c + 4) * k1 + i) * kk2 + j]));
+      }
+      if (c < nc) s0 = cadd(s0, __ldcg(&part[((int64_t)c * k1 + i) * kk2 + j]));
+    }
+    cplx s = cadd(s0, s1);
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, 1);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, 2);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
+    if (valid && q == 0) {
+      cplx out = cmul(alpha, s);
+      if (beta.x != 0.0 || beta.y != 0.0) out = cfma(beta, C[(int64_t)j * ldc + i], out);
+      C[(int64_t)j * ldc + i] = out;
+    }
+  }
+  if (threadIdx.x == 0) counters[blockIdx.y] = 0;
 }
 
 // ------------------------------------------------------------------------------------

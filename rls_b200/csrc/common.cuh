@@ -52,6 +52,17 @@ RLS_HD cplx cdiv(cplx a, cplx b) {
 }
 RLS_HD cplx cinv(cplx b) { return cdiv(make_double2(1.0, 0.0), b); }
 
+// 1/q by the hardware reciprocal estimate refined with two Newton–Raphson steps
+// (r ← r + r(1 − q r)); the relative error is far below what a Sturm count needs.
+__device__ __forceinline__ double recip_nr(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  double e = fma(-q, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-q, r, 1.0);
+  return fma(r, e, r);
+}
+
 // 16-byte global→shared copies issued without waiting (cp.async, L2 only); a thread's
 // copies are complete after cp_async_wait_all(), visible to the block after a barrier.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {

@@ -25,6 +25,7 @@
 namespace {
 
 constexpr double kEps = 2.220446049250313e-16;
+constexpr int kGramCounters = 128;
 
 struct DevBuf {
   void* p = nullptr;
@@ -64,6 +65,7 @@ struct rls_ctx {
   double* dscal = nullptr;         // small scalars (256)
   cplx* gram_part = nullptr;
   size_t gram_part_elems = 0;
+  int* gram_cnt = nullptr;         // per column group completion counters of k_gram (kGramCounters)
   cplx* tsqr_stack[2] = {nullptr, nullptr};
   size_t tsqr_stack_elems = 0;
   cplx* small[8] = {};             // small k×k / pr×k scratch (kmax × 64 each)
@@ -326,24 +328,37 @@ int gram(rls_ctx* ctx, int64_t nrows, const cplx* A, int64_t lda, int k1, const 
   if (k1 <= 0 || k2 <= 0) return RLS_OK;
   const int64_t chunk = 64;   // 2 rows per lane: many CTAs, short dependency chains
   const int nchunks = (int)((nrows + chunk - 1) / chunk);
+  if ((k1 + 7) / 8 > kGramCounters) {
+    set_err(ctx, "gram: %d columns exceed the counter array", k1);
+    return RLS_ERR_DIM;
+  }
   for (int j0 = 0; j0 < k2; j0 += 32) {
     const int kk2 = std::min(32, k2 - j0);
     if ((size_t)nchunks * k1 * kk2 > ctx->gram_part_elems) {
       set_err(ctx, "gram workspace too small (%d×%d×%d)", nchunks, k1, kk2);
       return RLS_ERR_DIM;
     }
-    dim3 grid(nchunks, (k1 + 7) / 8);
-    if (kk2 <= 8)
-      k_gram_partial<8><<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
-                                                       ctx->gram_part);
-    else
-      k_gram_partial<32><<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, B + (int64_t)j0 * ldb, ldb, kk2,
-                                                        ctx->gram_part);
-    RET(check_launch(ctx, "k_gram_partial"));
-    const int tot = k1 * kk2;
-    k_gram_reduce<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(nchunks, k1, kk2, ctx->gram_part, alpha, beta,
-                                                              C + (int64_t)j0 * ldc, ldc);
-    RET(check_launch(ctx, "k_gram_reduce"));
+    const dim3 grid(nchunks, (k1 + 7) / 8);
+    const cplx* Bj = B + (int64_t)j0 * ldb;
+    cplx* Cj = C + (int64_t)j0 * ldc;
+#define RLS_GRAM(K2, EX)                                                                                  \
+  k_gram<K2, EX><<<grid, 256, 0, ctx->stream>>>(nrows, chunk, A, lda, k1, Bj, ldb, kk2, ctx->gram_part, \
+                                                ctx->gram_cnt, alpha, beta, Cj, ldc)
+    switch (kk2) {
+      case 1: RLS_GRAM(1, true); break;
+      case 2: RLS_GRAM(2, true); break;
+      case 3: RLS_GRAM(3, true); break;
+      case 4: RLS_GRAM(4, true); break;
+      case 5: RLS_GRAM(5, true); break;
+      case 6: RLS_GRAM(6, true); break;
+      case 7: RLS_GRAM(7, true); break;
+      case 8: RLS_GRAM(8, true); break;
+      default:
+        if (kk2 <= 16) RLS_GRAM(16, false);
+        else RLS_GRAM(32, false);
+    }
+#undef RLS_GRAM
+    RET(check_launch(ctx, "k_gram"));
   }
   return RLS_OK;
 }
@@ -909,7 +924,7 @@ int block_unitary_update(rls_ctx* ctx) {
   const int p = ctx->p, r = ctx->r;
   if (p <= 1) return RLS_OK;
   const int pr = p * r, r2 = 2 * r;
-  const size_t smc = ((size_t)pr * r + 2 * (size_t)r * r + 4 * (size_t)r * r + r) * sizeof(cplx);
+  const size_t smc = (size_t)pr * r * sizeof(cplx);
   k_blockrot_coeffs<<<1, 32, smc, ctx->stream>>>(p, r, ctx->L, ctx->pr_max, ctx->Ulist);
   RET(check_launch(ctx, "k_blockrot_coeffs"));
   RotArrays arr{};
@@ -1280,6 +1295,7 @@ extern "C" int rls_ctx_create(rls_ctx** out, int device) {
   }
   if (st == RLS_OK) ctx->hstage_err = reinterpret_cast<int*>(ctx->hstage + kStageBytes);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->derr, 4);
+  if (st == RLS_OK) st = dalloc_t(ctx, &ctx->gram_cnt, kGramCounters);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->dscal, 256);
   if (st != RLS_OK) {
     g_create_err = ctx->err;

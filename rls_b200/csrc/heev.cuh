@@ -28,17 +28,6 @@ struct HeevWork {
   double* lu;     // per problem 16 warps × 6 × pr_max doubles
 };
 
-// 1/q by the hardware reciprocal estimate refined with two Newton–Raphson steps
-// (r ← r + r(1 − q r)); the relative error is far below what a Sturm count needs.
-__device__ __forceinline__ double recip_nr(double q) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
-  double e = fma(-q, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-q, r, 1.0);
-  return fma(r, e, r);
-}
-
 // Numbers of eigenvalues of the tridiagonal (d, e²) below x1 and below x2 (two
 // interleaved Sturm sequences).
 __device__ __forceinline__ void sturm_count2(const double* d, const double* e2, int n, double x1, double x2,

@@ -9,84 +9,95 @@
 // The rotations depend only on the last block column of L (k_blockrot_coeffs, one
 // warp); k_blockrot_apply then streams the rows of each array once applying all p-1
 // right products, and k_blockrot_left the columns of L, H1, H2 for the left products.
+// The QR of each 2r × r block follows LAPACK's zgeqrf/zlarfg conventions.
 #pragma once
 #include "common.cuh"
 #include "small.cuh"
 
-// Full m×m Q of the Householder QR of Y (m×k, m <= 32, in place: Y ← R and reflector
-// tails), one warp.  Lane c owns column c, so every dot product is a serial loop in one
-// lane: no shuffles on the dependency chain.
-__device__ void warp_house_fullq(cplx* Y, int ldy, int m, int k, cplx* Q, int ldq, cplx* tau) {
-  const int lane = threadIdx.x & 31;
-  __shared__ cplx s_t[32];
-  for (int j = 0; j < k; ++j) {
-    if (lane == 0) {
-      double x2 = 0.0;
-      for (int i = j + 1; i < m; ++i) x2 += cabs2(Y[j * ldy + i]);
-      double beta; cplx t, sc;
-      householder_coeffs(Y[j * ldy + j], x2, &beta, &t, &sc);
-      for (int i = j + 1; i < m; ++i) Y[j * ldy + i] = cmul(Y[j * ldy + i], sc);
-      Y[j * ldy + j] = cmk(beta, 0.0);
-      tau[j] = t;
-      s_t[0] = t;
-    }
-    __syncwarp();
-    const cplx tc = cconj(s_t[0]);
-    const int c = j + 1 + lane;
-    if (c < k) {   // apply H_jᴴ to column c
-      cplx s = Y[c * ldy + j];
-      for (int i = j + 1; i < m; ++i) s = cfmac(Y[j * ldy + i], Y[c * ldy + i], s);
-      const cplx f = cmul(tc, s);
-      Y[c * ldy + j] = csub(Y[c * ldy + j], f);
-      for (int i = j + 1; i < m; ++i) Y[c * ldy + i] = cfms(Y[j * ldy + i], f, Y[c * ldy + i]);
-    }
-    __syncwarp();
-  }
-  // Q = H_0 ... H_{k-1} I_m, last reflector first; lane c owns column c of Q.
-  if (lane < m) {
-    for (int i = 0; i < m; ++i) Q[lane * ldq + i] = (i == lane) ? cmk(1.0, 0.0) : czero();
-    for (int j = k - 1; j >= 0; --j) {
-      const cplx tj = tau[j];
-      cplx s = Q[lane * ldq + j];
-      for (int i = j + 1; i < m; ++i) s = cfmac(Y[j * ldy + i], Q[lane * ldq + i], s);
-      const cplx f = cmul(tj, s);
-      Q[lane * ldq + j] = csub(Q[lane * ldq + j], f);
-      for (int i = j + 1; i < m; ++i) Q[lane * ldq + i] = cfms(Y[j * ldy + i], f, Q[lane * ldq + i]);
-    }
-  }
-  __syncwarp();
-}
-
 // Rotation coefficients from the last block column of L alone: rotation i (i < p-1,
 // 0-based) is determined by [L(p-1, p-1); L(i, p-1)] after rotations 0..i-1, and those
 // only change block row p-1 of that column.  One warp; Lc (pr × r) in shared memory.
-__global__ void k_blockrot_coeffs(int p, int r, const cplx* __restrict__ L, int ld, cplx* Uout) {
+// Lane a holds row a of the 2r × r block Y (r <= 8, so 2r <= 16 lanes): each Householder
+// step of the QR of Y is a handful of warp sums, and Q = H_0 ... H_{r-1} (applied to the
+// identity, last reflector first) is kept one row per lane.  U_i = Qᴴ goes to Uout.
+// The reflectors follow LAPACK's zlarfg convention (β real), with Newton-refined
+// reciprocals in place of divisions.
+__global__ void __launch_bounds__(32) k_blockrot_coeffs(int p, int r, const cplx* __restrict__ L, int ld,
+                                                        cplx* Uout) {
   extern __shared__ cplx sm[];
   const int r2 = 2 * r, pr = p * r, bp = p - 1, lane = threadIdx.x;
-  cplx* Lc = sm;                 // pr × r
-  cplx* Y = Lc + pr * r;         // r2 × r
-  cplx* Q = Y + r2 * r;          // r2 × r2
-  cplx* tau = Q + r2 * r2;       // r
+  cplx* Lc = sm;                 // pr × r: the last block column of L
   for (int q = lane; q < pr * r; q += 32) Lc[q] = L[(int64_t)(bp * r + q / pr) * ld + (q % pr)];
   __syncwarp();
+  const bool act = lane < r2;
+  const int lrow = (lane < r) ? bp * r + lane : 0;   // row of Lc this lane reads / writes
   for (int i = 0; i < p - 1; ++i) {
-    for (int q = lane; q < r2 * r; q += 32) {
-      const int a = q % r2, c = q / r2;
-      Y[c * r2 + a] = Lc[c * pr + ((a < r) ? bp * r + a : i * r + (a - r))];
+    const int row = (lane < r) ? lrow : i * r + (lane - r);
+    cplx y[8], v[8];
+    cplx tau[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) y[c] = (act && c < r) ? Lc[c * pr + row] : czero();
+    // Householder QR of Y, column by column
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (j >= r) break;
+      const cplx alpha = cmk(__shfl_sync(0xffffffffu, y[j].x, j), __shfl_sync(0xffffffffu, y[j].y, j));
+      const double x2 = warp_sum((act && lane > j) ? cabs2(y[j]) : 0.0);
+      double beta;
+      cplx t, sc;
+      if (x2 == 0.0 && alpha.y == 0.0) {
+        beta = alpha.x; t = czero(); sc = czero();
+      } else {
+        const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + x2);
+        beta = (alpha.x >= 0.0) ? -nrm : nrm;
+        const double ib = recip_nr(beta);
+        t = cmk((beta - alpha.x) * ib, -alpha.y * ib);
+        const double ar = alpha.x - beta, ai = alpha.y;
+        const double id = recip_nr(ar * ar + ai * ai);
+        sc = cmk(ar * id, -ai * id);
+      }
+      const cplx vj = (lane == j) ? cmk(1.0, 0.0) : ((act && lane > j) ? cmul(y[j], sc) : czero());
+      v[j] = vj;
+      tau[j] = t;
+      const cplx tc = cconj(t);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {   // apply H_jᴴ to the columns c > j
+        if (c > j && c < r) {
+          const cplx s = warp_sum(cmulc(vj, y[c]));
+          y[c] = cfms(vj, cmul(tc, s), y[c]);
+        }
+      }
+      if (lane == j) y[j] = cmk(beta, 0.0);
+      else if (lane > j) y[j] = czero();
     }
-    __syncwarp();
-    warp_house_fullq(Y, r2, r2, r, Q, r2, tau);   // Y ← R (upper part), Q full
-    __syncwarp();
+    // Q = H_0 ... H_{r-1} I, row `lane` of Q in q[]
+    cplx q[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) q[c] = (c == lane) ? cmk(1.0, 0.0) : czero();
+#pragma unroll
+    for (int j = 7; j >= 0; --j) {
+      if (j >= r) continue;
+      const cplx vj = v[j], tj = tau[j];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        if (c < r2) {
+          const cplx s = warp_sum(cmulc(vj, q[c]));
+          q[c] = cfms(vj, cmul(tj, s), q[c]);
+        }
+      }
+    }
     cplx* U = Uout + (int64_t)i * r2 * r2;
-    for (int q = lane; q < r2 * r2; q += 32) {
-      const int a = q % r2, c = q / r2;
-      U[c * r2 + a] = cconj(Q[a * r2 + c]);        // U = Qᴴ
+    if (act) {
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        if (c < r2) U[lane * r2 + c] = cconj(q[c]);   // U(c, lane) = conj(Q(lane, c))
     }
-    // new column blocks: [R; 0] (U·Y)
-    for (int q = lane; q < r2 * r; q += 32) {
-      const int a = q % r2, c = q / r2;
-      const int row = (a < r) ? bp * r + a : i * r + (a - r);
-      Lc[c * pr + row] = (a < r && a <= c) ? Y[c * r2 + a] : czero();
+    // new column blocks: [R; 0]
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < r) Lc[c * pr + row] = (lane < r && lane <= c) ? y[c] : czero();
     }
     __syncwarp();
   }
