@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   const int b = blockIdx.x;
   const int n = pr;
   const int nlu = plan.nlu;
-  // shared layout: [A (n × lda cplx)] v v1 w tau (n cplx) yp (16n cplx) d e e2 lam (n doubles)
+  // shared layout: [A (n × lda cplx)] v v1 w tau (n cplx) d e e2 lam (n doubles)
   // LU (nlu·6n doubles) S (gs_cap·n cplx)
   cplx* base = reinterpret_cast<cplx*>(dsm);
   const int lda = plan.lda > 0 ? plan.lda : n;
@@ -138,8 +138,7 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   cplx* v1 = v + n;
   cplx* w = v1 + n;
   cplx* tau = w + n;
-  cplx* yp = tau + n;                     // 16 warps × n partial products of the reduction
-  double* d = reinterpret_cast<double*>(yp + (size_t)16 * n);
+  double* d = reinterpret_cast<double*>(tau + n);
   double* e = d + n;
   double* e2 = e + n;
   double* lam = e2 + n;
@@ -166,13 +165,12 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   __syncthreads();
 
   // 2. Householder tridiagonalisation: for column k reduce A[k+1:, k].  Both triangles of
-  //    the trailing block are kept, so y = τ·A·v is a plain column sweep.  Three barriers
-  //    per column:
-  //      B  warp w sums the columns j ≡ w (mod 16) of the trailing block for all rows
-  //         (lane = row), partial products to yp[w], partial yᴴv per warp;
-  //      R  y_i = Σ_w yp[w][i]; α₂ = −½ τ yᴴv;
-  //      D  A −= v wᴴ + w vᴴ on the trailing block, w = y + α₂·v, columns of warps 1..15;
-  //         warp 0 updates column k+1 and forms the next reflector meanwhile.
+  //    the trailing block are kept, so row i of A is column i conjugated and y = τ·A·v is
+  //    a contiguous sweep per row.  Two barriers per column:
+  //      B  warp w forms y_i for the rows i ≡ w (mod 16) of the trailing block (lanes
+  //         over the columns, one warp sum per row) and its partial of yᴴv;
+  //      D  α₂ = −½ τ yᴴv; A −= v wᴴ + w vᴴ on the trailing block, w = y + α₂·v, columns
+  //         of warps 1..15; warp 0 updates column k+1 and forms the next reflector.
   //    Reflectors alternate between two buffers.
   auto make_reflector = [&](int k) {   // warp 0; column k (rows ≥ k+1) is final
     const int m0 = k + 1;
@@ -215,52 +213,45 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
     const cplx t = tau[k];
     const cplx* vk = (k & 1) ? v1 : v;
     const bool active = (t.x != 0.0 || t.y != 0.0);
-    if (active) {   // B
-      cplx yv = czero();
-      for (int i0 = m0; i0 < n; i0 += 32) {
-        const int i = i0 + lane;
-        const bool ok = i < n;
+    if (active) {   // B: rows m0 + warp + 16t, two at a time
+      cplx yvw = czero();
+      for (int i = m0 + warp; i < n; i += 32) {
+        const int i2 = i + 16;
+        const bool two = i2 < n;
         cplx s0 = czero(), s1 = czero();
-        int j = m0 + warp;
-        for (; j + 16 < n; j += 32) {
-          if (ok) {
-            s0 = cfma(A[j * lda + i], vk[j], s0);
-            s1 = cfma(A[(j + 16) * lda + i], vk[j + 16], s1);
+        for (int j = m0 + lane; j < n; j += 32) {
+          const cplx vj = vk[j];
+          s0 = cfmac(A[i * lda + j], vj, s0);            // conj(A(j,i)) v_j = A(i,j) v_j
+          if (two) s1 = cfmac(A[i2 * lda + j], vj, s1);
+        }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        if (lane == 0) {
+          const cplx y0 = cmul(t, s0);
+          w[i] = y0;
+          yvw = cfmac(y0, vk[i], yvw);                   // Σ conj(y_i) v_i
+          if (two) {
+            const cplx y1 = cmul(t, s1);
+            w[i2] = y1;
+            yvw = cfmac(y1, vk[i2], yvw);
           }
         }
-        if (j < n && ok) s0 = cfma(A[j * lda + i], vk[j], s0);
-        if (ok) {
-          const cplx yi = cmul(t, cadd(s0, s1));
-          yp[warp * n + i] = yi;
-          yv = cfmac(yi, vk[i], yv);
-        }
       }
-      yv = warp_sum(yv);
-      if (lane == 0) yvp[warp] = yv;
+      if (lane == 0) yvp[warp] = yvw;
     }
     __syncthreads();
     cplx a2 = czero();
-    if (active) {   // R
-      for (int i = m0 + threadIdx.x; i < n; i += blockDim.x) {
-        cplx y0 = yp[i], y1 = yp[n + i], y2 = yp[2 * n + i], y3 = yp[3 * n + i];
+    if (active) {   // α₂ from the 16 warp partials: a fixed butterfly, lane 0's value broadcast
+      cplx yv = yvp[lane & 15];
 #pragma unroll
-        for (int q = 4; q < 16; q += 4) {
-          y0 = cadd(y0, yp[q * n + i]);
-          y1 = cadd(y1, yp[(q + 1) * n + i]);
-          y2 = cadd(y2, yp[(q + 2) * n + i]);
-          y3 = cadd(y3, yp[(q + 3) * n + i]);
-        }
-        w[i] = cadd(cadd(y0, y1), cadd(y2, y3));
+      for (int o = 8; o > 0; o >>= 1) {
+        yv.x += __shfl_xor_sync(0xffffffffu, yv.x, o);
+        yv.y += __shfl_xor_sync(0xffffffffu, yv.y, o);
       }
-      cplx s0 = cadd(yvp[0], yvp[1]), s1 = cadd(yvp[2], yvp[3]);
-#pragma unroll
-      for (int q = 4; q < 16; q += 4) {
-        s0 = cadd(s0, cadd(yvp[q], yvp[q + 1]));
-        s1 = cadd(s1, cadd(yvp[q + 2], yvp[q + 3]));
-      }
-      a2 = cscale(cmul(t, cadd(s0, s1)), -0.5);
+      yv.x = __shfl_sync(0xffffffffu, yv.x, 0);
+      yv.y = __shfl_sync(0xffffffffu, yv.y, 0);
+      a2 = cscale(cmul(t, yv), -0.5);
     }
-    __syncthreads();
     if (warp == 0) {   // D, column m0 (all trailing rows), then the next reflector
       if (active) {
         const cplx vj = vk[m0], wj = cfma(a2, vj, w[m0]);
@@ -489,7 +480,7 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
 // as fit.
 inline HeevPlan heev_plan(int pr, size_t avail) {
   HeevPlan p{};
-  const size_t vec = (size_t)(4 + 16) * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
+  const size_t vec = (size_t)4 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
   int lda = pr + ((4 - pr % 8) + 8) % 8;                    // ≡ 4 (mod 8)
   size_t need = vec + (size_t)pr * lda * sizeof(cplx);
   const size_t lu1 = (size_t)6 * pr * sizeof(double);
