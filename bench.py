@@ -46,7 +46,7 @@ METRIC = "σ_min grid pts/s (psTriRecy, sprand N=4000, 200×200 grid, k=20, tol 
 GRID = (0.45, 0.55, 0.0, 0.1, 200, 200, 20)
 N_MAT = 4000
 NORMC = 3.2
-NCU_TRSM_TRAFFIC = None   # bytes per k_trsm_half launch from an ncu capture (n = 4000); None until captured
+NCU_TRSM_TRAFFIC = 132.54e6 + 3.81e6   # DRAM bytes per k_trsm_half launch (ncu, n = 4000, k = 6)
 
 
 def parse():

@@ -202,6 +202,19 @@ int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
                           const rls_lobpcg_control* control, rls_c64* X_out,
                           double* sigma_r, double* sigma, int64_t* it);
 
+/* ---- gradient -------------------------------------------------------------------- */
+
+/* σ = σ_min(T − zI) = σ_min(C − zI) at one point and its derivatives with respect to
+ * z = x + iy.  No counterpart in the reference.  From the right singular vector v of
+ * R = T − zI (v0, n values, e.g. the first column of rls_lobpcg_svd_invtri's X_out,
+ * polished by refine_steps steps of inverse iteration on RᴴR) and u = R v / σ:
+ *   ∂σ/∂x = −Re(uᴴv),  ∂σ/∂y = Im(uᴴv).
+ * u_out and v_out (n values each, may be NULL) receive u and v in the Schur basis; with
+ * C = Q T Qᴴ the singular vectors of C − zI are Q u and Q v, and ∂σ/∂C_ij =
+ * Re(conj((Qu)_i) (Qv)_j).  Host memory. */
+int rls_sigma_grad(rls_ctx* ctx, rls_c64 z, const rls_c64* v0, int refine_steps, double* sigma,
+                   double* dsdx, double* dsdy, rls_c64* u_out, rls_c64* v_out);
+
 /* ---- allocation-free utility ---------------------------------------------------- */
 
 /* R (k × k, upper triangular, leading dimension k) of the QR factorisation of the

@@ -70,6 +70,7 @@ SIGNATURES = {
     "rls_lobpcg_svd_invtri": (C.c_int, [P, c64, P, C.POINTER(rls_lobpcg_control), P, P, P, P]),
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_tsqr_r_noalloc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int, P, P]),
+    "rls_sigma_grad": (C.c_int, [P, c64, P, C.c_int, P, P, P, P, P]),
     "rls_ctx_launches": (C.c_int64, [P]),
     "rls_ctx_set_ritz_basis": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_batch": (C.c_int, [P, C.c_int]),

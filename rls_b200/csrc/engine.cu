@@ -49,6 +49,7 @@ struct rls_ctx {
   cplx* Dinv = nullptr;     // nb tiles
   cplx* G = nullptr;        // tiles of the block-row scaled factor D⁻¹T (k_trsm_scale)
   cplx* trsm_u = nullptr;   // n_pad × 8: the adjoint solve's chain values
+  cplx* grad_ws = nullptr;  // 3 × n_pad: rls_sigma_grad's vectors
   cplx z_dinv = cmk(NAN, NAN);
   int* flags = nullptr;     // 2·nb (one per half block row)
   int* ticket = nullptr;    // 1
@@ -1340,11 +1341,13 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   // drop an old operator and space
-  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
+  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->grad_ws,
+                  (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
                   (void*)ctx->colpart, (void*)ctx->trmm_uO[0], (void*)ctx->trmm_us[0], (void*)ctx->trmm_Ofirst[0],
                   (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
                   (void*)ctx->trmm_Ofirst[1], (void*)ctx->trmm_Ocount[1]})
     dfree(ctx, q);
+  ctx->grad_ws = nullptr;
   release_space(ctx);
   ctx->n = n;
   ctx->nb = (int)((n + TILE - 1) / TILE);
@@ -1438,6 +1441,90 @@ extern "C" int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
   RET(sync_and_check(ctx));
   if (sigma) *sigma = res.sigma;
   if (it) *it = res.it;
+  return RLS_OK;
+}
+
+// y = a·x + b·y on one column of n rows.
+__global__ void k_axpby(int64_t n, cplx a, const cplx* __restrict__ x, cplx b, cplx* y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = cfma(a, x[i], cmul(b, y[i]));
+}
+
+namespace {
+// ||x||₂ of one n_pad column through the Gram kernel (one host round trip).
+int col_norm(rls_ctx* ctx, const cplx* x, double* out) {
+  const int64_t np = ctx->n_pad;
+  RET(gram(ctx, np, x, np, 1, x, np, 1, ctx->small[0], 1));
+  cplx h;
+  RET(d2h(ctx, &h, ctx->small[0], 1));
+  *out = std::sqrt(std::max(h.x, 0.0));
+  return RLS_OK;
+}
+int axpby(rls_ctx* ctx, cplx a, const cplx* x, cplx b, cplx* y) {
+  const int64_t np = ctx->n_pad;
+  k_axpby<<<(unsigned)((np + 255) / 256), 256, 0, ctx->stream>>>(np, a, x, b, y);
+  return check_launch(ctx, "k_axpby");
+}
+}  // namespace
+
+extern "C" int rls_sigma_grad(rls_ctx* ctx, rls_c64 z, const rls_c64* v0, int refine_steps, double* sigma,
+                              double* dsdx, double* dsdy, rls_c64* u_out, rls_c64* v_out) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->T) {
+    set_err(ctx, "no operator uploaded (call rls_set_schur first)");
+    return RLS_ERR_STATE;
+  }
+  if (!v0 || refine_steps < 0 || refine_steps > 64) {
+    set_err(ctx, "rls_sigma_grad: v0 must be given and 0 <= refine_steps <= 64");
+    return RLS_ERR_ARG;
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->V) RET(setup_space(ctx, 1, 1));
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  if (!ctx->grad_ws) RET(dalloc_t(ctx, &ctx->grad_ws, (size_t)3 * np));
+  cplx* v = ctx->grad_ws;
+  cplx* t1 = v + np;
+  cplx* t2 = t1 + np;
+  const cplx zz = cmk(z.re, z.im);
+  CK(cudaMemsetAsync(v, 0, sizeof(cplx) * np, ctx->stream));
+  CK(cudaMemcpyAsync(v, v0, sizeof(cplx) * n, cudaMemcpyHostToDevice, ctx->stream));
+  double nrm = 0.0;
+  RET(col_norm(ctx, v, &nrm));
+  if (!(nrm > 0.0) || !std::isfinite(nrm)) {
+    set_err(ctx, "rls_sigma_grad: v0 is zero or not finite");
+    return RLS_ERR_ARG;
+  }
+  RET(axpby(ctx, cmk(1.0 / nrm, 0.0), v, czero(), v));
+  // inverse iteration on RᴴR (R = T − zI): v ← R⁻¹ R⁻ᴴ v / ||·||
+  for (int s = 0; s < refine_steps; ++s) {
+    RET(trsm(ctx, zz, 1, v, t1, np, 1));
+    RET(trsm(ctx, zz, 0, t1, t2, np, 1));
+    RET(col_norm(ctx, t2, &nrm));
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) {
+      set_err(ctx, "rls_sigma_grad: inverse iteration broke down");
+      return RLS_ERR_BREAKDOWN;
+    }
+    RET(axpby(ctx, cmk(1.0 / nrm, 0.0), t2, czero(), v));
+  }
+  // u = R v / σ, σ = ||R v||
+  RET(trmm(ctx, 0, v, t1, np, 1));
+  RET(axpby(ctx, cneg(zz), v, cmk(1.0, 0.0), t1));
+  double sg = 0.0;
+  RET(col_norm(ctx, t1, &sg));
+  if (!(sg > 0.0)) {
+    set_err(ctx, "rls_sigma_grad: R v = 0 (z is an eigenvalue)");
+    return RLS_ERR_BREAKDOWN;
+  }
+  RET(axpby(ctx, cmk(1.0 / sg, 0.0), t1, czero(), t1));
+  RET(gram(ctx, np, t1, np, 1, v, np, 1, ctx->small[0], 1));   // uᴴv
+  cplx w;
+  RET(d2h(ctx, &w, ctx->small[0], 1));
+  if (u_out) CK(cudaMemcpyAsync(u_out, t1, sizeof(cplx) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (v_out) CK(cudaMemcpyAsync(v_out, v, sizeof(cplx) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  RET(sync_and_check(ctx));
+  if (sigma) *sigma = sg;
+  if (dsdx) *dsdx = -w.x;   // dσ = Re(uᴴ dR v), dR = −dz·I
+  if (dsdy) *dsdy = w.y;
   return RLS_OK;
 }
 

@@ -112,12 +112,14 @@ class LobpcgSvdControl:
                                   self.conv_range[0], self.conv_range[1])
 
 
-def pre_process(C_) -> np.ndarray:
+def pre_process(C_, return_q: bool = False):
     """psTriRecy.jl:6-14 (square dense branch): upper-triangular complex Schur factor.
 
     Host LAPACK zgees through SciPy, as the reference's ``schur(C)``.  A sparse C is
     densified first: σ_min(C − zI) is invariant under the unitary similarity, so the
-    Schur path computes the same σ as the reference's sparse QR path.
+    Schur path computes the same σ as the reference's sparse QR path.  With
+    ``return_q`` the Schur vectors Q (C = Q T Qᴴ) are returned too, for the gradient
+    with respect to C (Engine.sigma_grad).
     """
     import scipy.linalg as sla
     import scipy.sparse as sp
@@ -126,8 +128,8 @@ def pre_process(C_) -> np.ndarray:
     A = np.asarray(C_, dtype=np.complex128)
     if A.ndim != 2 or A.shape[0] != A.shape[1]:
         raise DimensionMismatch(-2, f"pre_process only supports square matrices here, got size {A.shape}")
-    T, _ = sla.schur(A, output="complex", check_finite=True)
-    return np.triu(T)
+    T, Q = sla.schur(A, output="complex", check_finite=True)
+    return (np.triu(T), Q) if return_q else np.triu(T)
 
 
 class SchurFactor:
@@ -267,6 +269,35 @@ class Engine:
         check(lib().rls_lobpcg_svd_invtri(self._h, c64(z.real, z.imag), ptr(x0), C.byref(cc), ptr(X), ptr(sr),
                                           C.byref(s), C.byref(it)), self._h)
         return s.value, it.value, X, sr
+
+    def sigma_grad(self, z: complex, v0, refine_steps: int = 2, Q=None, pattern=None):
+        """σ_min(C − zI) and its gradient at z (no reference counterpart).
+
+        v0 (n values) approximates the right singular vector of T − zI (e.g. the first
+        Ritz vector of lobpcg_svd_invtri).  Returns a dict with sigma, dsdx = ∂σ/∂Re z,
+        dsdy = ∂σ/∂Im z and the Schur-basis singular vectors u, v.  With the Schur vectors
+        Q of C (C = Q T Qᴴ, from pre_process) it adds uC = Q u, vC = Q v and dsdC =
+        Re(conj(uC_i) vC_j): on the (rows, cols) index arrays of ``pattern`` when given
+        (the nnz of a sparse C), else the dense n × n matrix.
+        """
+        v0 = np.ascontiguousarray(np.asarray(v0, dtype=np.complex128).reshape(-1))
+        if v0.shape[0] != self.n:
+            raise DimensionMismatch(-2, f"v0 has {v0.shape[0]} entries, the operator {self.n}")
+        u = np.zeros(self.n, dtype=np.complex128)
+        v = np.zeros(self.n, dtype=np.complex128)
+        sg, dx, dy = C.c_double(), C.c_double(), C.c_double()
+        check(lib().rls_sigma_grad(self._h, c64(z.real, z.imag), ptr(v0), int(refine_steps), C.byref(sg),
+                                   C.byref(dx), C.byref(dy), ptr(u), ptr(v)), self._h)
+        out = {"sigma": sg.value, "dsdx": dx.value, "dsdy": dy.value, "u": u, "v": v}
+        if Q is not None:
+            uC, vC = Q @ u, Q @ v
+            out["uC"], out["vC"] = uC, vC
+            if pattern is not None:
+                rows, cols = pattern
+                out["dsdC"] = np.real(np.conj(uC[rows]) * vC[cols])
+            else:
+                out["dsdC"] = np.real(np.outer(np.conj(uC), vC))
+        return out
 
 
 _engines = {}
