@@ -8,23 +8,28 @@ as the reference's preprocess_time_ns), 200 × 200 grid on [0.45,0.55]×[0,0.1],
 k = 20, PsTriRecyControl(normC=3.2, tol=1e-4, p_min=1, p=60, recy_tau=1.6),
 complex128 throughout.
 
-A step is `--chunk` consecutive points of the grid's traversal order, processed
-with the recycled space carried from the previous step exactly as the reference's
-loop carries it; W warm-up steps, then K timed steps.  The Schur factor (256 MB)
+A step is `--chunk` consecutive points of each lane's part of the traversal,
+processed with the lane's recycled space carried from the previous step exactly as
+the reference's loop carries it; W warm-up steps, then K timed steps.  The Schur factor (256 MB)
 is larger than L2, so every step streams it from HBM.
 
-  value : points / device time of the K timed steps (CUDA events on the engine's
-          stream), Schur factor resident in HBM.
-  e2e   : a fresh context through the public C ABI with host buffers: upload of
-          the Schur factor from host memory plus steps 0..W+K-1 (grid points in,
-          σ out), wall clock.
+  value : points / device time of the K timed steps, Schur factor resident in HBM.
+          The traversal is split on strip boundaries into --lanes concurrent lanes
+          (rls_b200.Lanes: one context, stream and host thread per lane); a step is
+          --chunk lane-local points in every lane; device time is the max over the
+          lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
+          with one lane (the reference's single recycled space).
+  e2e   : fresh lane contexts through the public C ABI with host buffers: upload
+          of the Schur factor from host memory to every lane plus steps 0..W+K-1
+          (grid points in, σ out), wall clock.
   --impl reference : the CPU restatement (oracle/, the reference's algorithm with
           LAPACK through SciPy on all host cores) on the same traversal, each step
           a bounded sample of --ref-chunk points.
 
-Multi-GPU (torchrun): every rank runs its own traversal starting at a different
-strip of the grid (independent recycled spaces, weak scaling); the only
-collective is the final max-over-ranks of the timings.
+Multi-GPU (torchrun): every rank takes a contiguous share of the grid's strips and
+splits it into lanes (independent recycled spaces, weak scaling); the only
+collectives are the broadcast of T before timing and the max over ranks of the
+timings.
 """
 from __future__ import annotations
 
@@ -55,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--chunk", type=int, default=200, help="grid points per step")
+    ap.add_argument("--chunk", type=int, default=200, help="grid points per lane per step")
+    ap.add_argument("--lanes", type=int, default=8, help="concurrent grid lanes per GPU")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
@@ -245,18 +251,19 @@ def run_ours(args):
         del buf
 
     rec = R.recursion_grid(*GRID)
-    off = strip_offset(rank, world, len(rec.Z), GRID[4] * GRID[6])
+    strip = GRID[4] * GRID[6]
+    off = strip_offset(rank, world, len(rec.Z), strip)
+    end = strip_offset(rank + 1, world, len(rec.Z), strip) if rank + 1 < world else len(rec.Z)
     sub = R.Recursion(*GRID)
-    sub.Z = np.ascontiguousarray(rec.Z[off:])
+    sub.Z = np.ascontiguousarray(rec.Z[off:end])
+    lanes = max(1, min(args.lanes, len(sub.Z) // strip))
     ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
     rng = np.random.default_rng(1 + rank)
     X0 = rng.random((args.n, 6)) + 1j * rng.random((args.n, 6))
     s = args.chunk
     need = (args.warmup + args.steps) * s
-    if need > len(sub.Z):
-        raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds the {len(sub.Z)} points of this rank")
 
-    # plain per-point drop-in (no speculative batching) on one step, for comparison
+    # plain per-point drop-in (no speculative batching, one lane) on one step, for comparison
     plain = None
     if args.plain_steps > 0:
         engp = Engine(local)
@@ -274,77 +281,105 @@ def run_ours(args):
             engp.pstrirecy_range(sub, ctl, a, a + s, sigp, stp, cstp)
         torch.cuda.synchronize()
         plain = {"value": args.plain_steps * s / (time.perf_counter() - t0), "unit": "pts/s",
-                 "steps": args.plain_steps, "mode": "one recycle step per launch sequence (set_batch(1))"}
+                 "steps": args.plain_steps, "mode": "one lane, one recycle step per launch sequence (set_batch(1))"}
         engp.close()
 
-    eng = Engine(local)
-    eng.set_schur(T)
-    sigma = np.full(len(sub.Z), np.nan)
-    st = PsTriRecyStats.alloc(len(sub.Z))
-    cst = eng.stats_struct(st)
-    for w in range(args.warmup):
-        eng.pstrirecy_range(sub, ctl, w * s, (w + 1) * s, sigma, st, cst, X0=X0)
-    eng.set_profile(True)
-    stream = torch.cuda.ExternalStream(eng.stream_ptr())
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
-                       os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
-    clk.start()
-    time.sleep(0.3)
-    l0 = eng.launches()
-    ev0.record(stream)
-    for k in range(args.steps):
-        a = (args.warmup + k) * s
-        eng.pstrirecy_range(sub, ctl, a, a + s, sigma, st, cst)
-    ev1.record(stream)
-    ev1.synchronize()
-    torch.cuda.synchronize()
-    l1 = eng.launches()
-    clk.stop()
-    if world > 1:
-        dist.barrier()
-    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
-    timed = slice(args.warmup * s, (args.warmup + args.steps) * s)
-    refines = int(np.sum(st.refine_it[timed] > 0))
-    prof = {k: eng.profile(k) for k in range(4)}
-    waits = eng.profile(4)
+    def timed_lanes(nl, profile):
+        """W warm-up and K timed steps of `nl` concurrent lanes; a step is `s` lane-local points
+        in every lane.  Device time = max over the lanes' streams of CUDA-event spans."""
+        ls = R.Lanes(nl, local, T)
+        offs = ls.offsets(sub)
+        if need > int(np.min(np.diff(offs))):
+            raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds a lane of {int(np.min(np.diff(offs)))} points")
+        sig = np.full(len(sub.Z), np.nan)
+        st = PsTriRecyStats.alloc(len(sub.Z))
+        cst = ls.engines[0].stats_struct(st)
+        for w in range(args.warmup):
+            ls.pstrirecy_range(sub, ctl, w * s, (w + 1) * s, sig, st, cst, X0=X0)
+        if profile:
+            ls.set_profile(True)
+        streams = [torch.cuda.ExternalStream(p) for p in ls.streams()]
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = None
+        if profile:
+            clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
+                               os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
+            clk.start()
+            time.sleep(0.3)
+        l0 = ls.launches()
+        for e, st_ in zip(ev0, streams):
+            e.record(st_)
+        for k in range(args.steps):
+            a = (args.warmup + k) * s
+            ls.pstrirecy_range(sub, ctl, a, a + s, sig, st, cst)
+        for e, st_ in zip(ev1, streams):
+            e.record(st_)
+        for e in ev1:
+            e.synchronize()
+        torch.cuda.synchronize()
+        l1 = ls.launches()
+        if clk is not None:
+            clk.stop()
+        if world > 1:
+            dist.barrier()
+        ms = max(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
+        timed = np.concatenate([np.arange(o + args.warmup * s, o + need) for o in offs[:-1]])
+        res = {"ms": max_over_ranks(ms, world, "cuda"), "launches": int(l1 - l0), "sig": sig, "timed": timed,
+               "refines": int(np.sum(st.refine_it[timed] > 0)), "clk": clk, "offs": offs}
+        if profile:
+            res["prof"] = {k: ls.profile(k) for k in range(4)}
+            res["waits"] = ls.profile(4)
+        ls.close()
+        return res
 
-    # end to end through the public C ABI on a fresh context, host buffers in and out
+    single = timed_lanes(1, False) if lanes > 1 else None
+    main = timed_lanes(lanes, True)
+    ms_max = main["ms"]
+    sigma, timed, refines, prof, waits, clk = (main["sig"], main["timed"], main["refines"], main["prof"],
+                                               main["waits"], main["clk"])
+
+    # end to end through the public API on fresh contexts: host buffers, T uploaded to every lane
     e2e = None
     if not args.no_e2e:
-        eng2 = Engine(local)
-        sigma2 = np.full(len(sub.Z), np.nan)
-        st2 = PsTriRecyStats.alloc(len(sub.Z))
-        cst2 = eng2.stats_struct(st2)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        eng2.set_schur(T)
+        ls2 = R.Lanes(lanes, local, T)
+        sigma2 = np.full(len(sub.Z), np.nan)
+        st2 = PsTriRecyStats.alloc(len(sub.Z))
+        cst2 = ls2.engines[0].stats_struct(st2)
         for k in range(args.warmup + args.steps):
-            eng2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sigma2, st2, cst2, X0=X0)
+            ls2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sigma2, st2, cst2, X0=X0)
         el = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        ls2.close()
         nsteps = args.warmup + args.steps
         T_bytes = args.n * args.n * 16
-        e2e = {"value": world * nsteps * s / el, "unit": "pts/s",
-               "h2d_bytes_per_step": int((T_bytes + nsteps * s * 16) / nsteps),
-               "d2h_bytes_per_step": int(s * 8),
-               "span": f"upload of T + steps 0..{nsteps - 1} of the traversal"}
-        same = np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12)
-        e2e["matches_device_run"] = bool(same)
-        eng2.close()
+        e2e = {"value": world * lanes * nsteps * s / el, "unit": "pts/s",
+               "h2d_bytes_per_step": int((lanes * T_bytes + lanes * nsteps * s * 16) / nsteps),
+               "d2h_bytes_per_step": int(lanes * s * 8),
+               "span": f"upload of T to {lanes} lane contexts + steps 0..{nsteps - 1}"}
+        e2e["matches_device_run"] = bool(np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12))
 
     out = base_line(args, world)
-    value = world * args.steps * s / (ms_max / 1e3)
+    value = world * lanes * args.steps * s / (ms_max / 1e3)
     out.update({"value": value, "ms_per_step": ms_max / args.steps})
-    out["config"]["points_per_step"] = s
-    out["config"]["parallelism"] = f"grid strips x{world} (independent traversals)"
-    out["config"]["refine_fraction_timed"] = refines / (args.steps * s)
+    out["config"]["points_per_step"] = lanes * s
+    out["config"]["lanes"] = lanes
+    out["config"]["parallelism"] = (f"grid strips: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
+                                    "(independent traversals from strip starts)")
+    out["config"]["refine_fraction_timed"] = refines / (lanes * args.steps * s)
     out["preprocess_s"] = pre_s
-    out["gpu_launches"] = int(l1 - l0)
+    out["gpu_launches"] = main["launches"]
     out["clocks"] = clk.summary()
+    if single is not None:
+        out["single_lane"] = {"value": world * args.steps * s / (single["ms"] / 1e3), "unit": "pts/s",
+                              "mode": "one traversal per GPU (the reference's single recycled space)",
+                              "matches_lanes_on_first_lane": bool(np.array_equal(
+                                  single["sig"][single["timed"][:args.steps * s]],
+                                  sigma[timed[:args.steps * s]]))}
     # roofline of the dominant profiled kernel
     names = {0: "k_trsm_half (R⁻¹/R⁻ᴴ on T−zI, block-row scaled factor)", 1: "k_heev_rr (projected eigensolve)",
              2: "k_gemm_rows (recycle X/W product)", 3: "k_trmm_partial+reduce (T·V, Tᴴ·[J5 V])"}
@@ -380,12 +415,12 @@ def run_ours(args):
         out["e2e"] = e2e
     if plain is not None:
         out["plain_per_point"] = plain
-        same = np.allclose(sigp[timed.start:timed.start + args.plain_steps * s],
-                           sigma[timed.start:timed.start + args.plain_steps * s], rtol=0, atol=1e-10)
+        a0 = args.warmup * s   # lane 0 starts at the rank's first point, as the plain run does
+        same = np.allclose(sigp[a0:a0 + args.plain_steps * s], sigma[a0:a0 + args.plain_steps * s], rtol=0,
+                           atol=1e-10)
         out["plain_per_point"]["matches_batched"] = bool(same)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    eng.close()
     if world > 1:
         dist.destroy_process_group()
 

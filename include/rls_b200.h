@@ -193,6 +193,27 @@ int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const 
                               const rls_pstrirecy_control* control, const rls_c64* X0, int64_t i_begin,
                               int64_t i_end, double* sigma_min, rls_pstrirecy_stats* stats);
 
+/* Concurrent grid lanes on one GPU.  No reference counterpart: the reference walks the
+ * whole traversal with one recycled space.  The traversal Z (nZ points) is split into
+ * nlanes contiguous ranges that start on strip boundaries of the recursion grid (n_x·k
+ * points per strip; rls_lane_offsets gives the split), and lane l runs psTriRecy on its
+ * range from an empty recycled space on context ctxs[l] (its own stream, operator
+ * uploaded with rls_set_schur), each lane in its own host thread.  Each lane is exactly
+ * the reference's run on that sub-grid; lanes keep the GPU busy where one traversal's
+ * latency-bound kernels leave most SMs idle.  sigma_min and the stats arrays are the
+ * full-length arrays; the stats scalars are summed over lanes.  The _range form runs,
+ * in every lane, the lane-local points j_begin..j_end-1 (a call with j_begin > 0
+ * continues each lane's run).  A log sink set on a context is called from that lane's
+ * thread. */
+int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets /* nlanes+1 */);
+int rls_pstrirecy_schur_lanes(rls_ctx* const* ctxs, int nlanes, const rls_c64* Z, int64_t nZ,
+                              const rls_grid* g, const rls_pstrirecy_control* control,
+                              const rls_c64* X0, double* sigma_min, rls_pstrirecy_stats* stats);
+int rls_pstrirecy_schur_lanes_range(rls_ctx* const* ctxs, int nlanes, const rls_c64* Z, int64_t nZ,
+                                    const rls_grid* g, const rls_pstrirecy_control* control,
+                                    const rls_c64* X0, int64_t j_begin, int64_t j_end,
+                                    double* sigma_min, rls_pstrirecy_stats* stats);
+
 /* lobpcgSvd (src/core/lobpcgSvd.jl:365-477) on C = InvMat(adjoint(T − zI)) with
  * K = I, as psTriRecy calls it at psTriRecy.jl:797-808.  X0 (n × r) may be
  * NULL.  X_out (n × r, may be NULL) receives keep.S[:, 1:r]; sigma_r (r

@@ -71,6 +71,12 @@ SIGNATURES = {
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_tsqr_r_noalloc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int, P, P]),
     "rls_sigma_grad": (C.c_int, [P, c64, P, C.c_int, P, P, P, P, P]),
+    "rls_lane_offsets": (C.c_int, [C.POINTER(rls_grid), C.c_int64, C.c_int, P]),
+    "rls_pstrirecy_schur_lanes": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
+                                            C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),
+    "rls_pstrirecy_schur_lanes_range": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
+                                                  C.POINTER(rls_pstrirecy_control), P, C.c_int64, C.c_int64, P,
+                                                  C.POINTER(rls_pstrirecy_stats)]),
     "rls_ctx_launches": (C.c_int64, [P]),
     "rls_ctx_set_ritz_basis": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_batch": (C.c_int, [P, C.c_int]),

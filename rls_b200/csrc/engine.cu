@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rls_b200.h"
@@ -140,6 +141,8 @@ struct rls_ctx {
     double bytes = 0.0;
     std::vector<double> pending_bytes;
   } kprof[4];
+
+  rls_pstrirecy_stats lane_stats{};   // this context's run as one lane of rls_pstrirecy_schur_lanes_range
 
   std::vector<DevBuf> owned;
 };
@@ -1745,6 +1748,87 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
                                    const rls_pstrirecy_control* ctl, const rls_c64* X0, double* sigma_min,
                                    rls_pstrirecy_stats* st) {
   return rls_pstrirecy_schur_range(ctx, Z, nZ, g, ctl, X0, 0, nZ, sigma_min, st);
+}
+
+extern "C" int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets) {
+  if (!g || nZ < 0 || nlanes < 1 || !offsets) return RLS_ERR_ARG;
+  const int64_t strip = std::max<int64_t>(1, g->n_x * std::max<int64_t>(g->k, 1));
+  const int64_t nstrips = std::max<int64_t>(1, (nZ + strip - 1) / strip);
+  if (nlanes > nstrips) {
+    g_create_err = "rls_lane_offsets: " + std::to_string(nlanes) + " lanes for " + std::to_string(nstrips) +
+                   " strips of the grid";
+    return RLS_ERR_DIM;
+  }
+  for (int l = 0; l < nlanes; ++l) offsets[l] = std::min<int64_t>(nZ, ((int64_t)l * nstrips / nlanes) * strip);
+  offsets[nlanes] = nZ;
+  return RLS_OK;
+}
+
+extern "C" int rls_pstrirecy_schur_lanes_range(rls_ctx* const* ctxs, int nlanes, const rls_c64* Z, int64_t nZ,
+                                               const rls_grid* g, const rls_pstrirecy_control* ctl,
+                                               const rls_c64* X0, int64_t j_begin, int64_t j_end,
+                                               double* sigma_min, rls_pstrirecy_stats* st) {
+  if (!ctxs || nlanes < 1 || nlanes > 64 || !Z || !g || !ctl || !sigma_min || j_begin < 0 || j_end < j_begin)
+    return RLS_ERR_ARG;
+  for (int l = 0; l < nlanes; ++l)
+    if (!ctxs[l]) return RLS_ERR_ARG;
+  std::vector<int64_t> off((size_t)nlanes + 1);
+  int rc = rls_lane_offsets(g, nZ, nlanes, off.data());
+  if (rc != RLS_OK) {
+    set_err(ctxs[0], "%s", g_create_err.c_str());
+    return rc;
+  }
+  std::vector<int> status((size_t)nlanes, RLS_OK);
+  auto lane = [&](int l) {
+    rls_ctx* c = ctxs[l];
+    const int64_t o = off[l], len = off[l + 1] - off[l];
+    const int64_t b = std::min(j_begin, len), e = std::min(j_end, len);
+    if (b >= e) return;
+    rls_pstrirecy_stats& ls = c->lane_stats;     // scalars persist across range calls
+    ls.p_count = (st && st->p_count) ? st->p_count + o : nullptr;
+    ls.r_recy = (st && st->r_recy) ? st->r_recy + o : nullptr;
+    ls.pts = (st && st->pts) ? st->pts + o : nullptr;
+    ls.M_vec_apps = (st && st->M_vec_apps) ? st->M_vec_apps + o : nullptr;
+    ls.M_vec_apps_no_recycle = (st && st->M_vec_apps_no_recycle) ? st->M_vec_apps_no_recycle + o : nullptr;
+    ls.R_vec_apps = (st && st->R_vec_apps) ? st->R_vec_apps + o : nullptr;
+    ls.refine_it = (st && st->refine_it) ? st->refine_it + o : nullptr;
+    status[l] = rls_pstrirecy_schur_range(c, Z + o, len, g, ctl, X0, b, e, sigma_min + o, &ls);
+  };
+  if (nlanes == 1) {
+    lane(0);
+  } else {
+    std::vector<std::thread> th;
+    th.reserve((size_t)nlanes);
+    for (int l = 0; l < nlanes; ++l) th.emplace_back(lane, l);
+    for (auto& t : th) t.join();
+  }
+  for (int l = 0; l < nlanes; ++l)
+    if (status[l] != RLS_OK) {
+      if (l > 0) set_err(ctxs[0], "lane %d: %s", l, ctxs[l]->err.c_str());
+      return status[l];
+    }
+  if (st) {
+    st->preprocess_time_ns = st->recycle_time_ns = st->qr_time_ns = st->refine_time_ns = st->update_time_ns = 0;
+    st->n_it = st->n_pts = 0;
+    st->mv_stats_available = 1;
+    for (int l = 0; l < nlanes; ++l) {
+      const rls_pstrirecy_stats& ls = ctxs[l]->lane_stats;
+      if (off[l + 1] - off[l] == 0) continue;
+      st->recycle_time_ns += ls.recycle_time_ns;
+      st->qr_time_ns += ls.qr_time_ns;
+      st->refine_time_ns += ls.refine_time_ns;
+      st->update_time_ns += ls.update_time_ns;
+      st->n_it += ls.n_it;
+      st->n_pts += ls.n_pts;
+    }
+  }
+  return RLS_OK;
+}
+
+extern "C" int rls_pstrirecy_schur_lanes(rls_ctx* const* ctxs, int nlanes, const rls_c64* Z, int64_t nZ,
+                                         const rls_grid* g, const rls_pstrirecy_control* ctl, const rls_c64* X0,
+                                         double* sigma_min, rls_pstrirecy_stats* st) {
+  return rls_pstrirecy_schur_lanes_range(ctxs, nlanes, Z, nZ, g, ctl, X0, 0, nZ, sigma_min, st);
 }
 
 extern "C" void* rls_ctx_stream(rls_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

@@ -300,6 +300,86 @@ class Engine:
         return out
 
 
+class Lanes:
+    """Concurrent grid lanes on one GPU (rls_pstrirecy_schur_lanes_range): one Engine per
+    lane, each with the Schur factor uploaded; the traversal is split on strip boundaries
+    of the recursion grid and every lane runs psTriRecy from an empty recycled space on
+    its part, in its own host thread inside the library.  No reference counterpart."""
+
+    def __init__(self, lanes: int, device: int = 0, T=None):
+        if lanes < 1:
+            raise ArgumentError(-1, f"lanes must be >= 1, got {lanes}")
+        self.engines = [Engine(device) for _ in range(lanes)]
+        self._arr = (C.c_void_p * lanes)(*[e._h for e in self.engines])
+        if T is not None:
+            self.set_schur(T)
+
+    @property
+    def n(self):
+        return self.engines[0].n
+
+    def set_schur(self, T):
+        for e in self.engines:
+            e.set_schur(T)
+
+    def set_batch(self, max_points: int):
+        for e in self.engines:
+            e.set_batch(max_points)
+
+    def set_profile(self, on: bool):
+        for e in self.engines:
+            e.set_profile(on)
+
+    def profile(self, kernel: int):
+        cnt, ms, work = 0, 0.0, 0.0
+        for e in self.engines:
+            c, m, w = e.profile(kernel)
+            cnt, ms, work = cnt + c, ms + m, work + w
+        return cnt, ms, work
+
+    def launches(self) -> int:
+        return sum(e.launches() for e in self.engines)
+
+    def streams(self):
+        return [e.stream_ptr() for e in self.engines]
+
+    def offsets(self, rec: Recursion):
+        off = np.zeros(len(self.engines) + 1, dtype=np.int64)
+        g = rec.c_grid()
+        check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), len(self.engines), ptr(off)), None)
+        return off
+
+    def pstrirecy_range(self, rec: Recursion, control: PsTriRecyControl, j_begin: int, j_end: int, sigma, st,
+                        cst, X0=None):
+        """Lane-local points j_begin..j_end-1 of every lane (j_begin == 0 starts the lanes);
+        sigma/st are the full-length outputs, cst their C view (Engine.stats_struct)."""
+        x0 = None
+        if X0 is not None and j_begin == 0:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+            if x0.shape != (self.n, control.r):
+                raise DimensionMismatch(-2, f"X0 must be {(self.n, control.r)}, got {x0.shape}")
+        g = rec.c_grid()
+        cc = control.c_struct()
+        check(lib().rls_pstrirecy_schur_lanes_range(self._arr, len(self.engines), ptr(rec.Z), len(rec.Z), C.byref(g),
+                                                    C.byref(cc), ptr(x0), int(j_begin), int(j_end), ptr(sigma),
+                                                    C.byref(cst)), self.engines[0]._h)
+        for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
+            setattr(st, f, int(getattr(cst, f)))
+
+    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None):
+        nZ = len(rec.Z)
+        sigma = np.full(nZ, np.nan)
+        st = PsTriRecyStats.alloc(nZ)
+        cst = self.engines[0].stats_struct(st)
+        self.pstrirecy_range(rec, control, 0, nZ, sigma, st, cst, X0=X0)
+        st.mv_stats_available = True
+        return sigma, st
+
+    def close(self):
+        for e in self.engines:
+            e.close()
+
+
 _engines = {}
 
 
@@ -321,17 +401,18 @@ def _print_startup(io, rec, control):
 
 
 def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int = 1, io=None, X0=None,
-              device: int = 0):
+              device: int = 0, lanes: int = 1):
     """psTriRecy (psTriRecy.jl:889-913) → (σ_min in rec.Z order, PsTriRecyStats).
 
     ``X0`` (n × r) stands in for the reference's ``rand!(X)``; None draws a
-    deterministic uniform [0,1) complex block on the device.
+    deterministic uniform [0,1) complex block on the device.  ``lanes`` > 1 splits the
+    traversal on strip boundaries into concurrent lanes on the same GPU (class Lanes);
+    1 keeps the reference's single traversal.
     """
     control = control or PsTriRecyControl()
     io = io if io is not None else sys.stdout
     if verbose >= 1:
         _print_startup(io, rec, control)
-    eng = _engine(device)
     t0 = time.perf_counter_ns()
     if isinstance(C_, SchurFactor):
         T = C_.T
@@ -339,6 +420,15 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
     else:
         T = pre_process(C_)
         pre_ns = time.perf_counter_ns() - t0
+    if lanes > 1:
+        ls = Lanes(lanes, device, T)
+        try:
+            sigma, st = ls.pstrirecy(rec, control, X0=X0)
+        finally:
+            ls.close()
+        st.preprocess_time_ns = pre_ns
+        return sigma, st
+    eng = _engine(device)
     eng.set_schur(T)
     if verbose >= 1:
         eng.set_log(lambda line: (io.write(line + "\n"), io.write("-" * 100 + "\n")), verbose)

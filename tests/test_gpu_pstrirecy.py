@@ -126,3 +126,32 @@ def test_batched_recycle_matches_per_point(sprand_case):
         assert np.array_equal(stB.refine_it > 0, st1.refine_it > 0)
         assert np.array_equal(stB.p_count, st1.p_count)
         assert np.array_equal(stB.r_recy, st1.r_recy)
+
+
+def test_lanes_cover_grid_and_match_truth(sprand_case):
+    """Concurrent lanes: every point computed, σ within the bar of the dense SVD, the first
+    lane identical to the single traversal over its points, stats merged per point."""
+    C, T, normC, _ = sprand_case
+    grid = (0.45, 0.55, 0.0, 0.1, 12, 20, 2)          # strips of 24 points, 10 strips
+    rec = R.recursion_grid(*grid)
+    n, r = T.shape[0], 6
+    X0 = _x0(n, r)
+    ctl = R.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=20, r=r, recy_tau=1.6)
+    e = R.Engine(0)
+    e.set_schur(T)
+    sig1, st1 = e.pstrirecy(rec, ctl, X0=X0)
+    e.close()
+    ls = R.Lanes(3, 0, T)
+    off = ls.offsets(rec)
+    sigL, stL = ls.pstrirecy(rec, ctl, X0=X0)
+    ls.close()
+    assert np.all(np.isfinite(sigL))
+    assert np.max(np.abs(sigL - sig1)) <= 1e-4 * normC
+    sel = np.arange(0, len(rec.Z), 7)
+    truth = np.array([dense_sigma_min(T, z) for z in rec.Z[sel]])
+    assert np.max(np.abs(sigL[sel] - truth)) <= 1e-4 * normC
+    assert np.array_equal(sigL[:off[1]], sig1[:off[1]])
+    assert np.array_equal(stL.refine_it[:off[1]], st1.refine_it[:off[1]])
+    assert stL.n_pts == int(np.sum(stL.refine_it > 0))
+    for b in off[:-1]:
+        assert stL.refine_it[b] > 0 and stL.p_count[b] == 0   # each lane starts from an empty space

@@ -118,3 +118,21 @@ def test_outside_and_missing_points(built_lib):
     rec.Z[3] = complex(5.0, 0.0)
     with pytest.raises(R.ArgumentError):
         R.recursion_natural_permutation(rec)
+
+
+def test_lane_offsets_split_on_strip_boundaries():
+    """rls_lane_offsets (host only): lanes start on strips of n_x·k points, cover the grid."""
+    import ctypes as C
+    from rls_b200._lib import lib, ptr, check, DimensionMismatch
+    rec = R.recursion_grid(0.45, 0.55, 0.0, 0.1, 200, 200, 20)
+    g = rec.c_grid()
+    strip = 200 * 20
+    for lanes in (1, 3, 4, 8, 10):
+        off = np.zeros(lanes + 1, dtype=np.int64)
+        check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), lanes, ptr(off)), None)
+        assert off[0] == 0 and off[-1] == len(rec.Z)
+        assert np.all(np.diff(off) > 0)
+        assert np.all(off[:-1] % strip == 0)
+    off = np.zeros(12, dtype=np.int64)
+    with pytest.raises(DimensionMismatch):
+        check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), 11, ptr(off)), None)
