@@ -20,8 +20,8 @@ is larger than L2, so every step streams it from HBM.
           lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
           with one lane (the reference's single recycled space).
   e2e   : fresh lane contexts through the public C ABI with host buffers: upload
-          of the Schur factor from host memory to every lane plus steps 0..W+K-1
-          (grid points in, σ out), wall clock.
+          of the Schur factor from host memory (to lane 0, copied on the device to
+          the other lanes) plus steps 0..W+K-1 (grid points in, σ out), wall clock.
   --impl reference : the CPU restatement (oracle/, the reference's algorithm with
           LAPACK through SciPy on all host cores) on the same traversal, each step
           a bounded sample of --ref-chunk points.
@@ -358,9 +358,9 @@ def run_ours(args):
         nsteps = args.warmup + args.steps
         T_bytes = args.n * args.n * 16
         e2e = {"value": world * lanes * nsteps * s / el, "unit": "pts/s",
-               "h2d_bytes_per_step": int((lanes * T_bytes + lanes * nsteps * s * 16) / nsteps),
+               "h2d_bytes_per_step": int((T_bytes + lanes * nsteps * s * 16) / nsteps),
                "d2h_bytes_per_step": int(lanes * s * 8),
-               "span": f"upload of T to {lanes} lane contexts + steps 0..{nsteps - 1}"}
+               "span": f"upload of T (host to lane 0, device copies to the other {lanes - 1}) + steps 0..{nsteps - 1}"}
         e2e["matches_device_run"] = bool(np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12))
 
     out = base_line(args, world)

@@ -169,6 +169,11 @@ int rls_reorder_to_natural_grid(const rls_grid* g, const rls_c64* Z, int64_t nZ,
  * Host memory. */
 int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
 
+/* Installs on dst the operator already uploaded to src (same device), by a device-to-device
+ * copy of its tiles: lane contexts (rls_pstrirecy_schur_lanes) share one host upload.  No
+ * reference counterpart. */
+int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src);
+
 /* ---- solvers ------------------------------------------------------------------ */
 
 /* psTriRecy on the uploaded Schur factor (src/core/psTriRecy.jl:708-881,

@@ -1334,13 +1334,11 @@ extern "C" int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verb
   return RLS_OK;
 }
 
-// Tiles of T: host-side packing then one copy.
-extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt) {
-  if (!ctx) return RLS_ERR_ARG;
-  if (!T || n < 1 || ldt < n) {
-    set_err(ctx, "rls_set_schur: invalid arguments (n=%lld, ldt=%lld)", (long long)n, (long long)ldt);
-    return RLS_ERR_ARG;
-  }
+namespace {
+// Installs an operator of order n whose tiles (packed layout, n_pad = 64·ceil(n/64)) are at
+// `tiles` (host memory for kind H2D, another context's device array for D2D), and allocates
+// the per-operator workspaces.
+int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, cudaMemcpyKind kind) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   // drop an old operator and space
@@ -1356,25 +1354,11 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   ctx->nb = (int)((n + TILE - 1) / TILE);
   ctx->n_pad = (int64_t)ctx->nb * TILE;
   const int nb = ctx->nb;
-  const size_t ntiles = (size_t)nb * (nb + 1) / 2;
-  std::vector<cplx> h(ntiles * TILE * TILE);
-  for (int J = 0; J < nb; ++J)
-    for (int I = 0; I <= J; ++I) {
-      cplx* tp = h.data() + tile_index(I, J) * TILE * TILE;
-      for (int cc = 0; cc < TILE; ++cc) {
-        const int64_t gc = (int64_t)J * TILE + cc;
-        for (int rr = 0; rr < TILE; ++rr) {
-          const int64_t gr = (int64_t)I * TILE + rr;
-          cplx v = czero();
-          if (gr < n && gc < n && gr <= gc) v = cmk(T[gc * ldt + gr].re, T[gc * ldt + gr].im);
-          tp[cc * TILE + rr] = v;
-        }
-      }
-    }
-  RET(dalloc_t(ctx, &ctx->T, h.size()));
-  CK(cudaMemcpyAsync(ctx->T, h.data(), h.size() * sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t elems = (size_t)nb * (nb + 1) / 2 * TILE * TILE;
+  RET(dalloc_t(ctx, &ctx->T, elems));
+  CK(cudaMemcpyAsync(ctx->T, tiles, elems * sizeof(cplx), kind, ctx->stream));
   RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
-  RET(dalloc_t(ctx, &ctx->G, h.size()));
+  RET(dalloc_t(ctx, &ctx->G, elems));
   RET(dalloc_t(ctx, &ctx->trsm_u, (size_t)ctx->n_pad * 8));
   RET(dalloc_t(ctx, &ctx->flags, (size_t)2 * nb));
   RET(dalloc_t(ctx, &ctx->ticket, 1));
@@ -1400,11 +1384,56 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
     CK(cudaMemcpyAsync(ctx->trmm_us[adj], us.data(), us.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->trmm_Ofirst[adj], Of.data(), nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->trmm_Ocount[adj], Oc.data(), nb * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the host vectors must outlive the async copies
   }
   RET(dalloc_t(ctx, &ctx->trmm_part, maxunits * 16 * TILE));
   RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
-  CK(cudaStreamSynchronize(ctx->stream));  // h must outlive the async copy
+  CK(cudaStreamSynchronize(ctx->stream));  // the source tiles must outlive the async copy
   return RLS_OK;
+}
+}  // namespace
+
+// Tiles of T: host-side packing then one copy.
+extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!T || n < 1 || ldt < n) {
+    set_err(ctx, "rls_set_schur: invalid arguments (n=%lld, ldt=%lld)", (long long)n, (long long)ldt);
+    return RLS_ERR_ARG;
+  }
+  const int nb = (int)((n + TILE - 1) / TILE);
+  const size_t ntiles = (size_t)nb * (nb + 1) / 2;
+  std::vector<cplx> h(ntiles * TILE * TILE);
+  for (int J = 0; J < nb; ++J)
+    for (int I = 0; I <= J; ++I) {
+      cplx* tp = h.data() + tile_index(I, J) * TILE * TILE;
+      for (int cc = 0; cc < TILE; ++cc) {
+        const int64_t gc = (int64_t)J * TILE + cc;
+        for (int rr = 0; rr < TILE; ++rr) {
+          const int64_t gr = (int64_t)I * TILE + rr;
+          cplx v = czero();
+          if (gr < n && gc < n && gr <= gc) v = cmk(T[gc * ldt + gr].re, T[gc * ldt + gr].im);
+          tp[cc * TILE + rr] = v;
+        }
+      }
+    }
+  return operator_setup(ctx, n, h.data(), cudaMemcpyHostToDevice);
+}
+
+extern "C" int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src) {
+  if (!dst || !src) return RLS_ERR_ARG;
+  if (!src->T) {
+    set_err(dst, "rls_set_schur_copy: the source context has no operator");
+    return RLS_ERR_STATE;
+  }
+  if (src->device != dst->device) {
+    set_err(dst, "rls_set_schur_copy: contexts on devices %d and %d", src->device, dst->device);
+    return RLS_ERR_ARG;
+  }
+  if (src == dst) return RLS_OK;
+  rls_ctx* ctx = dst;   // error reports go to dst
+  CK(cudaSetDevice(src->device));
+  CK(cudaStreamSynchronize(src->stream));
+  return operator_setup(dst, src->n, src->T, cudaMemcpyDeviceToDevice);
 }
 
 extern "C" int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0, const rls_lobpcg_control* c,

@@ -319,8 +319,11 @@ class Lanes:
         return self.engines[0].n
 
     def set_schur(self, T):
-        for e in self.engines:
-            e.set_schur(T)
+        """One host upload to the first lane; the others copy its tiles on the device."""
+        self.engines[0].set_schur(T)
+        for e in self.engines[1:]:
+            check(lib().rls_set_schur_copy(e._h, self.engines[0]._h), e._h)
+            e.n = self.engines[0].n
 
     def set_batch(self, max_points: int):
         for e in self.engines:
