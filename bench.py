@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk", type=int, default=200, help="grid points per lane per step")
-    ap.add_argument("--lanes", type=int, default=8, help="concurrent grid lanes per GPU")
+    ap.add_argument("--lanes", type=int, default=10, help="concurrent grid lanes per GPU (at most one per strip)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
