@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-spmm", action="store_true", help="skip the sparse shifted product measurement")
     ap.add_argument("--plain-steps", type=int, default=1, help="steps timed on the unbatched per-point path")
     ap.add_argument("--ncu-window", default=None,
                     help="WARM,COUNT: run WARM points, then COUNT points inside cudaProfilerStart/Stop, and exit "
@@ -162,6 +163,53 @@ def max_over_ranks(x, world, device):
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def banded_sparse(n, per_row, half_width, seed):
+    """Synthetic real sparse matrix with the af23560 shape: `per_row` N(0,1) entries per row
+    inside a band of half-width `half_width`, plus a dominant diagonal (duplicates summed)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n, dtype=np.int64), per_row - 1)
+    cols = np.clip(rows + rng.integers(-half_width, half_width + 1, size=rows.size), 0, n - 1)
+    vals = rng.standard_normal(rows.size)
+    d = np.arange(n, dtype=np.int64)
+    A = sp.csc_matrix((np.concatenate([vals, np.full(n, 4.0 * per_row)]),
+                       (np.concatenate([rows, d]), np.concatenate([cols, d]))), shape=(n, n))
+    A.sum_duplicates()
+    return A
+
+
+def spmm_measure(local, hbm_peak, reps=20, b=6):
+    """Shifted sparse product (ShiftedMat mul!) on two synthetic matrices, device-resident
+    operands, CUDA-event timing per launch (the engine's profile slot 5)."""
+    import torch
+    from rls_b200.solvers import Engine
+    out = {}
+    for name, n, per_row in (("af23560-shaped n=23560, ~20 nnz/row, band ±300", 23560, 20),
+                             ("banded n=1,000,000, ~16 nnz/row, band ±300", 1_000_000, 16)):
+        A = banded_sparse(n, per_row, 300, 20260318)
+        e = Engine(local)
+        e.sparse_upload(A)
+        X = torch.randn((b, n), dtype=torch.complex128, device="cuda")
+        Y = torch.empty((b, n), dtype=torch.complex128, device="cuda")
+        from rls_b200._lib import lib, c64
+        import ctypes as C
+        fn = lib().rls_spmm_shifted_dev
+        for _ in range(3):
+            fn(e._h, c64(-0.2, 0.1), 0, b, C.c_void_p(X.data_ptr()), n, C.c_void_p(Y.data_ptr()), n)
+        torch.cuda.synchronize()
+        e.set_profile(True)
+        for _ in range(reps):
+            for adj in (0, 1):
+                fn(e._h, c64(-0.2, 0.1), adj, b, C.c_void_p(X.data_ptr()), n, C.c_void_p(Y.data_ptr()), n)
+        cnt, ms, work = e.profile(5)
+        e.close()
+        achieved = (work / cnt) / (ms / cnt / 1e3) / 1e9
+        out[name] = {"nnz": int(A.nnz), "b": b, "launches": cnt, "avg_us": ms / cnt * 1e3,
+                     "bytes_per_launch": work / cnt, "achieved_gbs": achieved, "frac": achieved / hbm_peak}
+        del X, Y
+    return out
 
 
 def cpu_baseline(T, rec, ctl, X0, budget_s, min_pts=2):
@@ -405,6 +453,8 @@ def run_ours(args):
     if prof[1][0]:
         c1, t1, f1 = prof[1]
         out["heev_fp64"] = {"gflops": f1 / (t1 / 1e3) / 1e9, "launches": c1, "avg_us": t1 / c1 * 1e3}
+    if rank == 0 and world == 1 and not args.no_spmm:
+        out["spmm_shifted"] = spmm_measure(local, hbm_peak)
     if rank == 0 and world == 1:
         from oracle.pstrirecy import PsTriRecyControl as OC
         from oracle import recugrid as G

@@ -136,8 +136,9 @@ int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always);
  * set_profile resets the counters; profile_get returns launches, total device
  * milliseconds and algorithmic work (bytes; flops for kernel 1).  kernel 4
  * returns the host's blocking waits on the stream instead: their number and
- * total wall milliseconds (work = 0).  No reference counterpart (the reference
- * times phases with time_ns, psTriRecy.jl:306-309). */
+ * total wall milliseconds (work = 0); kernel 5 is the sparse shifted product
+ * (rls_spmm_shifted*).  No reference counterpart (the reference times phases
+ * with time_ns, psTriRecy.jl:306-309). */
 int rls_ctx_set_profile(rls_ctx* ctx, int on);
 int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work);
 
@@ -227,6 +228,25 @@ int rls_pstrirecy_schur_lanes_range(rls_ctx* const* ctxs, int nlanes, const rls_
 int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
                           const rls_lobpcg_control* control, rls_c64* X_out,
                           double* sigma_r, double* sigma, int64_t* it);
+
+/* ---- sparse shifted product ------------------------------------------------------ */
+
+/* Uploads a sparse m × n C in the layout of Julia's SparseMatrixCSC (colptr n+1, rowval and
+ * nzval nnz; indices 1-based with base = 1, 0-based with base = 0).  The device keeps the
+ * CSR of C and of Cᴴ.  Host memory.  Replaces the operand of `ShiftedMat`
+ * (src/types/RLSMatrices.jl:24-64). */
+int rls_sparse_upload_csc(rls_ctx* ctx, int64_t m, int64_t n, const int64_t* colptr,
+                          const int64_t* rowval, const rls_c64* nzval, int base);
+/* mul!(Y, ShiftedMat(C, s), X) (RLSMatrices.jl:47-56): Y = C X + s·X[1:min(m,n), :]
+ * (adj = 0; X n × b, Y m × b) or, for adjoint(ShiftedMat) (:64-66),
+ * Y = Cᴴ X + conj(s)·X[1:min(m,n), :] (adj = 1; X m × b, Y n × b).  Column-major
+ * with leading dimensions ldx, ldy.  rls_spmm_shifted takes host buffers and returns
+ * when Y is written; rls_spmm_shifted_dev takes device pointers and only enqueues the
+ * product on the context's stream (rls_ctx_stream). */
+int rls_spmm_shifted(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, int64_t ldx,
+                     rls_c64* Y, int64_t ldy);
+int rls_spmm_shifted_dev(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, int64_t ldx,
+                         rls_c64* Y, int64_t ldy);
 
 /* ---- gradient -------------------------------------------------------------------- */
 

@@ -7,13 +7,13 @@ no CPU fallback.
 from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_grid_linear,
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
-from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, SchurFactor, pre_process,
-                      psTriRecy)
+from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SchurFactor,
+                      pre_process, psTriRecy)
 from ._lib import RLSError, ArgumentError, DimensionMismatch
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
-    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "SchurFactor", "pre_process", "psTriRecy", "RLSError",
+    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SchurFactor", "pre_process", "psTriRecy", "RLSError",
     "ArgumentError", "DimensionMismatch",
 ]

@@ -72,6 +72,9 @@ SIGNATURES = {
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_tsqr_r_noalloc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int, P, P]),
     "rls_sigma_grad": (C.c_int, [P, c64, P, C.c_int, P, P, P, P, P]),
+    "rls_sparse_upload_csc": (C.c_int, [P, C.c_int64, C.c_int64, P, P, P, C.c_int]),
+    "rls_spmm_shifted": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),
+    "rls_spmm_shifted_dev": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),
     "rls_lane_offsets": (C.c_int, [C.POINTER(rls_grid), C.c_int64, C.c_int, P]),
     "rls_pstrirecy_schur_lanes": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
                                             C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),

@@ -22,6 +22,7 @@
 #include "heev.cuh"
 #include "rotate.cuh"
 #include "small.cuh"
+#include "sparse.cuh"
 
 namespace {
 
@@ -140,9 +141,12 @@ struct rls_ctx {
     double ms = 0.0;
     double bytes = 0.0;
     std::vector<double> pending_bytes;
-  } kprof[4];
+  } kprof[6];                      // 0..3 kernels below, 4 unused (host waits), 5 sparse products
 
   rls_pstrirecy_stats lane_stats{};   // this context's run as one lane of rls_pstrirecy_schur_lanes_range
+  CsrDev sp[2];                        // uploaded sparse C: [0] CSR of C, [1] CSR of Cᴴ
+  cplx* sp_xr = nullptr;               // row-major copy of up to 8 columns of X
+  size_t sp_xr_elems = 0;
 
   std::vector<DevBuf> owned;
 };
@@ -210,7 +214,7 @@ int check_launch(rls_ctx* ctx, const char* what) {
   return RLS_OK;
 }
 
-enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3 };
+enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3, KP_SPMM = 5 };
 
 void prof_begin(rls_ctx* ctx, int id, cudaEvent_t* e0) {
   if (!ctx->profile) return;
@@ -1779,6 +1783,188 @@ extern "C" int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, c
   return rls_pstrirecy_schur_range(ctx, Z, nZ, g, ctl, X0, 0, nZ, sigma_min, st);
 }
 
+extern "C" int rls_sparse_upload_csc(rls_ctx* ctx, int64_t m, int64_t n, const int64_t* colptr,
+                                     const int64_t* rowval, const rls_c64* nzval, int base) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (m < 1 || n < 1 || !colptr || (base != 0 && base != 1) || m >= (1ll << 31) || n >= (1ll << 31)) {
+    set_err(ctx, "rls_sparse_upload_csc: invalid arguments (m=%lld, n=%lld, base=%d)", (long long)m, (long long)n,
+            base);
+    return RLS_ERR_ARG;
+  }
+  const int64_t nnz = colptr[n] - base;
+  if (nnz < 0 || colptr[0] != base || (nnz > 0 && (!rowval || !nzval))) {
+    set_err(ctx, "rls_sparse_upload_csc: inconsistent column pointers");
+    return RLS_ERR_DIM;
+  }
+  for (int64_t c = 0; c < n; ++c)
+    if (colptr[c + 1] < colptr[c]) {
+      set_err(ctx, "rls_sparse_upload_csc: column pointers decrease at column %lld", (long long)(c + 1));
+      return RLS_ERR_DIM;
+    }
+  for (int64_t j = 0; j < nnz; ++j)
+    if (rowval[j] - base < 0 || rowval[j] - base >= m) {
+      set_err(ctx, "rls_sparse_upload_csc: row index %lld out of range 1..%lld", (long long)(rowval[j] - base + 1),
+              (long long)m);
+      return RLS_ERR_DIM;
+    }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (auto& a : ctx->sp) {
+    dfree(ctx, a.rowptr);
+    dfree(ctx, a.col);
+    dfree(ctx, a.val);
+    a = CsrDev{};
+  }
+  // [0]: CSR of C (m rows) by counting sort of the CSC entries; [1]: CSR of Cᴴ (n rows) is
+  // the CSC itself with conjugated values.
+  std::vector<int64_t> rp0((size_t)m + 1, 0), rp1((size_t)n + 1, 0);
+  std::vector<int32_t> c0((size_t)nnz), c1((size_t)nnz);
+  std::vector<cplx> v0((size_t)nnz), v1((size_t)nnz);
+  for (int64_t j = 0; j < nnz; ++j) ++rp0[(size_t)(rowval[j] - base) + 1];
+  for (int64_t i = 0; i < m; ++i) rp0[(size_t)i + 1] += rp0[(size_t)i];
+  std::vector<int64_t> next(rp0.begin(), rp0.end() - 1);
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t j = colptr[c] - base; j < colptr[c + 1] - base; ++j) {
+      const int64_t r = rowval[j] - base;
+      const int64_t q = next[(size_t)r]++;
+      c0[(size_t)q] = (int32_t)c;
+      v0[(size_t)q] = cmk(nzval[j].re, nzval[j].im);
+      c1[(size_t)j] = (int32_t)r;
+      v1[(size_t)j] = cmk(nzval[j].re, -nzval[j].im);
+    }
+  for (int64_t c = 0; c <= n; ++c) rp1[(size_t)c] = colptr[c] - base;
+  const int64_t rows[2] = {m, n}, cols[2] = {n, m};
+  std::vector<int64_t>* rps[2] = {&rp0, &rp1};
+  std::vector<int32_t>* cs[2] = {&c0, &c1};
+  std::vector<cplx>* vs[2] = {&v0, &v1};
+  for (int t = 0; t < 2; ++t) {
+    CsrDev& a = ctx->sp[t];
+    a.rows = rows[t];
+    a.cols = cols[t];
+    a.nnz = nnz;
+    const double mean = (double)nnz / (double)rows[t];
+    int g = 1;
+    while (g < 4 && g < mean) g <<= 1;
+    a.group = g;
+    RET(dalloc_t(ctx, &a.rowptr, (size_t)rows[t] + 1));
+    RET(dalloc_t(ctx, &a.col, (size_t)std::max<int64_t>(nnz, 1)));
+    RET(dalloc_t(ctx, &a.val, (size_t)std::max<int64_t>(nnz, 1)));
+    CK(cudaMemcpyAsync(a.rowptr, rps[t]->data(), sizeof(int64_t) * (rows[t] + 1), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    if (nnz > 0) {
+      CK(cudaMemcpyAsync(a.col, cs[t]->data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(a.val, vs[t]->data(), sizeof(cplx) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));   // the host arrays must outlive the copies
+  return RLS_OK;
+}
+
+namespace {
+int spmm_dev(rls_ctx* ctx, cplx s, int adj, int b, const cplx* X, int64_t ldx, cplx* Y, int64_t ldy) {
+  const CsrDev& A = ctx->sp[adj ? 1 : 0];
+  if (!A.rowptr) {
+    set_err(ctx, "no sparse matrix uploaded (call rls_sparse_upload_csc first)");
+    return RLS_ERR_STATE;
+  }
+  if (b < 1 || !X || !Y || ldx < A.cols || ldy < A.rows) {
+    set_err(ctx, "rls_spmm_shifted: invalid block (b=%d, ldx=%lld, ldy=%lld)", b, (long long)ldx, (long long)ldy);
+    return RLS_ERR_DIM;
+  }
+  const cplx sh = adj ? cconj(s) : s;
+  const int64_t nshift = std::min(A.rows, A.cols);
+  const int64_t threads = A.rows * A.group;
+  const unsigned grid = (unsigned)((threads + 255) / 256);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ctx->profile) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, ctx->stream));
+  }
+  const size_t need = (size_t)A.cols * 8;
+  if (ctx->sp_xr_elems < need) {
+    dfree(ctx, ctx->sp_xr);
+    ctx->sp_xr = nullptr;
+    ctx->sp_xr_elems = 0;
+    RET(dalloc_t(ctx, &ctx->sp_xr, need));
+    ctx->sp_xr_elems = need;
+  }
+  const unsigned gx = (unsigned)((A.cols + 255) / 256);
+  for (int c0 = 0; c0 < b; c0 += 8) {
+    const int bb = std::min(8, b - c0);
+    const cplx* Xc = X + (int64_t)c0 * ldx;
+    cplx* Yc = Y + (int64_t)c0 * ldy;
+#define RLS_SPMM_CASE(BB)                                                                             \
+  case BB:                                                                                            \
+    k_rows_major<BB><<<gx, 256, 0, ctx->stream>>>(A.cols, Xc, ldx, ctx->sp_xr);                       \
+    k_spmm_shifted<BB><<<grid, 256, 0, ctx->stream>>>(A, sh, nshift, ctx->sp_xr, Xc, ldx, Yc, ldy); \
+    break;
+    switch (bb) {
+      RLS_SPMM_CASE(1) RLS_SPMM_CASE(2) RLS_SPMM_CASE(3) RLS_SPMM_CASE(4)
+      RLS_SPMM_CASE(5) RLS_SPMM_CASE(6) RLS_SPMM_CASE(7) RLS_SPMM_CASE(8)
+    }
+#undef RLS_SPMM_CASE
+    RET(check_launch(ctx, "k_spmm_shifted"));
+  }
+  if (ctx->profile) {
+    CK(cudaEventRecord(e1, ctx->stream));
+    auto& k = ctx->kprof[KP_SPMM];
+    k.ev.push_back(e0);
+    k.ev.push_back(e1);
+    // algorithmic bytes: values and column indices once per 8-column chunk, row pointers, X and Y once
+    const double chunks = (double)((b + 7) / 8);
+    k.pending_bytes.push_back(chunks * (double)A.nnz * (sizeof(cplx) + sizeof(int32_t)) +
+                              (double)(A.rows + 1) * sizeof(int64_t) +
+                              (double)b * (double)(A.cols + A.rows) * sizeof(cplx));
+  }
+  return RLS_OK;
+}
+}  // namespace
+
+extern "C" int rls_spmm_shifted_dev(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, int64_t ldx,
+                                    rls_c64* Y, int64_t ldy) {
+  if (!ctx) return RLS_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  return spmm_dev(ctx, cmk(s.re, s.im), adj, b, reinterpret_cast<const cplx*>(X), ldx, reinterpret_cast<cplx*>(Y),
+                  ldy);
+}
+
+extern "C" int rls_spmm_shifted(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, int64_t ldx, rls_c64* Y,
+                                int64_t ldy) {
+  if (!ctx) return RLS_ERR_ARG;
+  const CsrDev& A = ctx->sp[adj ? 1 : 0];
+  if (!A.rowptr) {
+    set_err(ctx, "no sparse matrix uploaded (call rls_sparse_upload_csc first)");
+    return RLS_ERR_STATE;
+  }
+  if (b < 1 || !X || !Y || ldx < A.cols || ldy < A.rows) {
+    set_err(ctx, "rls_spmm_shifted: invalid block (b=%d, ldx=%lld, ldy=%lld)", b, (long long)ldx, (long long)ldy);
+    return RLS_ERR_DIM;
+  }
+  CK(cudaSetDevice(ctx->device));
+  cplx *dX = nullptr, *dY = nullptr;
+  if (cudaMalloc(&dX, sizeof(cplx) * A.cols * b) != cudaSuccess ||
+      cudaMalloc(&dY, sizeof(cplx) * A.rows * b) != cudaSuccess) {
+    cudaFree(dX);
+    set_err(ctx, "rls_spmm_shifted: device allocation failed");
+    return RLS_ERR_NOMEM;
+  }
+  int st = RLS_OK;
+  if (cudaMemcpy2DAsync(dX, A.cols * sizeof(cplx), X, ldx * sizeof(cplx), A.cols * sizeof(cplx), b,
+                        cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+    st = RLS_ERR_CUDA;
+  if (st == RLS_OK) st = spmm_dev(ctx, cmk(s.re, s.im), adj, b, dX, A.cols, dY, A.rows);
+  if (st == RLS_OK && cudaMemcpy2DAsync(Y, ldy * sizeof(cplx), dY, A.rows * sizeof(cplx), A.rows * sizeof(cplx), b,
+                                        cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+    st = RLS_ERR_CUDA;
+  if (st == RLS_OK) st = sync_and_check(ctx);
+  else cudaStreamSynchronize(ctx->stream);
+  cudaFree(dX);
+  cudaFree(dY);
+  if (st == RLS_ERR_CUDA) set_err(ctx, "rls_spmm_shifted: copy failed");
+  return st;
+}
+
 extern "C" int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets) {
   if (!g || nZ < 0 || nlanes < 1 || !offsets) return RLS_ERR_ARG;
   const int64_t strip = std::max<int64_t>(1, g->n_x * std::max<int64_t>(g->k, 1));
@@ -1892,7 +2078,7 @@ extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
 }
 
 extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work) {
-  if (!ctx || kernel < 0 || kernel > 4) return RLS_ERR_ARG;
+  if (!ctx || kernel < 0 || kernel > 5) return RLS_ERR_ARG;
   RET(sync_and_check(ctx));
   prof_resolve(ctx);
   if (kernel == 4) {

@@ -270,6 +270,33 @@ class Engine:
                                           C.byref(s), C.byref(it)), self._h)
         return s.value, it.value, X, sr
 
+    def sparse_upload(self, C):
+        """Uploads a sparse C (SciPy sparse, any format) for spmm_shifted / ShiftedMat."""
+        import scipy.sparse as sp
+        A = sp.csc_matrix(C, dtype=np.complex128)
+        A.sort_indices()
+        m, n = A.shape
+        colptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        rowval = np.ascontiguousarray(A.indices, dtype=np.int64)
+        nzval = np.ascontiguousarray(A.data, dtype=np.complex128)
+        check(lib().rls_sparse_upload_csc(self._h, m, n, ptr(colptr), ptr(rowval), ptr(nzval), 0), self._h)
+        self.sparse_shape = (m, n)
+
+    def spmm_shifted(self, s: complex, X, adj: bool = False):
+        """mul!(Y, ShiftedMat(C, s), X) (RLSMatrices.jl:47-56), or its adjoint: host arrays."""
+        m, n = self.sparse_shape
+        X = np.asfortranarray(np.asarray(X, dtype=np.complex128))
+        vec = X.ndim == 1
+        if vec:
+            X = X.reshape(-1, 1, order="F")
+        rows_in, rows_out = (m, n) if adj else (n, m)
+        if X.shape[0] != rows_in:
+            raise DimensionMismatch(-2, f"X has {X.shape[0]} rows, expected {rows_in}")
+        Y = np.zeros((rows_out, X.shape[1]), dtype=np.complex128, order="F")
+        check(lib().rls_spmm_shifted(self._h, c64(s.real, s.imag), int(adj), X.shape[1], ptr(X), X.shape[0], ptr(Y),
+                                     rows_out), self._h)
+        return Y[:, 0] if vec else Y
+
     def sigma_grad(self, z: complex, v0, refine_steps: int = 2, Q=None, pattern=None):
         """σ_min(C − zI) and its gradient at z (no reference counterpart).
 
@@ -298,6 +325,28 @@ class Engine:
             else:
                 out["dsdC"] = np.real(np.outer(np.conj(uC), vC))
         return out
+
+
+class ShiftedMat:
+    """ShiftedMat (src/types/RLSMatrices.jl:24-64) on the device: C − zI with C sparse,
+    applied as ``A @ X`` (mul!) and ``A.adjoint() @ X``.  The matrix is uploaded once to
+    the given Engine."""
+
+    def __init__(self, C, s: complex, engine: "Engine" = None, adj: bool = False, _uploaded: bool = False):
+        self.engine = engine or Engine(0)
+        self.s = complex(s)
+        self.adj = adj
+        if not _uploaded:
+            self.engine.sparse_upload(C)
+        m, n = self.engine.sparse_shape
+        self.shape = (n, m) if adj else (m, n)
+
+    def __matmul__(self, X):
+        return self.engine.spmm_shifted(self.s if not self.adj else np.conj(self.s), X, adj=self.adj)
+
+    def adjoint(self) -> "ShiftedMat":
+        """adjoint(ShiftedMat) = ShiftedMat(Cᴴ, conj(s)) (RLSMatrices.jl:64-66)."""
+        return ShiftedMat(None, np.conj(self.s), self.engine, adj=not self.adj, _uploaded=True)
 
 
 class Lanes:
