@@ -36,6 +36,9 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+# one hardware work queue per lane stream (read by the CUDA runtime at initialisation)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import statistics
 import subprocess
 import sys

@@ -4,6 +4,14 @@ Public names mirror the reference (src/core/recuGrid.jl, src/core/psTriRecy.jl,
 src/core/lobpcgSvd.jl).  All per-grid-point work runs in librls_b200.so; there is
 no CPU fallback.
 """
+import os as _os
+
+# Concurrent lanes (rls_b200.Lanes) run one CUDA stream each; with the default 8 hardware
+# work queues more than 8 streams share queues and serialise.  The CUDA runtime reads this
+# when it initialises in this process, so it is set before any CUDA call (a value the
+# caller set is kept).
+_os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_grid_linear,
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
