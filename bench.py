@@ -14,7 +14,8 @@ the reference's loop carries it; W warm-up steps, then K timed steps.  The Schur
 is larger than L2, so every step streams it from HBM.
 
   value : points / device time of the K timed steps, Schur factor resident in HBM.
-          The traversal is split on strip boundaries into --lanes concurrent lanes
+          The traversal is split on column boundaries (k points) into --lanes
+          near-equal concurrent lanes
           (rls_b200.Lanes: one context, stream and host thread per lane); a step is
           --chunk lane-local points in every lane; device time is the max over the
           lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
@@ -26,8 +27,9 @@ is larger than L2, so every step streams it from HBM.
           LAPACK through SciPy on all host cores) on the same traversal, each step
           a bounded sample of --ref-chunk points.
 
-Multi-GPU (torchrun): every rank takes a contiguous share of the grid's strips and
-splits it into lanes (independent recycled spaces, weak scaling); the only
+Multi-GPU (torchrun): every rank takes a contiguous, column-aligned share of the grid
+and splits it into --lanes lanes (independent recycled spaces; lanes per GPU fixed, the
+step shrinks to fit where a rank's share of the grid is small); the only
 collectives are the broadcast of T before timing and the max over ranks of the
 timings.
 """
@@ -63,8 +65,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--chunk", type=int, default=200, help="grid points per lane per step")
-    ap.add_argument("--lanes", type=int, default=10, help="concurrent grid lanes per GPU (at most one per strip)")
+    ap.add_argument("--chunk", type=int, default=200,
+                    help="grid points per lane per step (at most; lowered to fit the lane's share of the grid)")
+    ap.add_argument("--lanes", type=int, default=10, help="concurrent grid lanes per GPU")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
@@ -147,14 +150,24 @@ class ClockSampler:
                 "power_w_max": max((num(r[3]) or 0.0) for r in self.rows)}
 
 
-def strip_offset(rank, world, nZ, strip):
-    """First traversal index of this rank's share: the grid's nZ // strip serpentine strips
-    (strip = n_x · k points each) are split into `world` contiguous runs, and rank i starts
-    its own traversal, with its own recycled space, at the first strip of run i."""
-    nstrips = nZ // strip
-    if world > nstrips:
-        raise SystemExit(f"{world} ranks for {nstrips} strips of the grid")
-    return (rank * nstrips // world) * strip
+def column_offset(rank, world, nZ, col):
+    """First traversal index of this rank's share: the traversal's columns (col = k points
+    each, one grid column of a serpentine strip) are split into `world` near-equal contiguous
+    runs, and rank i starts its own traversal, with its own recycled space, at run i."""
+    ncols = -(-nZ // col)
+    if world > ncols:
+        raise SystemExit(f"{world} ranks for {ncols} columns of the traversal")
+    return min(nZ, (rank * ncols // world) * col)
+
+
+def lane_plan(nZ, world, lanes, chunk, nsteps, col):
+    """(lanes per rank, points per lane per step) for `world` ranks sharing an nZ-point
+    traversal: every rank runs the same number of lanes and the same step, sized so that
+    the smallest lane (column-aligned split, shares within two columns of nZ / world / lanes)
+    holds `nsteps` steps."""
+    share = nZ // world
+    lanes = max(1, min(lanes, share // max(col, nsteps)))
+    return lanes, max(1, min(chunk, (share // lanes - 2 * col) // nsteps))
 
 
 def max_over_ranks(x, world, device):
@@ -302,17 +315,17 @@ def run_ours(args):
         del buf
 
     rec = R.recursion_grid(*GRID)
-    strip = GRID[4] * GRID[6]
-    off = strip_offset(rank, world, len(rec.Z), strip)
-    end = strip_offset(rank + 1, world, len(rec.Z), strip) if rank + 1 < world else len(rec.Z)
+    col = GRID[6]
+    off = column_offset(rank, world, len(rec.Z), col)
+    end = column_offset(rank + 1, world, len(rec.Z), col) if rank + 1 < world else len(rec.Z)
     sub = R.Recursion(*GRID)
     sub.Z = np.ascontiguousarray(rec.Z[off:end])
-    lanes = max(1, min(args.lanes, len(sub.Z) // strip))
+    nst = args.warmup + args.steps
+    lanes, s = lane_plan(len(rec.Z), world, args.lanes, args.chunk, nst, col)
     ctl = PsTriRecyControl(normC=NORMC, tol=1e-4, p_min=1, p=60, recy_tau=1.6)
     rng = np.random.default_rng(1 + rank)
     X0 = rng.random((args.n, 6)) + 1j * rng.random((args.n, 6))
-    s = args.chunk
-    need = (args.warmup + args.steps) * s
+    need = nst * s
 
     # plain per-point drop-in (no speculative batching, one lane) on one step, for comparison
     plain = None
@@ -419,8 +432,9 @@ def run_ours(args):
     out.update({"value": value, "ms_per_step": ms_max / args.steps})
     out["config"]["points_per_step"] = lanes * s
     out["config"]["lanes"] = lanes
-    out["config"]["parallelism"] = (f"grid strips: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
-                                    "(independent traversals from strip starts)")
+    out["config"]["chunk"] = s
+    out["config"]["parallelism"] = (f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
+                                    "(independent traversals from column starts)")
     out["config"]["refine_fraction_timed"] = refines / (lanes * args.steps * s)
     out["preprocess_s"] = pre_s
     out["gpu_launches"] = main["launches"]

@@ -201,8 +201,9 @@ int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const 
 
 /* Concurrent grid lanes on one GPU.  No reference counterpart: the reference walks the
  * whole traversal with one recycled space.  The traversal Z (nZ points) is split into
- * nlanes contiguous ranges that start on strip boundaries of the recursion grid (n_x·k
- * points per strip; rls_lane_offsets gives the split), and lane l runs psTriRecy on its
+ * nlanes contiguous, near-equal ranges that start on column boundaries of the zigzag
+ * traversal (k points, one grid column of a strip; rls_lane_offsets gives the split), and
+ * lane l runs psTriRecy on its
  * range from an empty recycled space on context ctxs[l] (its own stream, operator
  * uploaded with rls_set_schur), each lane in its own host thread.  Each lane is exactly
  * the reference's run on that sub-grid; lanes keep the GPU busy where one traversal's

@@ -1967,14 +1967,16 @@ extern "C" int rls_spmm_shifted(rls_ctx* ctx, rls_c64 s, int adj, int b, const r
 
 extern "C" int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets) {
   if (!g || nZ < 0 || nlanes < 1 || !offsets) return RLS_ERR_ARG;
-  const int64_t strip = std::max<int64_t>(1, g->n_x * std::max<int64_t>(g->k, 1));
-  const int64_t nstrips = std::max<int64_t>(1, (nZ + strip - 1) / strip);
-  if (nlanes > nstrips) {
-    g_create_err = "rls_lane_offsets: " + std::to_string(nlanes) + " lanes for " + std::to_string(nstrips) +
-                   " strips of the grid";
+  // lanes start on column boundaries of the zigzag traversal (k points: one grid column of
+  // a strip), as evenly as those allow
+  const int64_t col = std::max<int64_t>(1, g->k);
+  const int64_t ncols = std::max<int64_t>(1, (nZ + col - 1) / col);
+  if (nlanes > ncols) {
+    g_create_err = "rls_lane_offsets: " + std::to_string(nlanes) + " lanes for " + std::to_string(ncols) +
+                   " columns of the traversal";
     return RLS_ERR_DIM;
   }
-  for (int l = 0; l < nlanes; ++l) offsets[l] = std::min<int64_t>(nZ, ((int64_t)l * nstrips / nlanes) * strip);
+  for (int l = 0; l < nlanes; ++l) offsets[l] = std::min<int64_t>(nZ, ((int64_t)l * ncols / nlanes) * col);
   offsets[nlanes] = nZ;
   return RLS_OK;
 }

@@ -351,8 +351,8 @@ class ShiftedMat:
 
 class Lanes:
     """Concurrent grid lanes on one GPU (rls_pstrirecy_schur_lanes_range): one Engine per
-    lane, each with the Schur factor uploaded; the traversal is split on strip boundaries
-    of the recursion grid and every lane runs psTriRecy from an empty recycled space on
+    lane, each with the Schur factor uploaded; the traversal is split into near-equal parts
+    starting on column boundaries (k points) of the zigzag traversal and every lane runs psTriRecy from an empty recycled space on
     its part, in its own host thread inside the library.  No reference counterpart."""
 
     def __init__(self, lanes: int, device: int = 0, T=None):
@@ -458,7 +458,7 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
 
     ``X0`` (n × r) stands in for the reference's ``rand!(X)``; None draws a
     deterministic uniform [0,1) complex block on the device.  ``lanes`` > 1 splits the
-    traversal on strip boundaries into concurrent lanes on the same GPU (class Lanes);
+    traversal on column boundaries into concurrent lanes on the same GPU (class Lanes);
     1 keeps the reference's single traversal.
     """
     control = control or PsTriRecyControl()

@@ -120,19 +120,26 @@ def test_outside_and_missing_points(built_lib):
         R.recursion_natural_permutation(rec)
 
 
-def test_lane_offsets_split_on_strip_boundaries():
-    """rls_lane_offsets (host only): lanes start on strips of n_x·k points, cover the grid."""
+def test_lane_offsets_split_on_column_boundaries():
+    """rls_lane_offsets (host only): near-equal lanes starting on k-point columns of the
+    zigzag traversal, covering the grid."""
     import ctypes as C
     from rls_b200._lib import lib, ptr, check, DimensionMismatch
     rec = R.recursion_grid(0.45, 0.55, 0.0, 0.1, 200, 200, 20)
     g = rec.c_grid()
-    strip = 200 * 20
-    for lanes in (1, 3, 4, 8, 10):
+    k = 20
+    for lanes in (1, 3, 4, 8, 10, 25, 2000):
         off = np.zeros(lanes + 1, dtype=np.int64)
         check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), lanes, ptr(off)), None)
         assert off[0] == 0 and off[-1] == len(rec.Z)
         assert np.all(np.diff(off) > 0)
-        assert np.all(off[:-1] % strip == 0)
-    off = np.zeros(12, dtype=np.int64)
+        assert np.all(off[:-1] % k == 0)
+        assert np.diff(off).max() - np.diff(off).min() <= k
+    # the first point of every lane starts a column of the traversal: same x as the next k-1 points
+    off = np.zeros(9, dtype=np.int64)
+    check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), 8, ptr(off)), None)
+    for o in off[:-1]:
+        assert np.allclose(rec.Z[o:o + k].real, rec.Z[o].real)
+    off = np.zeros(2002, dtype=np.int64)
     with pytest.raises(DimensionMismatch):
-        check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), 11, ptr(off)), None)
+        check(lib().rls_lane_offsets(C.byref(g), len(rec.Z), 2001, ptr(off)), None)

@@ -1,6 +1,6 @@
 """Host logic of the multi-rank benchmark, on CPU with two `gloo` ranks.
 
-Each rank runs its own traversal of the grid from the first strip of its share, with no
+Each rank runs its own traversal of the grid from the first column of its share, with no
 collective on the data path; the only exchange is the max over ranks of the timings.
 """
 import json
@@ -27,8 +27,7 @@ def _rank_main(rank, world, port, out_dir):
                             timeout=timedelta(seconds=60))
     try:
         rec = recursion_grid(*bench.GRID)
-        strip = bench.GRID[4] * bench.GRID[6]
-        off = bench.strip_offset(rank, world, len(rec.Z), strip)
+        off = bench.column_offset(rank, world, len(rec.Z), bench.GRID[6])
         t = bench.max_over_ranks(10.0 * (rank + 1), world, "cpu")
         first = rec.Z[off]
         with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
@@ -38,27 +37,43 @@ def _rank_main(rank, world, port, out_dir):
 
 
 @pytest.mark.parametrize("world", [2])
-def test_strip_shares_and_max_over_ranks(tmp_path, world):
+def test_column_shares_and_max_over_ranks(tmp_path, world):
     import torch.multiprocessing as mp
     mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
     res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
-    strip = bench.GRID[4] * bench.GRID[6]
+    x_st, x_ed, y_st, y_ed, n_x, n_y, k = bench.GRID
     offs = [r["off"] for r in res]
     assert offs[0] == 0
-    assert all(o % strip == 0 for o in offs)
+    assert all(o % k == 0 for o in offs)
     assert offs == sorted(set(offs))                      # distinct, increasing shares
     assert all(r["t"] == 10.0 * world for r in res)       # every rank sees the slowest rank's time
-    # every rank starts at the corner of its first strip: an x edge of the grid, on the
-    # strip's first row of y
-    x_st, x_ed, y_st, y_ed, n_x, n_y, k = bench.GRID
+    # every rank starts at the first row of y of a grid column in one of the serpentine strips
     dy = (y_ed - y_st) / (n_y - 1)
     for r in res:
-        s = r["off"] // strip
-        assert np.isclose(r["first"][0], x_st if s % 2 == 0 else x_ed)
-        assert np.isclose(r["first"][1], y_st + s * k * dy)
+        strip = r["off"] // (n_x * k)
+        assert np.isclose(r["first"][1], y_st + strip * k * dy)
 
 
-def test_strip_offset_rejects_more_ranks_than_strips():
+@pytest.mark.parametrize("world", [1, 2, 4, 8])
+def test_column_shares_fit_ten_lanes_per_rank(world):
+    """Ranks' shares are near-equal and column-aligned; each holds ten lanes of at least
+    (warm-up + timed steps) × the step the benchmark picks."""
+    from rls_b200.grid import recursion_grid
+    k = bench.GRID[6]
+    nZ = len(recursion_grid(*bench.GRID).Z)
+    offs = [bench.column_offset(r, world, nZ, k) for r in range(world)] + [nZ]
+    sizes = np.diff(offs)
+    assert sizes.min() > 0 and sizes.max() - sizes.min() <= k
+    nst = 3 + 5
+    lanes, s = bench.lane_plan(nZ, world, 10, 200, nst, k)
+    assert lanes == 10 and s >= 40
+    for size in sizes:
+        ncols = size // k
+        smallest_lane = (ncols // lanes) * k
+        assert smallest_lane >= nst * s
+
+
+def test_column_offset_rejects_more_ranks_than_columns():
     with pytest.raises(SystemExit):
-        bench.strip_offset(0, 11, 200 * 200, 200 * 20)
+        bench.column_offset(0, 2001, 200 * 200, 20)
