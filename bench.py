@@ -17,8 +17,9 @@ is larger than L2, so every step streams it from HBM.
           The traversal is split on column boundaries (k points) into --lanes
           near-equal concurrent lanes
           (rls_b200.Lanes: one context, stream and host thread per lane); a step is
-          --chunk lane-local points in every lane; device time is the max over the
-          lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
+          --chunk lane-local points in every lane, and the K timed steps run as one
+          lane-parallel call (no wait across lanes between steps); device time is the
+          max over the lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
           with one lane (the reference's single recycled space).
   e2e   : fresh lane contexts through the public C ABI with host buffers: upload
           of the Schur factor from host memory (to lane 0, copied on the device to
@@ -67,7 +68,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk", type=int, default=200,
                     help="grid points per lane per step (at most; lowered to fit the lane's share of the grid)")
-    ap.add_argument("--lanes", type=int, default=10, help="concurrent grid lanes per GPU")
+    ap.add_argument("--lanes", type=int, default=20, help="concurrent grid lanes per GPU")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
@@ -350,7 +351,10 @@ def run_ours(args):
 
     def timed_lanes(nl, profile):
         """W warm-up and K timed steps of `nl` concurrent lanes; a step is `s` lane-local points
-        in every lane.  Device time = max over the lanes' streams of CUDA-event spans."""
+        in every lane.  The K timed steps are one lane-parallel call: each lane walks its K·s
+        points without waiting for the other lanes at step boundaries, as one psTriRecy call
+        with lanes does over a whole grid.  Device time = max over the lanes' streams of
+        CUDA-event spans."""
         ls = R.Lanes(nl, local, T)
         offs = ls.offsets(sub)
         if need > int(np.min(np.diff(offs))):
@@ -377,9 +381,7 @@ def run_ours(args):
         l0 = ls.launches()
         for e, st_ in zip(ev0, streams):
             e.record(st_)
-        for k in range(args.steps):
-            a = (args.warmup + k) * s
-            ls.pstrirecy_range(sub, ctl, a, a + s, sig, st, cst)
+        ls.pstrirecy_range(sub, ctl, args.warmup * s, need, sig, st, cst)
         for e, st_ in zip(ev1, streams):
             e.record(st_)
         for e in ev1:
