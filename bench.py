@@ -22,8 +22,8 @@ is larger than L2, so every step streams it from HBM.
           max over the lanes' streams of CUDA-event spans.  single_lane repeats the timed steps
           with one lane (the reference's single recycled space).
   e2e   : fresh lane contexts through the public C ABI with host buffers: upload
-          of the Schur factor from host memory (to lane 0, copied on the device to
-          the other lanes) plus steps 0..W+K-1 (grid points in, σ out), wall clock.
+          of the Schur factor from host memory (to lane 0, whose device copy the
+          other lanes share) plus steps 0..W+K-1 (grid points in, σ out), wall clock.
   --impl reference : the CPU restatement (oracle/, the reference's algorithm with
           LAPACK through SciPy on all host cores) on the same traversal, each step
           a bounded sample of --ref-chunk points.
@@ -426,7 +426,7 @@ def run_ours(args):
         e2e = {"value": world * lanes * nsteps * s / el, "unit": "pts/s",
                "h2d_bytes_per_step": int((T_bytes + lanes * nsteps * s * 16) / nsteps),
                "d2h_bytes_per_step": int(lanes * s * 8),
-               "span": f"upload of T (host to lane 0, device copies to the other {lanes - 1}) + steps 0..{nsteps - 1}"}
+               "span": f"upload of T (host to lane 0, shared by the other {lanes - 1}) + steps 0..{nsteps - 1}"}
         e2e["matches_device_run"] = bool(np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12))
 
     out = base_line(args, world)

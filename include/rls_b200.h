@@ -170,9 +170,12 @@ int rls_reorder_to_natural_grid(const rls_grid* g, const rls_c64* Z, int64_t nZ,
  * Host memory. */
 int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
 
-/* Installs on dst the operator already uploaded to src (same device), by a device-to-device
- * copy of its tiles: lane contexts (rls_pstrirecy_schur_lanes) share one host upload.  No
- * reference counterpart. */
+/* Installs on dst the operator already uploaded to src (same device).  The two contexts
+ * share src's device tiles of T, which no call writes after the upload; the tiles are freed
+ * with the last context that uses them, and a later rls_set_schur on either context gives
+ * that context a new copy and leaves the other's operator as it was.  Lane contexts
+ * (rls_pstrirecy_schur_lanes) thereby hold one copy of T between them.  No reference
+ * counterpart. */
 int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src);
 
 /* ---- solvers ------------------------------------------------------------------ */

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -47,7 +48,8 @@ struct rls_ctx {
   // operator
   int64_t n = 0, n_pad = 0;
   int nb = 0;
-  cplx* T = nullptr;        // tiles
+  cplx* T = nullptr;        // tiles (read-only once uploaded)
+  std::shared_ptr<cplx> T_buf;  // owns T; contexts given it by rls_set_schur_copy share it
   cplx* Dinv = nullptr;     // nb tiles
   cplx* G = nullptr;        // tiles of the block-row scaled factor D⁻¹T (k_trsm_scale)
   cplx* trsm_u = nullptr;   // n_pad × 8: the adjoint solve's chain values
@@ -1320,6 +1322,8 @@ extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->owned) cudaFree(b.p);
   ctx->owned.clear();
+  ctx->T_buf.reset();
+  ctx->T = nullptr;
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->hstage) cudaFreeHost(ctx->hstage);
   delete ctx;
@@ -1339,14 +1343,16 @@ extern "C" int rls_ctx_set_log(rls_ctx* ctx, rls_log_fn fn, void* user, int verb
 }
 
 namespace {
-// Installs an operator of order n whose tiles (packed layout, n_pad = 64·ceil(n/64)) are at
-// `tiles` (host memory for kind H2D, another context's device array for D2D), and allocates
-// the per-operator workspaces.
-int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, cudaMemcpyKind kind) {
+// Installs an operator of order n whose tiles (packed layout, n_pad = 64·ceil(n/64)) are
+// either copied from host memory (`tiles`) or, when `shared` is set, another context's
+// device tiles used in place, and allocates the per-operator workspaces.
+int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<cplx> shared) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
-  // drop an old operator and space
-  for (void* q : {(void*)ctx->T, (void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->grad_ws,
+  // drop an old operator (freed with its last user) and space
+  ctx->T_buf.reset();
+  ctx->T = nullptr;
+  for (void* q : {(void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->grad_ws,
                   (void*)ctx->flags, (void*)ctx->ticket, (void*)ctx->trmm_part,
                   (void*)ctx->colpart, (void*)ctx->trmm_uO[0], (void*)ctx->trmm_us[0], (void*)ctx->trmm_Ofirst[0],
                   (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
@@ -1359,8 +1365,26 @@ int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, cudaMemcpyKind ki
   ctx->n_pad = (int64_t)ctx->nb * TILE;
   const int nb = ctx->nb;
   const size_t elems = (size_t)nb * (nb + 1) / 2 * TILE * TILE;
-  RET(dalloc_t(ctx, &ctx->T, elems));
-  CK(cudaMemcpyAsync(ctx->T, tiles, elems * sizeof(cplx), kind, ctx->stream));
+  if (shared) {
+    ctx->T_buf = std::move(shared);
+  } else {
+    cplx* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, elems * sizeof(cplx));
+    if (e != cudaSuccess) {
+      set_err(ctx, "device allocation of %zu bytes failed: %s", elems * sizeof(cplx), cudaGetErrorString(e));
+      return RLS_ERR_NOMEM;
+    }
+    const int dev = ctx->device;
+    ctx->T_buf = std::shared_ptr<cplx>(p, [dev](cplx* q) {
+      int prev = 0;
+      cudaGetDevice(&prev);
+      cudaSetDevice(dev);
+      cudaFree(q);
+      cudaSetDevice(prev);
+    });
+    CK(cudaMemcpyAsync(p, tiles, elems * sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->T = ctx->T_buf.get();
   RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
   RET(dalloc_t(ctx, &ctx->G, elems));
   RET(dalloc_t(ctx, &ctx->trsm_u, (size_t)ctx->n_pad * 8));
@@ -1420,7 +1444,7 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
         }
       }
     }
-  return operator_setup(ctx, n, h.data(), cudaMemcpyHostToDevice);
+  return operator_setup(ctx, n, h.data(), nullptr);
 }
 
 extern "C" int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src) {
@@ -1437,7 +1461,7 @@ extern "C" int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src) {
   rls_ctx* ctx = dst;   // error reports go to dst
   CK(cudaSetDevice(src->device));
   CK(cudaStreamSynchronize(src->stream));
-  return operator_setup(dst, src->n, src->T, cudaMemcpyDeviceToDevice);
+  return operator_setup(dst, src->n, nullptr, src->T_buf);
 }
 
 extern "C" int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0, const rls_lobpcg_control* c,

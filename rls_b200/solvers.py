@@ -368,7 +368,7 @@ class Lanes:
         return self.engines[0].n
 
     def set_schur(self, T):
-        """One host upload to the first lane; the others copy its tiles on the device."""
+        """One host upload to the first lane; the others share its device tiles."""
         self.engines[0].set_schur(T)
         for e in self.engines[1:]:
             check(lib().rls_set_schur_copy(e._h, self.engines[0]._h), e._h)

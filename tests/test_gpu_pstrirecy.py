@@ -12,6 +12,7 @@ from oracle.lobpcg import LobpcgSvdControl as OLobCtl, LobpcgSvdKeep, lobpcg_svd
 from oracle.pstrirecy import InvAdjR
 from oracle import recugrid as ogrid
 import rls_b200 as R
+from rls_b200._lib import lib, check
 from rls_b200.examples import sprand, landau
 
 pytestmark = pytest.mark.gpu
@@ -55,6 +56,32 @@ def test_lobpcg_single_point_matches_oracle(sprand_case):
     # Ritz vector of σ_min agrees with the oracle's up to phase
     ov = abs(np.vdot(X[:, 0], keep.S[:, 0])) / (np.linalg.norm(X[:, 0]) * np.linalg.norm(keep.S[:, 0]))
     assert ov > 1 - 1e-6
+
+
+def test_shared_schur_tiles_survive_reupload_and_source_close(sprand_case):
+    """rls_set_schur_copy shares the source's device tiles: a later rls_set_schur on the source
+    leaves the sharer's operator unchanged, and the sharer keeps working after the source closes."""
+    C, T, normC, grid = sprand_case
+    n, r = T.shape[0], 6
+    X0 = _x0(n, r)
+    z = 0.5 + 0.05j
+    ctl = R.LobpcgSvdControl(m=n, n=n, r=r, conv_range=(1, 1), tol=1e-6, side="L", normC=normC)
+    T2 = 2.0 * T                                         # σ_min(2T − zI) = 2·σ_min(T − z/2·I)
+    src, dst = R.Engine(0), R.Engine(0)
+    src.set_schur(T)
+    check(lib().rls_set_schur_copy(dst._h, src._h), dst._h)
+    dst.n = src.n
+    truth = dense_sigma_min(C, z)
+    s_dst0 = dst.lobpcg_svd_invtri(z, ctl, X0=X0)[3][0]
+    src.set_schur(T2)
+    s_src = src.lobpcg_svd_invtri(z, ctl, X0=X0)[3][0]
+    s_dst1 = dst.lobpcg_svd_invtri(z, ctl, X0=X0)[3][0]
+    src.close()
+    s_dst2 = dst.lobpcg_svd_invtri(z, ctl, X0=X0)[3][0]
+    dst.close()
+    assert abs(s_dst0 - truth) <= 1e-6 * normC
+    assert s_dst1 == s_dst0 and s_dst2 == s_dst0
+    assert abs(s_src - 2.0 * dense_sigma_min(C, z / 2)) <= 1e-4 * normC
 
 
 @pytest.mark.parametrize("p,r", [(60, 6), (6, 2)])
