@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--chunk", type=int, default=200,
                     help="grid points per lane per step (at most; lowered to fit the lane's share of the grid)")
     ap.add_argument("--lanes", type=int, default=20, help="concurrent grid lanes per GPU")
+    ap.add_argument("--trsm-ctas", type=int, default=0,
+                    help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=N_MAT)
@@ -356,6 +358,8 @@ def run_ours(args):
         with lanes does over a whole grid.  Device time = max over the lanes' streams of
         CUDA-event spans."""
         ls = R.Lanes(nl, local, T)
+        if nl > 1:
+            ls.set_trsm_ctas(args.trsm_ctas)
         offs = ls.offsets(sub)
         if need > int(np.min(np.diff(offs))):
             raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds a lane of {int(np.min(np.diff(offs)))} points")
@@ -414,6 +418,8 @@ def run_ours(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ls2 = R.Lanes(lanes, local, T)
+        if lanes > 1:
+            ls2.set_trsm_ctas(args.trsm_ctas)
         sigma2 = np.full(len(sub.Z), np.nan)
         st2 = PsTriRecyStats.alloc(len(sub.Z))
         cst2 = ls2.engines[0].stats_struct(st2)
@@ -435,6 +441,7 @@ def run_ours(args):
     out["config"]["points_per_step"] = lanes * s
     out["config"]["lanes"] = lanes
     out["config"]["chunk"] = s
+    out["config"]["trsm_ctas"] = args.trsm_ctas or "one per half block row"
     out["config"]["parallelism"] = (f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
                                     "(independent traversals from column starts)")
     out["config"]["refine_fraction_timed"] = refines / (lanes * args.steps * s)

@@ -126,6 +126,14 @@ int64_t rls_ctx_launches(const rls_ctx* ctx);
  * rejected point is refined from its own recycle output.  1 = one point at a time
  * (the plain per-point drop-in).  Default 16.  No reference counterpart. */
 int rls_ctx_set_batch(rls_ctx* ctx, int max_points);
+
+/* How the calling thread waits for the device when the engine needs a result on the host
+ * (convergence tests, ranks, error word).  spin_us < 0 (the default): spin until the
+ * stream is idle, the lowest latency for one traversal.  spin_us ≥ 0: poll for that many
+ * microseconds, then sleep until the device is done, so that threads of concurrent lanes
+ * (rls_pstrirecy_schur_lanes) that outnumber the host's cores do not take the cores of
+ * the threads that are issuing work.  No reference counterpart. */
+int rls_ctx_set_host_wait(rls_ctx* ctx, int spin_us);
 /* Ritz basis of the recycle step when the Ritz dimension equals the space size
  * (r_ == p·r): 1 (default) forms X = V·G1·G2 as for r_ < p·r; 0 keeps the
  * reference's X = V·G2 (fastRaylRitz.jl:199-202), whose result depends on the
@@ -177,6 +185,13 @@ int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
  * (rls_pstrirecy_schur_lanes) thereby hold one copy of T between them.  No reference
  * counterpart. */
 int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src);
+
+/* How many CTAs each triangular solve on T − zI occupies (the per-refine R⁻¹ / R⁻ᴴ of
+ * InvMat, src/types/RLSMatrices.jl).  0 (the default) gives one CTA per 32-row half block
+ * row, 2·ceil(n/64), the lowest latency for one traversal; a smaller number, at least 1,
+ * makes each CTA solve several half block rows in dependency order and leaves SMs to
+ * concurrent lanes.  Values above 2·ceil(n/64) act as 0.  No reference counterpart. */
+int rls_set_trsm_ctas(rls_ctx* ctx, int ctas);
 
 /* ---- solvers ------------------------------------------------------------------ */
 

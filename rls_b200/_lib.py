@@ -64,6 +64,8 @@ SIGNATURES = {
     "rls_reorder_to_natural_grid": (C.c_int, [C.POINTER(rls_grid), P, C.c_int64, P, P]),
     "rls_set_schur": (C.c_int, [P, C.c_int64, P, C.c_int64]),
     "rls_set_schur_copy": (C.c_int, [P, P]),
+    "rls_set_trsm_ctas": (C.c_int, [P, C.c_int]),
+    "rls_ctx_set_host_wait": (C.c_int, [P, C.c_int]),
     "rls_pstrirecy_schur": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P, P,
                                       C.POINTER(rls_pstrirecy_stats)]),
     "rls_pstrirecy_schur_range": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P,

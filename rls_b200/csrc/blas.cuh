@@ -403,9 +403,11 @@ inline size_t scale_smem_bytes() { return ((size_t)TILE * SC_ALD + (size_t)TILE 
 //   adj = 0: R x = b   → x_b = D_b⁻¹ b_b − Σ_{J>b} G(b,J) x_J, written to X;
 //   adj = 1: Rᴴ x = b  → u_b = b_b − Σ_{J<b} G(J,b)ᴴ u_J, written to U; k_trsm_finish
 //            then forms X = D⁻ᴴ U block by block.
-// Two CTAs per 64-row block, each owning 32 rows (grid 2·nb, 256 threads), taken by
-// ticket in dependency order: a CTA only waits on the two halves of blocks owned by
-// CTAs that started before it, so every wait ends even when not all CTAs are resident.
+// Work unit: a half block row (32 rows of a 64-row block), 2·nb units, 256 threads per
+// CTA.  Units are taken by ticket in dependency order, and a CTA takes tickets until they
+// run out, so any grid of 1..2·nb CTAs solves the system: a unit only waits on units with
+// smaller tickets, each held by a CTA that is already running, so every wait ends even
+// when not all CTAs are resident.  A smaller grid leaves SMs to concurrent work.
 // Waits are bounded by RLS_SPIN_LIMIT polls; on expiry the CTA records
 // DEVERR_SPIN_TIMEOUT and carries on, so the launch always terminates.  Each
 // dependency costs one 32×64×k product; the next tile is prefetched into registers
@@ -487,64 +489,69 @@ __global__ void __launch_bounds__(256) k_trsm_half(int nb, const cplx* __restric
   cplx* sAcc = sX + TILE * K;          // 32·K
   cplx* sPart = sAcc + 32 * K;         // 8·K·32
   __shared__ int sblk;
-  if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
-  __syncthreads();
-  const int pos = sblk >> 1, h = sblk & 1;
-  const int b = adj ? pos : (nb - 1 - pos);
-  const int64_t r0 = (int64_t)b * TILE + h * 32;   // first row of this half
-  cplx* out = adj ? U : X;                          // where the chain's values live
-  const int ndep = adj ? b : (nb - 1 - b);
-  HalfTile pf;
-  auto dep_of = [&](int d) { return adj ? d : (nb - 1 - d); };
-  auto tile_of = [&](int dep) {
-    return adj ? G + tile_index(dep, b) * (TILE * TILE) : G + tile_index(b, dep) * (TILE * TILE);
-  };
-  if (ndep > 0) pf.load(tile_of(dep_of(0)), h, adj);
-  // start value: D_b⁻¹ b_b (forward) or b_b (adjoint) on this half's rows
-  if (!adj) {
-    HalfTile dt;
-    dt.load(Dinv + (int64_t)b * TILE * TILE, h, 0);
-    for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
-      const int rr = q % TILE, c = q / TILE;
-      sX[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
-    }
-    dt.store(sA, 0);
+  for (;;) {
+    // every thread has read the previous ticket: the unit below passes at least one barrier
+    if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
     __syncthreads();
-    half_product<K>(sA, sX, sPart, sAcc, 0);
-  } else {
+    const int unit = sblk;
+    if (unit >= 2 * nb) break;                        // uniform over the block
+    const int pos = unit >> 1, h = unit & 1;
+    const int b = adj ? pos : (nb - 1 - pos);
+    const int64_t r0 = (int64_t)b * TILE + h * 32;   // first row of this half
+    cplx* out = adj ? U : X;                          // where the chain's values live
+    const int ndep = adj ? b : (nb - 1 - b);
+    HalfTile pf;
+    auto dep_of = [&](int d) { return adj ? d : (nb - 1 - d); };
+    auto tile_of = [&](int dep) {
+      return adj ? G + tile_index(dep, b) * (TILE * TILE) : G + tile_index(b, dep) * (TILE * TILE);
+    };
+    if (ndep > 0) pf.load(tile_of(dep_of(0)), h, adj);
+    // start value: D_b⁻¹ b_b (forward) or b_b (adjoint) on this half's rows
+    if (!adj) {
+      HalfTile dt;
+      dt.load(Dinv + (int64_t)b * TILE * TILE, h, 0);
+      for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
+        const int rr = q % TILE, c = q / TILE;
+        sX[c * TILE + rr] = B[(int64_t)c * ldx + (int64_t)b * TILE + rr];
+      }
+      dt.store(sA, 0);
+      __syncthreads();
+      half_product<K>(sA, sX, sPart, sAcc, 0);
+    } else {
+      for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
+        const int rr = q % 32, c = q / 32;
+        sAcc[c * 32 + rr] = B[(int64_t)c * ldx + r0 + rr];
+      }
+      __syncthreads();
+    }
+    for (int d = 0; d < ndep; ++d) {
+      const int dep = dep_of(d);
+      pf.store(sA, adj);
+      if (d + 1 < ndep) pf.load(tile_of(dep_of(d + 1)), h, adj);   // in flight during the wait
+      if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {             // threads 0 and 32: one half each
+        const int* f = &flags[2 * dep + (threadIdx.x >> 5)];
+        int spins = 0;
+        while (ld_acquire(f) != epoch) {
+          if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
+          if (spins > 64) __nanosleep(32);
+        }
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
+        const int rr = q % TILE, c = q / TILE;
+        sX[c * TILE + rr] = __ldcg(&out[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
+      }
+      __syncthreads();
+      half_product<K>(sA, sX, sPart, sAcc, 1);
+    }
     for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
       const int rr = q % 32, c = q / 32;
-      sAcc[c * 32 + rr] = B[(int64_t)c * ldx + r0 + rr];
+      out[(int64_t)c * ldx + r0 + rr] = sAcc[c * 32 + rr];
     }
+    // bar.sync orders every thread's stores before thread 0's release (cumulative).
     __syncthreads();
+    if (threadIdx.x == 0) st_release(&flags[2 * b + h], epoch);
   }
-  for (int d = 0; d < ndep; ++d) {
-    const int dep = dep_of(d);
-    pf.store(sA, adj);
-    if (d + 1 < ndep) pf.load(tile_of(dep_of(d + 1)), h, adj);   // in flight during the wait
-    if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {             // threads 0 and 32: one half each
-      const int* f = &flags[2 * dep + (threadIdx.x >> 5)];
-      int spins = 0;
-      while (ld_acquire(f) != epoch) {
-        if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
-        if (spins > 64) __nanosleep(32);
-      }
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < TILE * K; q += blockDim.x) {
-      const int rr = q % TILE, c = q / TILE;
-      sX[c * TILE + rr] = __ldcg(&out[(int64_t)c * ldx + (int64_t)dep * TILE + rr]);
-    }
-    __syncthreads();
-    half_product<K>(sA, sX, sPart, sAcc, 1);
-  }
-  for (int q = threadIdx.x; q < 32 * K; q += blockDim.x) {
-    const int rr = q % 32, c = q / 32;
-    out[(int64_t)c * ldx + r0 + rr] = sAcc[c * 32 + rr];
-  }
-  // bar.sync orders every thread's stores before thread 0's release (cumulative).
-  __syncthreads();
-  if (threadIdx.x == 0) st_release(&flags[2 * b + h], epoch);
 }
 
 // X_b = D_b⁻ᴴ U_b on each half block row (grid 2·nb, 256 threads): the last step of the

@@ -57,6 +57,7 @@ struct rls_ctx {
   cplx z_dinv = cmk(NAN, NAN);
   int* flags = nullptr;     // 2·nb (one per half block row)
   int* ticket = nullptr;    // 1
+  int trsm_ctas = 0;        // CTAs of a triangular solve (0: one per half block row)
   int epoch = 0;
   int* trmm_uO[2] = {nullptr, nullptr};
   int* trmm_us[2] = {nullptr, nullptr};
@@ -124,6 +125,10 @@ struct rls_ctx {
   // blocking host waits on the stream, counted while profiling
   int64_t host_waits = 0;
   double host_wait_ms = 0.0;
+  // host waits (sync_and_check): < 0 spin in cudaStreamSynchronize; ≥ 0 poll this many
+  // microseconds, then sleep on wait_ev (a blocking-sync event) until the stream reaches it
+  int wait_spin_us = -1;
+  cudaEvent_t wait_ev = nullptr;
 
   // optional per-kernel event timing (rls_ctx_set_profile)
   bool profile = false;
@@ -257,7 +262,21 @@ void prof_resolve(rls_ctx* ctx) {
 int sync_and_check(rls_ctx* ctx) {
   const auto t0 = std::chrono::steady_clock::now();
   CK(cudaMemcpyAsync(ctx->hstage_err, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->wait_spin_us < 0) {
+    CK(cudaStreamSynchronize(ctx->stream));
+  } else {
+    CK(cudaEventRecord(ctx->wait_ev, ctx->stream));
+    const auto until = t0 + std::chrono::microseconds(ctx->wait_spin_us);
+    for (;;) {
+      const cudaError_t q = cudaEventQuery(ctx->wait_ev);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) CK(q);
+      if (std::chrono::steady_clock::now() >= until) {
+        CK(cudaEventSynchronize(ctx->wait_ev));   // the thread sleeps: its core serves other lanes
+        break;
+      }
+    }
+  }
   if (ctx->profile) {
     ctx->host_waits += 1;
     ctx->host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -614,9 +633,10 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
   prof_begin(ctx, KP_TRSM, &e0);
   const size_t smem = trsm_half_smem_bytes(k);
   const unsigned grid = (unsigned)(2 * ctx->nb);
+  const unsigned ctas = ctx->trsm_ctas > 0 ? std::min<unsigned>((unsigned)ctx->trsm_ctas, grid) : grid;
 #define RLS_TRSM_CASE(K)                                                                                         \
   case K:                                                                                                        \
-    k_trsm_half<K><<<grid, 256, smem, ctx->stream>>>(ctx->nb, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, ld, adj,     \
+    k_trsm_half<K><<<ctas, 256, smem, ctx->stream>>>(ctx->nb, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, ld, adj,     \
                                                      ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);           \
     break;
   switch (k) {
@@ -1304,6 +1324,12 @@ extern "C" int rls_ctx_create(rls_ctx** out, int device) {
     st = RLS_ERR_NOMEM;
   }
   if (st == RLS_OK) ctx->hstage_err = reinterpret_cast<int*>(ctx->hstage + kStageBytes);
+  if (st == RLS_OK && cudaEventCreateWithFlags(&ctx->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming) !=
+                          cudaSuccess) {
+    ctx->wait_ev = nullptr;
+    set_err(ctx, "event creation failed");
+    st = RLS_ERR_CUDA;
+  }
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->derr, 4);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->gram_cnt, kGramCounters);
   if (st == RLS_OK) st = dalloc_t(ctx, &ctx->dscal, 256);
@@ -1324,6 +1350,7 @@ extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
   ctx->owned.clear();
   ctx->T_buf.reset();
   ctx->T = nullptr;
+  if (ctx->wait_ev) cudaEventDestroy(ctx->wait_ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->hstage) cudaFreeHost(ctx->hstage);
   delete ctx;
@@ -1445,6 +1472,16 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
       }
     }
   return operator_setup(ctx, n, h.data(), nullptr);
+}
+
+extern "C" int rls_set_trsm_ctas(rls_ctx* ctx, int ctas) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (ctas < 0) {
+    set_err(ctx, "rls_set_trsm_ctas: %d CTAs", ctas);
+    return RLS_ERR_ARG;
+  }
+  ctx->trsm_ctas = ctas;
+  return RLS_OK;
 }
 
 extern "C" int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src) {
@@ -2075,6 +2112,12 @@ extern "C" int rls_pstrirecy_schur_lanes(rls_ctx* const* ctxs, int nlanes, const
 extern "C" void* rls_ctx_stream(rls_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 extern "C" int64_t rls_ctx_launches(const rls_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int rls_ctx_set_host_wait(rls_ctx* ctx, int spin_us) {
+  if (!ctx) return RLS_ERR_ARG;
+  ctx->wait_spin_us = spin_us < 0 ? -1 : spin_us;
+  return RLS_OK;
+}
 
 extern "C" int rls_ctx_set_batch(rls_ctx* ctx, int max_points) {
   if (!ctx || max_points < 1 || max_points > BATCH_MAX) return RLS_ERR_ARG;

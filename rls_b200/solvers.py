@@ -239,6 +239,15 @@ class Engine:
         """Speculative recycle batch size (1 = plain per-point path)."""
         check(lib().rls_ctx_set_batch(self._h, int(max_points)), self._h)
 
+    def set_trsm_ctas(self, ctas: int):
+        """CTAs per triangular solve (0: one per half block row, the single-traversal
+        optimum; fewer leave SMs to concurrent lanes)."""
+        check(lib().rls_set_trsm_ctas(self._h, int(ctas)), self._h)
+
+    def set_host_wait(self, spin_us: int):
+        """Host waits: spin (spin_us < 0, default) or poll spin_us µs and then sleep."""
+        check(lib().rls_ctx_set_host_wait(self._h, int(spin_us)), self._h)
+
     def stream_ptr(self) -> int:
         return int(lib().rls_ctx_stream(self._h) or 0)
 
@@ -377,6 +386,14 @@ class Lanes:
     def set_batch(self, max_points: int):
         for e in self.engines:
             e.set_batch(max_points)
+
+    def set_trsm_ctas(self, ctas: int):
+        for e in self.engines:
+            e.set_trsm_ctas(ctas)
+
+    def set_host_wait(self, spin_us: int):
+        for e in self.engines:
+            e.set_host_wait(spin_us)
 
     def set_profile(self, on: bool):
         for e in self.engines:

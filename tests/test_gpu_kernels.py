@@ -11,7 +11,7 @@ import scipy.linalg as sla
 
 from oracle.linalg import svd_inplace, lq_rows_inplace
 from oracle.recycle import find_rr_dim, affine_combine
-from rls_b200._lib import lib, check, ptr, c64
+from rls_b200._lib import lib, check, ptr, c64, ArgumentError
 from rls_b200.solvers import Engine
 
 pytestmark = pytest.mark.gpu
@@ -47,6 +47,35 @@ def test_trsm_matches_ztrsm(eng_T, adj, k):
     ref = sla.solve_triangular(R, B, lower=False, trans="C" if adj else "N")
     err = np.linalg.norm(X - ref) / np.linalg.norm(ref)
     assert err < 1e-12, err
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+@pytest.mark.parametrize("ctas", [1, 5, 64])
+def test_trsm_on_fewer_ctas_matches_ztrsm(eng_T, adj, ctas):
+    """rls_set_trsm_ctas: CTAs that solve several half block rows each, down to a single
+    CTA walking all of them in dependency order, give the same solution."""
+    e, T = eng_T
+    n = T.shape[0]
+    rng = np.random.default_rng(7 + adj)
+    B = np.asfortranarray(crand(rng, n, 6))
+    z = -0.1 + 0.25j
+    X = np.zeros((n, 6), dtype=np.complex128, order="F")
+    X0 = np.zeros_like(X)
+    check(lib().rls_test_trsm(e._h, c64(z.real, z.imag), adj, 6, ptr(B), ptr(X0)), e._h)
+    check(lib().rls_set_trsm_ctas(e._h, ctas), e._h)
+    try:
+        check(lib().rls_test_trsm(e._h, c64(z.real, z.imag), adj, 6, ptr(B), ptr(X)), e._h)
+    finally:
+        check(lib().rls_set_trsm_ctas(e._h, 0), e._h)
+    ref = sla.solve_triangular(T - z * np.eye(n), B, lower=False, trans="C" if adj else "N")
+    assert np.linalg.norm(X - ref) / np.linalg.norm(ref) < 1e-12
+    assert np.array_equal(X, X0)             # same products in the same order per row
+
+
+def test_set_trsm_ctas_rejects_negative(eng_T):
+    e, _ = eng_T
+    with pytest.raises(ArgumentError):
+        check(lib().rls_set_trsm_ctas(e._h, -1), e._h)
 
 
 @pytest.mark.parametrize("adj", [0, 1])

@@ -58,6 +58,25 @@ def test_lobpcg_single_point_matches_oracle(sprand_case):
     assert ov > 1 - 1e-6
 
 
+def test_sleeping_host_waits_give_identical_sigma(sprand_case):
+    """rls_ctx_set_host_wait only changes how the host thread waits: σ and the per-point
+    statistics are bit-identical to the spinning default."""
+    C, T, normC, grid = sprand_case
+    rec = R.recursion_grid(*grid)
+    n, r = T.shape[0], 6
+    ctl = R.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=20, r=r, recy_tau=1.6)
+    out = []
+    for spin in (-1, 0, 50):
+        e = R.Engine(0)
+        e.set_schur(T)
+        e.set_host_wait(spin)
+        out.append(e.pstrirecy(rec, ctl, X0=_x0(n, r)))
+        e.close()
+    for sig, st in out[1:]:
+        assert np.array_equal(sig, out[0][0])
+        assert np.array_equal(st.refine_it, out[0][1].refine_it)
+
+
 def test_shared_schur_tiles_survive_reupload_and_source_close(sprand_case):
     """rls_set_schur_copy shares the source's device tiles: a later rls_set_schur on the source
     leaves the sharer's operator unchanged, and the sharer keeps working after the source closes."""
