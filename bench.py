@@ -10,8 +10,9 @@ complex128 throughout.
 
 A step is `--chunk` consecutive points of each lane's part of the traversal,
 processed with the lane's recycled space carried from the previous step exactly as
-the reference's loop carries it; W warm-up steps, then K timed steps.  The Schur factor (256 MB)
-is larger than L2, so every step streams it from HBM.
+the reference's loop carries it; W warm-up steps, then K timed steps.  The Schur
+factor's tiles (132 MB; 256 MB dense) and every lane's scaled copy of them (132 MB
+each) are larger than the 126 MB L2, so every step streams them from HBM.
 
   value : points / device time of the K timed steps, Schur factor resident in HBM.
           The traversal is split on column boundaries (k points) into --lanes
@@ -253,7 +254,8 @@ def base_line(args, n_gpus):
             "config": {"workload": "psTriRecy sprand N=4000 dense-Schur, 200x200 grid [0.45,0.55]x[0,0.1], k=20, "
                                    "tol=1e-4, p=60, r=6, recy_tau=1.6",
                        "n": args.n, "grid": list(GRID), "points_per_step": None,
-                       "l2": "inputs larger than L2 (Schur factor 256 MB streamed every step)"}}
+                       "l2": "inputs larger than L2 (Schur tiles 132 MB and each lane's scaled copy 132 MB, "
+                              "streamed every step; L2 126 MB)"}}
 
 
 def run_reference(args):
