@@ -77,6 +77,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_MAT)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmm", action="store_true", help="skip the sparse shifted product measurement")
+    ap.add_argument("--no-ic", action="store_true", help="skip the IC preconditioner apply measurement")
     ap.add_argument("--plain-steps", type=int, default=1, help="steps timed on the unbatched per-point path")
     ap.add_argument("--ncu-window", default=None,
                     help="WARM,COUNT: run WARM points, then COUNT points inside cudaProfilerStart/Stop, and exit "
@@ -229,6 +230,47 @@ def spmm_measure(local, hbm_peak, reps=20, b=6):
         out[name] = {"nnz": int(A.nnz), "b": b, "launches": cnt, "avg_us": ms / cnt * 1e3,
                      "bytes_per_launch": work / cnt, "achieved_gbs": achieved, "frac": achieved / hbm_peak}
         del X, Y
+    return out
+
+
+def lltp_measure(local, hbm_peak, reps=10, b=6):
+    """SparseLLTP ldiv! (psPrecRecy's incomplete-Cholesky preconditioner apply) on the
+    af23560-shaped factor: device-resident B and X, CUDA-event time per call (the engine's
+    profile slot 6).  Beside it, as this operator's CPU baseline, the same apply by the CPU
+    restatement (SciPy sparse substitution, one host thread)."""
+    import torch
+    import ctypes as C
+    from rls_b200._lib import lib
+    from rls_b200.examples import ic_factor_banded
+    from rls_b200.solvers import Engine, SparseLLTP
+    n = 23560
+    L = ic_factor_banded(n, 300, 2.0 / 3.0, seed=20260318, complex_values=False)
+    p = np.random.default_rng(7).permutation(n)
+    invp = np.argsort(p)
+    e = Engine(local)
+    SparseLLTP(L, p, invp, e)
+    dB = torch.randn((b, n), dtype=torch.complex128, device="cuda")
+    dX = torch.empty_like(dB)
+    torch.cuda.synchronize()
+    fn = lib().rls_lltp_ldiv_dev
+    for _ in range(3):
+        fn(e._h, b, C.c_void_p(dB.data_ptr()), n, C.c_void_p(dX.data_ptr()), n)
+    e.set_profile(True)
+    for _ in range(reps):
+        fn(e._h, b, C.c_void_p(dB.data_ptr()), n, C.c_void_p(dX.data_ptr()), n)
+    cnt, ms, work = e.profile(6)
+    e.close()
+    achieved = (work / cnt) / (ms / cnt / 1e3) / 1e9
+    out = {"factor": "af23560-shaped IC factor: n=23560, lower band 300, fill 2/3, real", "nnz": int(L.nnz),
+           "b": b, "calls": cnt, "avg_us": ms / cnt * 1e3, "bytes_per_call": work / cnt, "achieved_gbs": achieved,
+           "frac": achieved / hbm_peak}
+    from oracle.precond import lltp_ldiv
+    B = np.random.default_rng(8).standard_normal((n, b)) + 0j
+    t0 = time.perf_counter()
+    lltp_ldiv(L, p, invp, B)
+    out["cpu_baseline"] = {"avg_us": (time.perf_counter() - t0) * 1e6, "cores": 1, "kind": "port",
+                           "sample": "one apply, SciPy spsolve_triangular forward and backward"}
+    del dB, dX
     return out
 
 
@@ -483,6 +525,8 @@ def run_ours(args):
         out["heev_fp64"] = {"gflops": f1 / (t1 / 1e3) / 1e9, "launches": c1, "avg_us": t1 / c1 * 1e3}
     if rank == 0 and world == 1 and not args.no_spmm:
         out["spmm_shifted"] = spmm_measure(local, hbm_peak)
+    if rank == 0 and world == 1 and not args.no_ic:
+        out["ic_precond_apply"] = lltp_measure(local, hbm_peak)
     if rank == 0 and world == 1:
         from oracle.pstrirecy import PsTriRecyControl as OC
         from oracle import recugrid as G

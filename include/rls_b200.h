@@ -32,7 +32,8 @@ typedef enum {
   RLS_ERR_NOMEM = -4,      /* device allocation failed                  */
   RLS_ERR_TIMEOUT = -5,    /* a bounded device wait gave up             */
   RLS_ERR_BREAKDOWN = -6,  /* numerical breakdown (LAPACK info != 0)    */
-  RLS_ERR_STATE = -7       /* call order (e.g. no operator uploaded)    */
+  RLS_ERR_STATE = -7,      /* call order (e.g. no operator uploaded)    */
+  RLS_ERR_SINGULAR = -8    /* SingularException in the reference        */
 } rls_status;
 
 /* Grid description; mirrors the fields of `Recursion` (src/core/recuGrid.jl:1-12). */
@@ -145,7 +146,8 @@ int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always);
  * milliseconds and algorithmic work (bytes; flops for kernel 1).  kernel 4
  * returns the host's blocking waits on the stream instead: their number and
  * total wall milliseconds (work = 0); kernel 5 is the sparse shifted product
- * (rls_spmm_shifted*).  No reference counterpart (the reference times phases
+ * (rls_spmm_shifted*); kernel 6 the preconditioner solve (rls_lltp_ldiv*).  No
+ * reference counterpart (the reference times phases
  * with time_ns, psTriRecy.jl:306-309). */
 int rls_ctx_set_profile(rls_ctx* ctx, int on);
 int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work);
@@ -266,6 +268,27 @@ int rls_spmm_shifted(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, 
                      rls_c64* Y, int64_t ldy);
 int rls_spmm_shifted_dev(rls_ctx* ctx, rls_c64 s, int adj, int b, const rls_c64* X, int64_t ldx,
                          rls_c64* Y, int64_t ldy);
+
+/* ---- incomplete-Cholesky preconditioner apply (psPrecRecy) ------------------------ */
+
+/* Uploads the factor of a SparseLLTP (src/preconditioner/RLSPreconditioner.jl:8-26, built
+ * by get_hsl_LLTP, hsl_preconditioner.jl:159-252): L, n × n in the reference's CSC layout
+ * (colptr n+1, rowval and nzval nnz; only the lower triangle is used, as
+ * LowerTriangular(L) does), the permutation p and its inverse invp as the struct holds
+ * them.  Indices are base 0 or 1 (1 = Julia's SparseMatrixCSC and Vector{Int}).  A real L
+ * is passed with zero imaginary parts.  Replaces any earlier factor of the context. */
+int rls_lltp_upload(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                    const rls_c64* nzval, const int64_t* p, const int64_t* invp, int base);
+
+/* ldiv!(X, K, B) for the uploaded SparseLLTP (RLSPreconditioner.jl:79-116):
+ * temp = B[p, :]; X = L \ temp; temp = Lᴴ \ X; X = temp[invp, :], i.e. X = P·L⁻ᴴ·L⁻¹·Pᴴ·B,
+ * B and X n × b, column-major with leading dimensions ldb, ldx.  rls_lltp_ldiv takes host
+ * buffers and may be given X == B (the reference's ldiv!(K, B)); rls_lltp_ldiv_dev takes
+ * device pointers with X ≠ B.  Both return when X is written.  A zero or absent diagonal
+ * entry of L gives RLS_ERR_SINGULAR, naming the first such index j as the reference's
+ * SingularException(j) does. */
+int rls_lltp_ldiv(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx);
+int rls_lltp_ldiv_dev(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx);
 
 /* ---- gradient -------------------------------------------------------------------- */
 

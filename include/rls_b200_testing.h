@@ -3,7 +3,7 @@
  * parity tests.  They have no counterpart in the reference: each runs one device
  * routine of the engine on host inputs so that it can be compared with the
  * LAPACK routine the reference calls at that point.  Host pointers, column-major.
- * All need rls_set_schur() and rls_test_setup() first.
+ * All but rls_test_lltp_plan_dense need rls_set_schur() and rls_test_setup() first.
  */
 #ifndef RLS_B200_TESTING_H
 #define RLS_B200_TESTING_H
@@ -13,6 +13,16 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* Host only (no context, no device): the block-row form that rls_lltp_upload builds for
+ * L (op = 0) or Lᴴ (op = 1), checked for what the device solve relies on (every off-block
+ * term reads a block row solved before its own, indices in range, in-block terms strictly
+ * on the solved side of the diagonal) and written out as the dense n × n operator it
+ * stands for (n ≤ 4096, column-major).  singular_at receives the first 1-based index with
+ * a zero diagonal (0 if none), levels the longest chain of dependent block rows.  Compare
+ * tril(L) or its adjoint. */
+int rls_test_lltp_plan_dense(int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval,
+                             int base, int op, rls_c64* dense, int64_t* singular_at, int* levels);
 
 /* Allocates the recycled-space and LOBPCG workspaces for block size r and p_max blocks. */
 int rls_test_setup(rls_ctx* ctx, int r, int p_max);

@@ -15,13 +15,13 @@ _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_grid_linear,
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
-from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SchurFactor,
-                      pre_process, psTriRecy)
-from ._lib import RLSError, ArgumentError, DimensionMismatch
+from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
+                      SchurFactor, pre_process, psTriRecy)
+from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
-    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SchurFactor", "pre_process", "psTriRecy", "RLSError",
-    "ArgumentError", "DimensionMismatch",
+    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
+    "psTriRecy", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException",
 ]

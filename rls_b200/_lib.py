@@ -77,6 +77,9 @@ SIGNATURES = {
     "rls_sparse_upload_csc": (C.c_int, [P, C.c_int64, C.c_int64, P, P, P, C.c_int]),
     "rls_spmm_shifted": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),
     "rls_spmm_shifted_dev": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),
+    "rls_lltp_upload": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.c_int]),
+    "rls_lltp_ldiv": (C.c_int, [P, C.c_int, P, C.c_int64, P, C.c_int64]),
+    "rls_lltp_ldiv_dev": (C.c_int, [P, C.c_int, P, C.c_int64, P, C.c_int64]),
     "rls_lane_offsets": (C.c_int, [C.POINTER(rls_grid), C.c_int64, C.c_int, P]),
     "rls_pstrirecy_schur_lanes": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
                                             C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),
@@ -91,6 +94,7 @@ SIGNATURES = {
     # kernel-level test entry points (include/rls_b200_testing.h)
     "rls_test_setup": (C.c_int, [P, C.c_int, C.c_int]),
     "rls_test_trsm": (C.c_int, [P, c64, C.c_int, C.c_int, P, P]),
+    "rls_test_lltp_plan_dense": (C.c_int, [C.c_int64, P, P, P, C.c_int, C.c_int, P, P, P]),
     "rls_test_trmm": (C.c_int, [P, C.c_int, C.c_int, P, P]),
     "rls_test_qr": (C.c_int, [P, C.c_int64, C.c_int, P, P, P]),
     "rls_test_svd_rr": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P, P]),
@@ -132,6 +136,10 @@ class ArgumentError(RLSError, ValueError):
     """Raised where the reference throws ArgumentError."""
 
 
+class SingularException(RLSError):
+    """Raised where the reference throws LinearAlgebra.SingularException."""
+
+
 def check(status, ctx=None):
     if status == 0:
         return
@@ -143,6 +151,8 @@ def check(status, ctx=None):
         raise DimensionMismatch(status, msg)
     if status == -1:
         raise ArgumentError(status, msg)
+    if status == -8:
+        raise SingularException(status, msg)
     raise RLSError(status, msg)
 
 

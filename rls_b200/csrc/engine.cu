@@ -24,6 +24,7 @@
 #include "rotate.cuh"
 #include "small.cuh"
 #include "sparse.cuh"
+#include "sptrsv.cuh"
 
 namespace {
 
@@ -148,12 +149,26 @@ struct rls_ctx {
     double ms = 0.0;
     double bytes = 0.0;
     std::vector<double> pending_bytes;
-  } kprof[6];                      // 0..3 kernels below, 4 unused (host waits), 5 sparse products
+  } kprof[7];                      // 0..3 kernels below, 4 unused (host waits), 5 sparse products
 
   rls_pstrirecy_stats lane_stats{};   // this context's run as one lane of rls_pstrirecy_schur_lanes_range
   CsrDev sp[2];                        // uploaded sparse C: [0] CSR of C, [1] CSR of Cᴴ
   cplx* sp_xr = nullptr;               // row-major copy of up to 8 columns of X
   size_t sp_xr_elems = 0;
+
+  // SparseLLTP factor (rls_lltp_upload): [0] rows of L, [1] rows of Lᴴ
+  struct Lltp {
+    int64_t n = 0;
+    TriBlocks op[2];
+    int64_t* p = nullptr;        // 0-based
+    int64_t* invp = nullptr;
+    cplx* w1 = nullptr;          // n × 8: L⁻¹·Pᴴ·B (one chunk of columns)
+    cplx* w2 = nullptr;          // n × 8: Lᴴ⁻¹ of it
+    int* flags = nullptr;        // 2·nblk: published block rows, [0, nblk) for L, [nblk, 2·nblk) for Lᴴ
+    int* ticket = nullptr;       // 2
+    int epoch = 0;
+    int64_t singular_at = 0;     // first 1-based index with a zero diagonal, 0 if none
+  } lltp;
 
   std::vector<DevBuf> owned;
 };
@@ -221,7 +236,7 @@ int check_launch(rls_ctx* ctx, const char* what) {
   return RLS_OK;
 }
 
-enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3, KP_SPMM = 5 };
+enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3, KP_SPMM = 5, KP_SPTRSV = 6 };
 
 void prof_begin(rls_ctx* ctx, int id, cudaEvent_t* e0) {
   if (!ctx->profile) return;
@@ -1296,6 +1311,7 @@ extern "C" const char* rls_status_string(int s) {
     case RLS_ERR_TIMEOUT: return "bounded device wait expired";
     case RLS_ERR_BREAKDOWN: return "numerical breakdown";
     case RLS_ERR_STATE: return "invalid call order";
+    case RLS_ERR_SINGULAR: return "singular triangular factor";
     default: return "unknown status";
   }
 }
@@ -2026,6 +2042,324 @@ extern "C" int rls_spmm_shifted(rls_ctx* ctx, rls_c64 s, int adj, int b, const r
   return st;
 }
 
+// ---- SparseLLTP ldiv! (RLSPreconditioner.jl:79-116) ----------------------------------
+
+namespace {
+// Host form of one triangular operator in block rows (see sptrsv.cuh).
+struct TriHost {
+  int64_t n = 0, nblk = 0;
+  std::vector<int64_t> rowptr;
+  std::vector<int32_t> col;
+  std::vector<cplx> val, blk, dinv;
+  int levels = 0;   // longest chain of block rows (a block row with no off-block term is level 1)
+};
+
+// Block-row forms of L (op[0]) and Lᴴ (op[1]) from the CSC of L.  Only the lower triangle is
+// read, as LowerTriangular(L) does; duplicate entries add up.  L's off-block terms are kept in
+// ascending column order per row and Lᴴ's in descending order, so that a row reads the block
+// rows finished last at the end.  Returns the first 1-based index whose diagonal is zero or
+// absent (the j of the reference's SingularException(j)), or 0.
+int64_t lltp_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval, int base,
+                  TriHost op[2]) {
+  const int64_t nblk = (n + SPT_ROWS - 1) / SPT_ROWS;
+  std::vector<cplx> diag((size_t)n, czero());
+  for (int t = 0; t < 2; ++t) {
+    op[t] = TriHost{};
+    op[t].n = n;
+    op[t].nblk = nblk;
+    op[t].rowptr.assign((size_t)n + 1, 0);
+    op[t].blk.assign((size_t)nblk * SPT_ROWS * SPT_ROWS, czero());
+    op[t].dinv.assign((size_t)n, czero());
+  }
+  auto in_blk = [&](int t, int64_t row, int64_t x) -> cplx& {   // coefficient of x[x] in row `row`
+    const int64_t b = row / SPT_ROWS;
+    return op[t].blk[(size_t)((b * SPT_ROWS + x % SPT_ROWS) * SPT_ROWS + row % SPT_ROWS)];
+  };
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t e = colptr[c] - base; e < colptr[c + 1] - base; ++e) {
+      const int64_t r = rowval[e] - base;
+      const cplx v = cmk(nzval[e].re, nzval[e].im);
+      if (r < c) continue;
+      if (r == c) { diag[(size_t)c] = cadd(diag[(size_t)c], v); continue; }
+      if (r / SPT_ROWS == c / SPT_ROWS) {
+        in_blk(0, r, c) = cadd(in_blk(0, r, c), v);            // row r of L reads x[c]
+        in_blk(1, c, r) = cadd(in_blk(1, c, r), cconj(v));     // row c of Lᴴ reads x[r]
+      } else {
+        ++op[0].rowptr[(size_t)r + 1];
+        ++op[1].rowptr[(size_t)c + 1];
+      }
+    }
+  for (int t = 0; t < 2; ++t) {
+    for (int64_t i = 0; i < n; ++i) op[t].rowptr[(size_t)i + 1] += op[t].rowptr[(size_t)i];
+    op[t].col.resize((size_t)op[t].rowptr[(size_t)n]);
+    op[t].val.resize((size_t)op[t].rowptr[(size_t)n]);
+  }
+  std::vector<int64_t> next0(op[0].rowptr.begin(), op[0].rowptr.end() - 1);
+  std::vector<int64_t> next1(op[1].rowptr.begin(), op[1].rowptr.end() - 1);
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t e = colptr[c] - base; e < colptr[c + 1] - base; ++e) {
+      const int64_t r = rowval[e] - base;
+      if (r <= c || r / SPT_ROWS == c / SPT_ROWS) continue;
+      const cplx v = cmk(nzval[e].re, nzval[e].im);
+      const int64_t q0 = next0[(size_t)r]++;
+      op[0].col[(size_t)q0] = (int32_t)c;
+      op[0].val[(size_t)q0] = v;
+      const int64_t q1 = next1[(size_t)c]++;
+      op[1].col[(size_t)q1] = (int32_t)r;
+      op[1].val[(size_t)q1] = cconj(v);
+    }
+  // Lᴴ rows: descending solution index (nearest block rows last); L rows are ascending already
+  // when the CSC columns are visited in order, and the sort below only fixes unsorted input.
+  for (int t = 0; t < 2; ++t)
+    for (int64_t i = 0; i < n; ++i) {
+      const size_t a = (size_t)op[t].rowptr[(size_t)i], z = (size_t)op[t].rowptr[(size_t)i + 1];
+      if (z - a < 2) continue;
+      std::vector<std::pair<int32_t, cplx>> row(z - a);
+      for (size_t q = a; q < z; ++q) row[q - a] = {op[t].col[q], op[t].val[q]};
+      if (t == 0)
+        std::stable_sort(row.begin(), row.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      else
+        std::stable_sort(row.begin(), row.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+      for (size_t q = a; q < z; ++q) { op[t].col[q] = row[q - a].first; op[t].val[q] = row[q - a].second; }
+    }
+  int64_t singular = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const cplx d = diag[(size_t)i];
+    if (d.x == 0.0 && d.y == 0.0) {
+      if (!singular) singular = i + 1;
+      continue;
+    }
+    op[0].dinv[(size_t)i] = cinv(d);
+    op[1].dinv[(size_t)i] = cinv(cconj(d));
+  }
+  // chain lengths in block rows
+  for (int t = 0; t < 2; ++t) {
+    std::vector<int> lev((size_t)nblk, 1);
+    int best = nblk > 0 ? 1 : 0;
+    for (int64_t q = 0; q < nblk; ++q) {
+      const int64_t b = t == 0 ? q : nblk - 1 - q;
+      int l = 1;
+      for (int64_t i = b * SPT_ROWS; i < std::min(n, (b + 1) * SPT_ROWS); ++i)
+        for (int64_t e = op[t].rowptr[(size_t)i]; e < op[t].rowptr[(size_t)i + 1]; ++e)
+          l = std::max(l, lev[(size_t)(op[t].col[(size_t)e] / SPT_ROWS)] + 1);
+      lev[(size_t)b] = l;
+      best = std::max(best, l);
+    }
+    op[t].levels = best;
+  }
+  return singular;
+}
+
+// Argument checks shared by rls_lltp_upload and the plan test entry.
+int lltp_check_csc(int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval, int base,
+                   std::string& why) {
+  if (n < 1 || n >= (1ll << 31) || !colptr || (base != 0 && base != 1)) {
+    why = "invalid arguments (n=" + std::to_string(n) + ", base=" + std::to_string(base) + ")";
+    return RLS_ERR_ARG;
+  }
+  const int64_t nnz = colptr[n] - base;
+  if (nnz < 0 || colptr[0] != base || (nnz > 0 && (!rowval || !nzval))) {
+    why = "inconsistent column pointers";
+    return RLS_ERR_DIM;
+  }
+  for (int64_t c = 0; c < n; ++c)
+    if (colptr[c + 1] < colptr[c]) {
+      why = "column pointers decrease at column " + std::to_string(c + 1);
+      return RLS_ERR_DIM;
+    }
+  for (int64_t e = 0; e < nnz; ++e)
+    if (rowval[e] - base < 0 || rowval[e] - base >= n) {
+      why = "row index " + std::to_string(rowval[e] - base + 1) + " out of range 1.." + std::to_string(n);
+      return RLS_ERR_DIM;
+    }
+  return RLS_OK;
+}
+
+int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int64_t ldx) {
+  auto& F = ctx->lltp;
+  if (!F.op[0].rowptr) {
+    set_err(ctx, "no preconditioner factor uploaded (call rls_lltp_upload first)");
+    return RLS_ERR_STATE;
+  }
+  if (b < 1 || !B || !X || ldb < F.n || ldx < F.n) {
+    set_err(ctx, "rls_lltp_ldiv: invalid block (b=%d, ldb=%lld, ldx=%lld, n=%lld)", b, (long long)ldb,
+            (long long)ldx, (long long)F.n);
+    return RLS_ERR_DIM;
+  }
+  if (F.singular_at) {
+    set_err(ctx, "SingularException(%lld): the factor's diagonal entry %lld is zero", (long long)F.singular_at,
+            (long long)F.singular_at);
+    return RLS_ERR_SINGULAR;
+  }
+  const int64_t nblk = F.op[0].nblk;
+  const unsigned grid = (unsigned)std::min<int64_t>((nblk + 3) / 4, 148 * 4);
+  const unsigned gg = (unsigned)((F.n + 255) / 256);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ctx->profile) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, ctx->stream));
+  }
+  for (int c0 = 0; c0 < b; c0 += 8) {
+    const int kk = std::min(8, b - c0);
+    F.epoch += 1;
+    if (F.epoch > (1 << 30)) {
+      F.epoch = 1;
+      CK(cudaMemsetAsync(F.flags, 0, sizeof(int) * 2 * nblk, ctx->stream));
+    }
+    CK(cudaMemsetAsync(F.ticket, 0, 2 * sizeof(int), ctx->stream));
+    const cplx* Bc = B + (int64_t)c0 * ldb;
+    cplx* Xc = X + (int64_t)c0 * ldx;
+#define RLS_SPT_CASE(K)                                                                                            \
+  case K:                                                                                                          \
+    k_sptrsv_blocks<K, false><<<grid, 128, 0, ctx->stream>>>(F.op[0], Bc, ldb, F.p, F.w1, F.n, F.ticket, F.flags,   \
+                                                             F.epoch, ctx->derr);                                  \
+    k_sptrsv_blocks<K, true><<<grid, 128, 0, ctx->stream>>>(F.op[1], F.w1, F.n, nullptr, F.w2, F.n, F.ticket + 1,   \
+                                                            F.flags + nblk, F.epoch, ctx->derr);                   \
+    k_gather_rows<K><<<gg, 256, 0, ctx->stream>>>(F.n, F.invp, F.w2, F.n, Xc, ldx);                                \
+    break;
+    switch (kk) {
+      RLS_SPT_CASE(1) RLS_SPT_CASE(2) RLS_SPT_CASE(3) RLS_SPT_CASE(4)
+      RLS_SPT_CASE(5) RLS_SPT_CASE(6) RLS_SPT_CASE(7) RLS_SPT_CASE(8)
+    }
+#undef RLS_SPT_CASE
+    RET(check_launch(ctx, "k_sptrsv_blocks"));
+  }
+  if (ctx->profile) {
+    CK(cudaEventRecord(e1, ctx->stream));
+    auto& k = ctx->kprof[KP_SPTRSV];
+    k.ev.push_back(e0);
+    k.ev.push_back(e1);
+    // algorithmic bytes per 8-column chunk: both operators' off-block entries (value + column),
+    // row pointers, diagonal blocks and inverse diagonals once; B read, the two intermediates
+    // written and read, X written
+    double ops = 0.0;
+    for (const auto& o : F.op)
+      ops += (double)o.nnz_off * (sizeof(cplx) + sizeof(int32_t)) + (double)(o.n + 1) * sizeof(int64_t) +
+             (double)o.nblk * SPT_ROWS * SPT_ROWS * sizeof(cplx) + (double)o.n * sizeof(cplx);
+    k.pending_bytes.push_back((double)((b + 7) / 8) * ops + 6.0 * (double)b * (double)F.n * sizeof(cplx));
+  }
+  return RLS_OK;
+}
+}  // namespace
+
+extern "C" int rls_lltp_upload(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                               const rls_c64* nzval, const int64_t* p, const int64_t* invp, int base) {
+  if (!ctx) return RLS_ERR_ARG;
+  std::string why;
+  int st = lltp_check_csc(n, colptr, rowval, nzval, base, why);
+  if (st != RLS_OK) {
+    set_err(ctx, "rls_lltp_upload: %s", why.c_str());
+    return st;
+  }
+  if (!p || !invp) {
+    set_err(ctx, "rls_lltp_upload: the permutation and its inverse are required");
+    return RLS_ERR_ARG;
+  }
+  for (int64_t i = 0; i < n; ++i)
+    if (p[i] - base < 0 || p[i] - base >= n || invp[i] - base < 0 || invp[i] - base >= n) {
+      set_err(ctx, "rls_lltp_upload: permutation entry %lld out of range 1..%lld", (long long)(i + 1), (long long)n);
+      return RLS_ERR_DIM;
+    }
+  TriHost h[2];
+  const int64_t singular = lltp_plan(n, colptr, rowval, nzval, base, h);
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  auto& F = ctx->lltp;
+  for (auto& o : F.op) {
+    for (void* q : {(void*)o.rowptr, (void*)o.col, (void*)o.val, (void*)o.blk, (void*)o.dinv}) dfree(ctx, q);
+    o = TriBlocks{};
+  }
+  for (void* q : {(void*)F.p, (void*)F.invp, (void*)F.w1, (void*)F.w2, (void*)F.flags, (void*)F.ticket})
+    dfree(ctx, q);
+  F = rls_ctx::Lltp{};
+  const int64_t nblk = h[0].nblk;
+  std::vector<int64_t> p0((size_t)n), ip0((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    p0[(size_t)i] = p[i] - base;
+    ip0[(size_t)i] = invp[i] - base;
+  }
+  for (int t = 0; t < 2; ++t) {
+    TriBlocks& o = F.op[t];
+    o.n = n;
+    o.nblk = nblk;
+    o.nnz_off = h[t].rowptr[(size_t)n];
+    RET(dalloc_t(ctx, &o.rowptr, (size_t)n + 1));
+    RET(dalloc_t(ctx, &o.col, (size_t)std::max<int64_t>(o.nnz_off, 1)));
+    RET(dalloc_t(ctx, &o.val, (size_t)std::max<int64_t>(o.nnz_off, 1)));
+    RET(dalloc_t(ctx, &o.blk, h[t].blk.size()));
+    RET(dalloc_t(ctx, &o.dinv, (size_t)n));
+    CK(cudaMemcpyAsync(o.rowptr, h[t].rowptr.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream));
+    if (o.nnz_off > 0) {
+      CK(cudaMemcpyAsync(o.col, h[t].col.data(), sizeof(int32_t) * o.nnz_off, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(o.val, h[t].val.data(), sizeof(cplx) * o.nnz_off, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(o.blk, h[t].blk.data(), sizeof(cplx) * h[t].blk.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(o.dinv, h[t].dinv.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  RET(dalloc_t(ctx, &F.p, (size_t)n));
+  RET(dalloc_t(ctx, &F.invp, (size_t)n));
+  RET(dalloc_t(ctx, &F.w1, (size_t)n * 8));
+  RET(dalloc_t(ctx, &F.w2, (size_t)n * 8));
+  RET(dalloc_t(ctx, &F.flags, (size_t)2 * nblk));
+  RET(dalloc_t(ctx, &F.ticket, 2));
+  CK(cudaMemcpyAsync(F.p, p0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(F.invp, ip0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  F.n = n;
+  F.singular_at = singular;
+  CK(cudaStreamSynchronize(ctx->stream));   // the host arrays must outlive the copies
+  return RLS_OK;
+}
+
+extern "C" int rls_lltp_ldiv_dev(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx) {
+  if (!ctx) return RLS_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (B == X) {
+    set_err(ctx, "rls_lltp_ldiv_dev: X must not alias B (use rls_lltp_ldiv for the in-place form)");
+    return RLS_ERR_ARG;
+  }
+  RET(lltp_ldiv_dev(ctx, b, reinterpret_cast<const cplx*>(B), ldb, reinterpret_cast<cplx*>(X), ldx));
+  return sync_and_check(ctx);
+}
+
+extern "C" int rls_lltp_ldiv(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx) {
+  if (!ctx) return RLS_ERR_ARG;
+  const int64_t n = ctx->lltp.n;
+  if (!ctx->lltp.op[0].rowptr) {
+    set_err(ctx, "no preconditioner factor uploaded (call rls_lltp_upload first)");
+    return RLS_ERR_STATE;
+  }
+  if (b < 1 || !B || !X || ldb < n || ldx < n) {
+    set_err(ctx, "rls_lltp_ldiv: invalid block (b=%d, ldb=%lld, ldx=%lld, n=%lld)", b, (long long)ldb,
+            (long long)ldx, (long long)n);
+    return RLS_ERR_DIM;
+  }
+  CK(cudaSetDevice(ctx->device));
+  cplx *dB = nullptr, *dX = nullptr;
+  if (cudaMalloc(&dB, sizeof(cplx) * n * b) != cudaSuccess || cudaMalloc(&dX, sizeof(cplx) * n * b) != cudaSuccess) {
+    cudaFree(dB);
+    set_err(ctx, "rls_lltp_ldiv: device allocation failed");
+    return RLS_ERR_NOMEM;
+  }
+  int st = RLS_OK;
+  if (cudaMemcpy2DAsync(dB, n * sizeof(cplx), B, ldb * sizeof(cplx), n * sizeof(cplx), b, cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess) {
+    set_err(ctx, "rls_lltp_ldiv: copy failed");
+    st = RLS_ERR_CUDA;
+  }
+  if (st == RLS_OK) st = lltp_ldiv_dev(ctx, b, dB, n, dX, n);
+  if (st == RLS_OK && cudaMemcpy2DAsync(X, ldx * sizeof(cplx), dX, n * sizeof(cplx), n * sizeof(cplx), b,
+                                        cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
+    set_err(ctx, "rls_lltp_ldiv: copy failed");
+    st = RLS_ERR_CUDA;
+  }
+  if (st == RLS_OK) st = sync_and_check(ctx);
+  else cudaStreamSynchronize(ctx->stream);
+  cudaFree(dB);
+  cudaFree(dX);
+  return st;
+}
+
 extern "C" int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets) {
   if (!g || nZ < 0 || nlanes < 1 || !offsets) return RLS_ERR_ARG;
   // lanes start on column boundaries of the zigzag traversal (k points: one grid column of
@@ -2147,7 +2481,7 @@ extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
 }
 
 extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work) {
-  if (!ctx || kernel < 0 || kernel > 5) return RLS_ERR_ARG;
+  if (!ctx || kernel < 0 || kernel > 6) return RLS_ERR_ARG;
   RET(sync_and_check(ctx));
   prof_resolve(ctx);
   if (kernel == 4) {

@@ -35,6 +35,69 @@ int need_space(rls_ctx* ctx) {
 
 }  // namespace
 
+extern "C" int rls_test_lltp_plan_dense(int64_t n, const int64_t* colptr, const int64_t* rowval,
+                                        const rls_c64* nzval, int base, int op, rls_c64* dense,
+                                        int64_t* singular_at, int* levels) {
+  std::string why;
+  int st = lltp_check_csc(n, colptr, rowval, nzval, base, why);
+  if (st != RLS_OK) {
+    g_create_err = "rls_test_lltp_plan_dense: " + why;
+    return st;
+  }
+  if ((op != 0 && op != 1) || n > 4096 || !dense) {
+    g_create_err = "rls_test_lltp_plan_dense: invalid arguments";
+    return RLS_ERR_ARG;
+  }
+  TriHost h[2];
+  const int64_t sing = lltp_plan(n, colptr, rowval, nzval, base, h);
+  const TriHost& o = h[op];
+  auto fail = [&](const std::string& what) {
+    g_create_err = "rls_test_lltp_plan_dense: plan invariant broken: " + what;
+    return RLS_ERR_STATE;
+  };
+  const int64_t nblk = (n + SPT_ROWS - 1) / SPT_ROWS;
+  if (o.nblk != nblk || (int64_t)o.rowptr.size() != n + 1 || o.rowptr[0] != 0 ||
+      o.rowptr[(size_t)n] != (int64_t)o.col.size() || o.col.size() != o.val.size() ||
+      (int64_t)o.blk.size() != nblk * SPT_ROWS * SPT_ROWS || (int64_t)o.dinv.size() != n)
+    return fail("sizes");
+  for (int64_t i = 0; i < n; ++i) {
+    if (o.rowptr[(size_t)i + 1] < o.rowptr[(size_t)i]) return fail("row pointers");
+    for (int64_t e = o.rowptr[(size_t)i]; e < o.rowptr[(size_t)i + 1]; ++e) {
+      const int64_t j = o.col[(size_t)e];
+      if (j < 0 || j >= n) return fail("column range");
+      if (op == 0 ? (j / SPT_ROWS >= i / SPT_ROWS) : (j / SPT_ROWS <= i / SPT_ROWS)) return fail("block order");
+      if (e > o.rowptr[(size_t)i] && (op == 0 ? j < o.col[(size_t)e - 1] : j > o.col[(size_t)e - 1]))
+        return fail("entry order");
+    }
+  }
+  for (int64_t b = 0; b < nblk; ++b)
+    for (int s = 0; s < SPT_ROWS; ++s)
+      for (int r = 0; r < SPT_ROWS; ++r) {
+        const cplx v = o.blk[(size_t)((b * SPT_ROWS + s) * SPT_ROWS + r)];
+        if (v.x == 0.0 && v.y == 0.0) continue;
+        if (b * SPT_ROWS + r >= n || b * SPT_ROWS + s >= n || (op == 0 ? s >= r : s <= r)) return fail("block terms");
+      }
+  for (int64_t q = 0; q < n * n; ++q) dense[q] = rls_c64{0.0, 0.0};
+  auto add = [&](int64_t row, int64_t x, cplx v) {
+    dense[x * n + row].re += v.x;
+    dense[x * n + row].im += v.y;
+  };
+  for (int64_t i = 0; i < n; ++i) {
+    const cplx d = o.dinv[(size_t)i];
+    if (d.x != 0.0 || d.y != 0.0) add(i, i, cinv(d));
+    for (int64_t e = o.rowptr[(size_t)i]; e < o.rowptr[(size_t)i + 1]; ++e) add(i, o.col[(size_t)e], o.val[(size_t)e]);
+  }
+  for (int64_t b = 0; b < nblk; ++b)
+    for (int s = 0; s < SPT_ROWS; ++s)
+      for (int r = 0; r < SPT_ROWS; ++r) {
+        const cplx v = o.blk[(size_t)((b * SPT_ROWS + s) * SPT_ROWS + r)];
+        if (v.x != 0.0 || v.y != 0.0) add(b * SPT_ROWS + r, b * SPT_ROWS + s, v);
+      }
+  if (singular_at) *singular_at = sing;
+  if (levels) *levels = o.levels;
+  return RLS_OK;
+}
+
 extern "C" int rls_test_setup(rls_ctx* ctx, int r, int p_max) {
   if (!ctx || !ctx->T) return RLS_ERR_STATE;
   if (r < 1 || r > 8 || p_max < 1) return RLS_ERR_ARG;

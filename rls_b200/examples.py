@@ -75,3 +75,28 @@ def skewlap3d(N: int = 25) -> sp.csc_matrix:
 
 SKEWLAP_NORMC = 7471.59                                # skewlap3d.jl:41
 SKEWLAP_GRID = dict(x_st=-550.0, x_ed=100.0, y_st=-200.0, y_ed=200.0, n_x=200, n_y=200, k=20)
+
+
+def ic_factor_banded(n: int, band: int, fill: float, seed: int, complex_values: bool = True) -> sp.csc_matrix:
+    """Synthetic stand-in for the threshold IC factor L that psPrecRecy builds
+    (get_hsl_LLTP, src/preconditioner/hsl_preconditioner.jl:159-252): sparse lower triangular,
+    each row keeping a random `fill` fraction of the `band` columns to its left (values
+    N(0, 1)/band, complex unless complex_values is False) and a diagonal of 1 + the row's
+    absolute sum, so that it is well conditioned.  n = 23,560, band = 300, fill = 2/3 gives
+    the af23560-shaped factor (≈200 nonzeros per row, 4.7·10⁶ in all).  Returns CSC."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for i in range(n):
+        lo = max(0, i - band)
+        cand = np.arange(lo, i)
+        keep = cand[rng.random(cand.size) < fill]
+        rows.append(np.full(keep.size, i))
+        cols.append(keep)
+    r = np.concatenate(rows) if rows else np.zeros(0, int)
+    c = np.concatenate(cols) if cols else np.zeros(0, int)
+    v = rng.standard_normal(r.size) / max(band, 1)
+    if complex_values:
+        v = v + 1j * rng.standard_normal(r.size) / max(band, 1)
+    off = sp.csr_matrix((v, (r, c)), shape=(n, n), dtype=np.complex128)
+    diag = 1.0 + np.asarray(abs(off).sum(axis=1)).ravel()
+    return (off + sp.diags(diag.astype(np.complex128))).tocsc()

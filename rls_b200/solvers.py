@@ -358,6 +358,47 @@ class ShiftedMat:
         return ShiftedMat(None, np.conj(self.s), self.engine, adj=not self.adj, _uploaded=True)
 
 
+class SparseLLTP:
+    """SparseLLTP (src/preconditioner/RLSPreconditioner.jl:8-26) on the device: the IC factor
+    L (sparse; only its lower triangle is used), the permutation p and its stored inverse
+    invp (0-based here; the C ABI also takes Julia's 1-based vectors).  ``ldiv(B)`` is
+    ldiv!(X, K, B) = P·L⁻ᴴ·L⁻¹·Pᴴ·B (:79-116); ``ldiv(B, out=B)`` is ldiv!(K, B)."""
+
+    def __init__(self, L, p, invp, engine: "Engine" = None):
+        import scipy.sparse as sp
+        self.engine = engine or Engine(0)
+        A = sp.csc_matrix(L, dtype=np.complex128)
+        A.sort_indices()
+        n = A.shape[0]
+        if A.shape != (n, n):
+            raise DimensionMismatch(-2, f"SparseLLTP needs a square factor, got {A.shape}")
+        p = np.ascontiguousarray(p, dtype=np.int64)
+        invp = np.ascontiguousarray(invp, dtype=np.int64)
+        if p.shape != (n,) or invp.shape != (n,):
+            raise DimensionMismatch(-2, f"permutation lengths {p.shape}, {invp.shape} for n = {n}")
+        colptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        rowval = np.ascontiguousarray(A.indices, dtype=np.int64)
+        nzval = np.ascontiguousarray(A.data, dtype=np.complex128)
+        check(lib().rls_lltp_upload(self.engine._h, n, ptr(colptr), ptr(rowval), ptr(nzval), ptr(p), ptr(invp), 0),
+              self.engine._h)
+        self.shape = (n, n)
+
+    def ldiv(self, B, out=None):
+        B = np.asarray(B)
+        vec = B.ndim == 1
+        Bf = np.asfortranarray(B.reshape(B.shape[0], -1), dtype=np.complex128)
+        n, b = Bf.shape
+        if n != self.shape[0]:
+            raise DimensionMismatch(-2, f"B has {n} rows, the factor {self.shape[0]}")
+        X = np.empty((n, b), dtype=np.complex128, order="F")
+        check(lib().rls_lltp_ldiv(self.engine._h, b, ptr(Bf), n, ptr(X), n), self.engine._h)
+        res = X[:, 0] if vec else X
+        if out is not None:
+            out[...] = res
+            return out
+        return res
+
+
 class Lanes:
     """Concurrent grid lanes on one GPU (rls_pstrirecy_schur_lanes_range): one Engine per
     lane, each with the Schur factor uploaded; the traversal is split into near-equal parts
