@@ -18,7 +18,7 @@ extern "C" {
  * L (op = 0) or Lᴴ (op = 1), checked for what the device solve relies on (every off-block
  * term reads a block row solved before its own, indices in range, in-block terms strictly
  * on the solved side of the diagonal) and written out as the dense n × n operator it
- * stands for (n ≤ 4096, column-major).  singular_at receives the first 1-based index with
+ * stands for (n ≤ 4096, column-major; dense = NULL checks only, any n).  singular_at receives the first 1-based index with
  * a zero diagonal (0 if none), levels the longest chain of dependent block rows.  Compare
  * tril(L) or its adjoint. */
 int rls_test_lltp_plan_dense(int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval,

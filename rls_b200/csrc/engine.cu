@@ -164,7 +164,7 @@ struct rls_ctx {
     int64_t* invp = nullptr;
     cplx* w1 = nullptr;          // n × 8: L⁻¹·Pᴴ·B (one chunk of columns)
     cplx* w2 = nullptr;          // n × 8: Lᴴ⁻¹ of it
-    int* flags = nullptr;        // 2·nblk: published block rows, [0, nblk) for L, [nblk, 2·nblk) for Lᴴ
+    int* flags = nullptr;        // 2·nblk flags, SPT_FLAG_STRIDE ints apart: L's block rows, then Lᴴ's
     int* ticket = nullptr;       // 2
     int epoch = 0;
     int64_t singular_at = 0;     // first 1-based index with a zero diagonal, 0 if none
@@ -2051,6 +2051,8 @@ struct TriHost {
   std::vector<int64_t> rowptr;
   std::vector<int32_t> col;
   std::vector<cplx> val, blk, dinv;
+  std::vector<int64_t> depptr, segend;   // see TriBlocks
+  std::vector<int32_t> deps;
   int levels = 0;   // longest chain of block rows (a block row with no off-block term is level 1)
 };
 
@@ -2132,6 +2134,36 @@ int64_t lltp_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const
     op[0].dinv[(size_t)i] = cinv(d);
     op[1].dinv[(size_t)i] = cinv(cconj(d));
   }
+  // per block row: the block rows it reads, in the order they finish (the order of each row's
+  // terms), and where each row's terms from each of them end
+  for (int t = 0; t < 2; ++t) {
+    TriHost& o = op[t];
+    o.depptr.assign((size_t)nblk + 1, 0);
+    o.deps.clear();
+    o.segend.clear();
+    for (int64_t b = 0; b < nblk; ++b) {
+      const int64_t i0 = b * SPT_ROWS, i1 = std::min(n, (b + 1) * SPT_ROWS);
+      std::vector<int32_t> ds;
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t e = o.rowptr[(size_t)i]; e < o.rowptr[(size_t)i + 1]; ++e)
+          ds.push_back(o.col[(size_t)e] / SPT_ROWS);
+      std::sort(ds.begin(), ds.end());
+      ds.erase(std::unique(ds.begin(), ds.end()), ds.end());
+      if (t == 1) std::reverse(ds.begin(), ds.end());
+      const size_t k0 = o.deps.size();
+      o.deps.insert(o.deps.end(), ds.begin(), ds.end());
+      o.depptr[(size_t)b + 1] = (int64_t)o.deps.size();
+      o.segend.resize(o.deps.size() * SPT_ROWS, 0);
+      for (int64_t i = i0; i < i1; ++i) {
+        int64_t e = o.rowptr[(size_t)i];
+        const int64_t ez = o.rowptr[(size_t)i + 1];
+        for (size_t k = k0; k < o.deps.size(); ++k) {
+          while (e < ez && o.col[(size_t)e] / SPT_ROWS == o.deps[k]) ++e;
+          o.segend[k * SPT_ROWS + (size_t)(i - i0)] = e;
+        }
+      }
+    }
+  }
   // chain lengths in block rows
   for (int t = 0; t < 2; ++t) {
     std::vector<int> lev((size_t)nblk, 1);
@@ -2192,7 +2224,7 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
     return RLS_ERR_SINGULAR;
   }
   const int64_t nblk = F.op[0].nblk;
-  const unsigned grid = (unsigned)std::min<int64_t>((nblk + 3) / 4, 148 * 4);
+  const unsigned grid = (unsigned)std::min<int64_t>((nblk + SPT_WARPS - 1) / SPT_WARPS, 148 * 16);
   const unsigned gg = (unsigned)((F.n + 255) / 256);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ctx->profile) {
@@ -2205,17 +2237,17 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
     F.epoch += 1;
     if (F.epoch > (1 << 30)) {
       F.epoch = 1;
-      CK(cudaMemsetAsync(F.flags, 0, sizeof(int) * 2 * nblk, ctx->stream));
+      CK(cudaMemsetAsync(F.flags, 0, sizeof(int) * 2 * nblk * SPT_FLAG_STRIDE, ctx->stream));
     }
     CK(cudaMemsetAsync(F.ticket, 0, 2 * sizeof(int), ctx->stream));
     const cplx* Bc = B + (int64_t)c0 * ldb;
     cplx* Xc = X + (int64_t)c0 * ldx;
 #define RLS_SPT_CASE(K)                                                                                            \
   case K:                                                                                                          \
-    k_sptrsv_blocks<K, false><<<grid, 128, 0, ctx->stream>>>(F.op[0], Bc, ldb, F.p, F.w1, F.n, F.ticket, F.flags,   \
-                                                             F.epoch, ctx->derr);                                  \
-    k_sptrsv_blocks<K, true><<<grid, 128, 0, ctx->stream>>>(F.op[1], F.w1, F.n, nullptr, F.w2, F.n, F.ticket + 1,   \
-                                                            F.flags + nblk, F.epoch, ctx->derr);                   \
+    k_sptrsv_blocks<K, false><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(F.op[0], Bc, ldb, F.p, F.w1, F.n,          \
+                                                                        F.ticket, F.flags, F.epoch, ctx->derr);   \
+    k_sptrsv_blocks<K, true><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(                                           \
+        F.op[1], F.w1, F.n, nullptr, F.w2, F.n, F.ticket + 1, F.flags + nblk * SPT_FLAG_STRIDE, F.epoch, ctx->derr); \
     k_gather_rows<K><<<gg, 256, 0, ctx->stream>>>(F.n, F.invp, F.w2, F.n, Xc, ldx);                                \
     break;
     switch (kk) {
@@ -2236,7 +2268,8 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
     double ops = 0.0;
     for (const auto& o : F.op)
       ops += (double)o.nnz_off * (sizeof(cplx) + sizeof(int32_t)) + (double)(o.n + 1) * sizeof(int64_t) +
-             (double)o.nblk * SPT_ROWS * SPT_ROWS * sizeof(cplx) + (double)o.n * sizeof(cplx);
+             (double)o.nblk * SPT_ROWS * SPT_ROWS * sizeof(cplx) + (double)o.n * sizeof(cplx) +
+             (double)o.ndeps * (sizeof(int32_t) + SPT_ROWS * sizeof(int64_t));
     k.pending_bytes.push_back((double)((b + 7) / 8) * ops + 6.0 * (double)b * (double)F.n * sizeof(cplx));
   }
   return RLS_OK;
@@ -2267,7 +2300,9 @@ extern "C" int rls_lltp_upload(rls_ctx* ctx, int64_t n, const int64_t* colptr, c
   CK(cudaStreamSynchronize(ctx->stream));
   auto& F = ctx->lltp;
   for (auto& o : F.op) {
-    for (void* q : {(void*)o.rowptr, (void*)o.col, (void*)o.val, (void*)o.blk, (void*)o.dinv}) dfree(ctx, q);
+    for (void* q : {(void*)o.rowptr, (void*)o.col, (void*)o.val, (void*)o.blk, (void*)o.dinv, (void*)o.depptr,
+                    (void*)o.deps, (void*)o.segend})
+      dfree(ctx, q);
     o = TriBlocks{};
   }
   for (void* q : {(void*)F.p, (void*)F.invp, (void*)F.w1, (void*)F.w2, (void*)F.flags, (void*)F.ticket})
@@ -2296,12 +2331,23 @@ extern "C" int rls_lltp_upload(rls_ctx* ctx, int64_t n, const int64_t* colptr, c
     }
     CK(cudaMemcpyAsync(o.blk, h[t].blk.data(), sizeof(cplx) * h[t].blk.size(), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(o.dinv, h[t].dinv.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, ctx->stream));
+    o.ndeps = (int64_t)h[t].deps.size();
+    RET(dalloc_t(ctx, &o.depptr, (size_t)nblk + 1));
+    RET(dalloc_t(ctx, &o.deps, (size_t)std::max<int64_t>(o.ndeps, 1)));
+    RET(dalloc_t(ctx, &o.segend, (size_t)std::max<int64_t>(o.ndeps, 1) * SPT_ROWS));
+    CK(cudaMemcpyAsync(o.depptr, h[t].depptr.data(), sizeof(int64_t) * (nblk + 1), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    if (o.ndeps > 0) {
+      CK(cudaMemcpyAsync(o.deps, h[t].deps.data(), sizeof(int32_t) * o.ndeps, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(o.segend, h[t].segend.data(), sizeof(int64_t) * o.ndeps * SPT_ROWS, cudaMemcpyHostToDevice,
+                         ctx->stream));
+    }
   }
   RET(dalloc_t(ctx, &F.p, (size_t)n));
   RET(dalloc_t(ctx, &F.invp, (size_t)n));
   RET(dalloc_t(ctx, &F.w1, (size_t)n * 8));
   RET(dalloc_t(ctx, &F.w2, (size_t)n * 8));
-  RET(dalloc_t(ctx, &F.flags, (size_t)2 * nblk));
+  RET(dalloc_t(ctx, &F.flags, (size_t)2 * nblk * SPT_FLAG_STRIDE));
   RET(dalloc_t(ctx, &F.ticket, 2));
   CK(cudaMemcpyAsync(F.p, p0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(F.invp, ip0.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));

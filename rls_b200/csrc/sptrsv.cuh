@@ -8,19 +8,25 @@
 // only waits on block rows whose warps started before it: every wait ends even when not
 // all warps are resident, and a block row starts as soon as the block rows it reads are
 // published (dataflow; the level-set parallelism of a level schedule without a barrier
-// per level).  A lane first sums its row's off-block terms, waiting on each producing
-// block row's flag (entries ordered so the nearest block rows come last), then the warp
-// solves the 32 × 32 diagonal block in 32 shuffle steps with the multipliers in registers.
-// For the banded IC factors of psPrecRecy, whose row i almost always reads row i − 1, the
-// critical path is n/32 block hand-offs instead of n row hand-offs.
+// per level).  The plan lists, per block row, the block rows it reads in the order they
+// finish, and per row where its terms from each of them end: the warp waits on each in
+// turn (one lane polls the block row's flag, alone on its 128-byte line, with a capped
+// exponential back-off), then every lane streams its terms from that block row four at a
+// time with independent loads.  The warp then solves the 32 × 32 diagonal block in 32
+// shuffle steps, multipliers in shared memory.  For the banded IC factors of psPrecRecy,
+// whose row i almost always reads row i − 1, the critical path is n/32 block hand-offs,
+// each carrying only the terms of the block row just finished.
 //
-// Flags carry an epoch (st.release / ld.acquire at gpu scope); every wait is bounded by
-// RLS_SPIN_LIMIT polls, after which the lane records DEVERR_SPIN_TIMEOUT and carries on,
-// so a launch always terminates.
+// Flags carry an epoch (st.release / ld.acquire at gpu scope; the polling lane's acquire
+// reaches the other lanes through __syncwarp); every wait is bounded by RLS_SPIN_LIMIT
+// polls, after which the warp records DEVERR_SPIN_TIMEOUT and carries on, so a launch
+// always terminates.
 #pragma once
 #include "common.cuh"
 
-constexpr int SPT_ROWS = 32;   // rows per block row (one warp)
+constexpr int SPT_ROWS = 32;          // rows per block row (one warp)
+constexpr int SPT_FLAG_STRIDE = 32;   // ints between two block rows' flags (128 bytes)
+constexpr int SPT_WARPS = 2;          // warps per CTA
 
 // One triangular operator in block-row form (rows of L, or rows of Lᴴ).
 struct TriBlocks {
@@ -32,6 +38,10 @@ struct TriBlocks {
   cplx* val = nullptr;          // nnz_off: its coefficient
   cplx* blk = nullptr;          // nblk·32·32: blk[(b·32 + s)·32 + r] = coefficient of x[32b+s] in row 32b+r
   cplx* dinv = nullptr;         // n: 1 / diagonal
+  int64_t ndeps = 0;
+  int64_t* depptr = nullptr;    // nblk + 1: block row b reads deps[depptr[b] .. depptr[b+1])
+  int32_t* deps = nullptr;      // ndeps: those block rows, in the order they finish
+  int64_t* segend = nullptr;    // ndeps·32: segend[k·32 + r] = end of row 32b+r's terms from deps[k]
 };
 
 __device__ __forceinline__ int spt_ld_acquire(const int* p) {
@@ -45,12 +55,16 @@ __device__ __forceinline__ void spt_st_release(int* p, int v) {
 
 // out[:, 0:K] = A⁻¹ · rhs[gather, 0:K]  (gather = nullptr: identity).  BACK: block rows and the
 // in-block sweep run from the last row to the first (the operator is upper triangular).
-// 128 threads per CTA (4 warps), any grid.  out must not alias rhs.
+// SPT_WARPS warps per CTA, any grid.  out must not alias rhs.  flags: one per block row,
+// SPT_FLAG_STRIDE ints apart.
 template <int K, bool BACK>
-__global__ void __launch_bounds__(128) k_sptrsv_blocks(TriBlocks A, const cplx* __restrict__ rhs, int64_t ldr,
-                                                       const int64_t* __restrict__ gather, cplx* out, int64_t ldo,
-                                                       int* ticket, int* flags, int epoch, int* err) {
+__global__ void __launch_bounds__(32 * SPT_WARPS) k_sptrsv_blocks(TriBlocks A, const cplx* __restrict__ rhs,
+                                                                  int64_t ldr, const int64_t* __restrict__ gather,
+                                                                  cplx* out, int64_t ldo, int* ticket, int* flags,
+                                                                  int epoch, int* err) {
+  __shared__ cplx sm_m[SPT_WARPS][SPT_ROWS * SPT_ROWS];   // each lane's own row of multipliers
   const int lane = threadIdx.x & 31;
+  cplx* mw = sm_m[threadIdx.x >> 5];
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(ticket, 1);
@@ -59,34 +73,58 @@ __global__ void __launch_bounds__(128) k_sptrsv_blocks(TriBlocks A, const cplx* 
     const int64_t b = BACK ? (A.nblk - 1 - t) : t;
     const int64_t i = b * SPT_ROWS + lane;
     const bool live = i < A.n;
-    // this row's in-block multipliers, in flight while the off-block terms are gathered
-    cplx m[SPT_ROWS];
     const cplx* mb = A.blk + b * (SPT_ROWS * SPT_ROWS);
-#pragma unroll
-    for (int s = 0; s < SPT_ROWS; ++s) m[s] = mb[s * SPT_ROWS + lane];
+#pragma unroll 8
+    for (int s = 0; s < SPT_ROWS; ++s) mw[s * SPT_ROWS + lane] = mb[s * SPT_ROWS + lane];
     cplx acc[K], r[K];
     cplx d = czero();
 #pragma unroll
     for (int c = 0; c < K; ++c) { acc[c] = czero(); r[c] = czero(); }
+    int64_t e = 0;
     if (live) {
       d = A.dinv[i];
       const int64_t src = gather ? gather[i] : i;
 #pragma unroll
       for (int c = 0; c < K; ++c) r[c] = rhs[(int64_t)c * ldr + src];
-      const int64_t e1 = A.rowptr[i + 1];
-      int64_t waited = -1;
-      for (int64_t e = A.rowptr[i]; e < e1; ++e) {
+      e = A.rowptr[i];
+    }
+    const int64_t k1 = A.depptr[b + 1];
+    for (int64_t k = A.depptr[b]; k < k1; ++k) {
+      if (lane == 0) {
+        const int* f = &flags[(int64_t)A.deps[k] * SPT_FLAG_STRIDE];
+        int spins = 0;
+        unsigned ns = 32;
+        while (spt_ld_acquire(f) != epoch) {
+          if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
+          if (spins > 16) {
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+          }
+        }
+      }
+      __syncwarp();
+      const int64_t eend = live ? A.segend[k * SPT_ROWS + lane] : 0;
+      for (; e + 4 <= eend; e += 4) {
+        int64_t j[4];
+        cplx v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          j[u] = A.col[e + u];
+          v[u] = A.val[e + u];
+        }
+        cplx xv[4][K];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < K; ++c) xv[u][c] = __ldcg(&out[(int64_t)c * ldo + j[u]]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < K; ++c) acc[c] = cfma(v[u], xv[u][c], acc[c]);
+      }
+      for (; e < eend; ++e) {
         const int64_t j = A.col[e];
         const cplx v = A.val[e];
-        const int64_t jb = j / SPT_ROWS;
-        if (jb != waited) {
-          int spins = 0;
-          while (spt_ld_acquire(&flags[jb]) != epoch) {
-            if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
-            if (spins > 64) __nanosleep(64);
-          }
-          waited = jb;
-        }
 #pragma unroll
         for (int c = 0; c < K; ++c) acc[c] = cfma(v, __ldcg(&out[(int64_t)c * ldo + j]), acc[c]);
       }
@@ -95,9 +133,10 @@ __global__ void __launch_bounds__(128) k_sptrsv_blocks(TriBlocks A, const cplx* 
     cplx x[K];
 #pragma unroll
     for (int c = 0; c < K; ++c) x[c] = czero();
-#pragma unroll
+#pragma unroll 4
     for (int q = 0; q < SPT_ROWS; ++q) {
       const int s = BACK ? (SPT_ROWS - 1 - q) : q;
+      const cplx ms = mw[s * SPT_ROWS + lane];
 #pragma unroll
       for (int c = 0; c < K; ++c) {
         const cplx mine = cmul(csub(r[c], acc[c]), d);
@@ -105,7 +144,7 @@ __global__ void __launch_bounds__(128) k_sptrsv_blocks(TriBlocks A, const cplx* 
         xs.x = __shfl_sync(0xffffffffu, mine.x, s);
         xs.y = __shfl_sync(0xffffffffu, mine.y, s);
         if (lane == s) x[c] = xs;
-        acc[c] = cfma(m[s], xs, acc[c]);
+        acc[c] = cfma(ms, xs, acc[c]);
       }
     }
     if (live) {
@@ -114,7 +153,7 @@ __global__ void __launch_bounds__(128) k_sptrsv_blocks(TriBlocks A, const cplx* 
     }
     __threadfence();
     __syncwarp();
-    if (lane == 0) spt_st_release(&flags[b], epoch);
+    if (lane == 0) spt_st_release(&flags[b * SPT_FLAG_STRIDE], epoch);
   }
 }
 

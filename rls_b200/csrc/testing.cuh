@@ -44,7 +44,7 @@ extern "C" int rls_test_lltp_plan_dense(int64_t n, const int64_t* colptr, const 
     g_create_err = "rls_test_lltp_plan_dense: " + why;
     return st;
   }
-  if ((op != 0 && op != 1) || n > 4096 || !dense) {
+  if ((op != 0 && op != 1) || (dense && n > 4096)) {
     g_create_err = "rls_test_lltp_plan_dense: invalid arguments";
     return RLS_ERR_ARG;
   }
@@ -77,6 +77,38 @@ extern "C" int rls_test_lltp_plan_dense(int64_t n, const int64_t* colptr, const 
         if (v.x == 0.0 && v.y == 0.0) continue;
         if (b * SPT_ROWS + r >= n || b * SPT_ROWS + s >= n || (op == 0 ? s >= r : s <= r)) return fail("block terms");
       }
+  // dependency lists and segments: every row's terms are covered, segment by segment, and
+  // each segment holds exactly the terms from its block row
+  if ((int64_t)o.depptr.size() != nblk + 1 || o.depptr[0] != 0 || o.depptr[(size_t)nblk] != (int64_t)o.deps.size() ||
+      o.segend.size() != o.deps.size() * SPT_ROWS)
+    return fail("dependency list sizes");
+  for (int64_t b = 0; b < nblk; ++b) {
+    const int64_t k0 = o.depptr[(size_t)b], k1 = o.depptr[(size_t)b + 1];
+    if (k1 < k0) return fail("dependency pointers");
+    for (int64_t k = k0; k < k1; ++k) {
+      const int64_t d = o.deps[(size_t)k];
+      if (d < 0 || d >= nblk || (op == 0 ? d >= b : d <= b)) return fail("dependency block order");
+      if (k > k0 && (op == 0 ? d <= o.deps[(size_t)k - 1] : d >= o.deps[(size_t)k - 1])) return fail("dependency order");
+    }
+    for (int r = 0; r < SPT_ROWS; ++r) {
+      const int64_t i = b * SPT_ROWS + r;
+      int64_t e = i < n ? o.rowptr[(size_t)i] : 0;
+      for (int64_t k = k0; k < k1; ++k) {
+        const int64_t z = o.segend[(size_t)(k * SPT_ROWS + r)];
+        if (i >= n) {
+          if (z != 0) return fail("segments of padding rows");
+          continue;
+        }
+        if (z < e || z > o.rowptr[(size_t)i + 1]) return fail("segment ends");
+        for (; e < z; ++e)
+          if (o.col[(size_t)e] / SPT_ROWS != o.deps[(size_t)k]) return fail("segment contents");
+      }
+      if (i < n && e != o.rowptr[(size_t)i + 1]) return fail("uncovered terms");
+    }
+  }
+  if (singular_at) *singular_at = sing;
+  if (levels) *levels = o.levels;
+  if (!dense) return RLS_OK;
   for (int64_t q = 0; q < n * n; ++q) dense[q] = rls_c64{0.0, 0.0};
   auto add = [&](int64_t row, int64_t x, cplx v) {
     dense[x * n + row].re += v.x;

@@ -110,3 +110,16 @@ def test_plan_rejects_bad_indices():
     D = np.zeros((2, 2), dtype=np.complex128)
     with pytest.raises(DimensionMismatch):
         check(lib().rls_test_lltp_plan_dense(2, ptr(colptr), ptr(rowval), ptr(nzval), 0, 0, ptr(D), None, None), None)
+
+
+def test_plan_invariants_on_the_af23560_shaped_factor():
+    """The full-size factor of the benchmark (n = 23,560, 4.7·10⁶ nonzeros): plan checks only."""
+    from rls_b200.examples import ic_factor_banded
+    L = ic_factor_banded(23560, 300, 2.0 / 3.0, seed=20260318, complex_values=False)
+    colptr, rowval, nzval = _csc_arrays(L)
+    for op in (0, 1):
+        sing = C.c_int64()
+        lev = C.c_int()
+        check(lib().rls_test_lltp_plan_dense(23560, ptr(colptr), ptr(rowval), ptr(nzval), 0, op, None,
+                                             C.byref(sing), C.byref(lev)), None)
+        assert sing.value == 0 and lev.value == -(-23560 // 32)      # one chain through every block row
