@@ -288,6 +288,22 @@ int rls_lltp_upload(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_
  * entry of L gives RLS_ERR_SINGULAR, naming the first such index j as the reference's
  * SingularException(j) does. */
 int rls_lltp_ldiv(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx);
+
+/* get_hsl_LLTP(C, z, tau1, tau2, α, lsize, rsize, p) (hsl_preconditioner.jl:159-252) on the
+ * host, no context: the threshold incomplete-Cholesky factor of the permuted, L2-scaled
+ * lower((C − zI)ᴴ(C − zI)) that psPrecRecy builds at start-up and on every rebuild.  C is
+ * n × n in the reference's CSC layout (rows strictly increasing in each column), p a
+ * permutation; indices base 0 or 1, outputs in the same base.  Writes L (lcolptr n+1,
+ * lrowval and lnzval of capacity cap ≥ n·(1 + min(lsize, n−1)); NULL lrowval / lnzval skip
+ * the entries) and invp, and the diagonal shift α the factorisation succeeded with
+ * (shift_used, may be NULL).  L, p, invp are the fields of the SparseLLTP to pass to
+ * rls_lltp_upload.  Only the control get_hsl_LLTP sets is supported (L2 scaling, no
+ * R·Rᴴ term); lsize < 1 (n > 1) is an ArgumentError, as the reference cannot run it.
+ * The shift grows by 2× per breakdown, as the reference's, for at most 200 retries. */
+int rls_ic_factor(int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval, int base,
+                  rls_c64 z, double tau1, double tau2, double alpha, int64_t lsize, int64_t rsize,
+                  const int64_t* p, int64_t cap, int64_t* lcolptr, int64_t* lrowval, rls_c64* lnzval,
+                  int64_t* invp, double* shift_used);
 int rls_lltp_ldiv_dev(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx);
 
 /* ---- gradient -------------------------------------------------------------------- */

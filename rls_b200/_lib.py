@@ -80,6 +80,8 @@ SIGNATURES = {
     "rls_lltp_upload": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.c_int]),
     "rls_lltp_ldiv": (C.c_int, [P, C.c_int, P, C.c_int64, P, C.c_int64]),
     "rls_lltp_ldiv_dev": (C.c_int, [P, C.c_int, P, C.c_int64, P, C.c_int64]),
+    "rls_ic_factor": (C.c_int, [C.c_int64, P, P, P, C.c_int, c64, C.c_double, C.c_double, C.c_double, C.c_int64,
+                                C.c_int64, P, C.c_int64, P, P, P, P, P]),
     "rls_lane_offsets": (C.c_int, [C.POINTER(rls_grid), C.c_int64, C.c_int, P]),
     "rls_pstrirecy_schur_lanes": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
                                             C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),

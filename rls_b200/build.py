@@ -2,7 +2,8 @@
 
     python -m rls_b200.build [--force]
 
-The grid code is compiled by g++ with -ffp-contract=off (bit-exact coordinates);
+The grid code and the IC factorisation are compiled by g++ with -ffp-contract=off
+(bit-exact coordinates and factors);
 the CUDA translation unit by nvcc for sm_100a only.
 """
 from __future__ import annotations
@@ -47,15 +48,17 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     grid_o = os.path.join(BUILD, "grid.o")
     eng_o = os.path.join(BUILD, "engine.o")
-    _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-c",
-          os.path.join(CSRC, "grid.cpp"), "-o", grid_o])
+    ic_o = os.path.join(BUILD, "icfact.o")
+    for src, obj in (("grid.cpp", grid_o), ("icfact.cpp", ic_o)):
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-c",
+              os.path.join(CSRC, src), "-o", obj])
     cmd = [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-c",
            os.path.join(CSRC, "engine.cu"), "-o", eng_o]
     if verbose_ptxas:
         cmd[1:1] = ["-Xptxas", "-v"]
     _run(cmd)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, "-lcudart"])
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, ic_o, "-lcudart"])
     os.replace(tmp, LIB)
     return LIB
 

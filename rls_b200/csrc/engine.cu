@@ -25,6 +25,7 @@
 #include "small.cuh"
 #include "sparse.cuh"
 #include "sptrsv.cuh"
+#include "host_err.h"
 
 namespace {
 
@@ -1317,6 +1318,8 @@ extern "C" const char* rls_status_string(int s) {
 }
 
 static thread_local std::string g_create_err;
+
+void rls_host_error(const std::string& msg) { g_create_err = msg; }
 
 extern "C" int rls_ctx_create(rls_ctx** out, int device) {
   if (!out) return RLS_ERR_ARG;

@@ -358,6 +358,47 @@ class ShiftedMat:
         return ShiftedMat(None, np.conj(self.s), self.engine, adj=not self.adj, _uploaded=True)
 
 
+def ic_factor(Cm, z, tau1, tau2, alpha, lsize, rsize, p):
+    """get_hsl_LLTP's factorisation on the host (rls_ic_factor; hsl_preconditioner.jl:159-252):
+    returns (L as a SciPy CSC matrix, invp, the diagonal shift used), 0-based p and invp.  No
+    device is needed."""
+    import scipy.sparse as sp
+    A = sp.csc_matrix(Cm, dtype=np.complex128)
+    A.sum_duplicates()
+    A.sort_indices()
+    n = A.shape[0]
+    if A.shape != (n, n):
+        raise DimensionMismatch(-2, f"get_hsl_LLTP only supports square C, got size {A.shape}")
+    p = np.ascontiguousarray(p, dtype=np.int64)
+    if p.shape != (n,):
+        raise DimensionMismatch(-2, f"permutation length mismatch: length(p)={p.size} n={n}")
+    colptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+    rowval = np.ascontiguousarray(A.indices, dtype=np.int64)
+    nzval = np.ascontiguousarray(A.data, dtype=np.complex128)
+    lsz = min(max(0, int(lsize)), n - 1)
+    cap = n + lsz * n
+    lcolptr = np.zeros(n + 1, dtype=np.int64)
+    lrow = np.zeros(max(cap, 1), dtype=np.int64)
+    lval = np.zeros(max(cap, 1), dtype=np.complex128)
+    invp = np.zeros(n, dtype=np.int64)
+    shift = C.c_double()
+    z = complex(z)
+    check(lib().rls_ic_factor(n, ptr(colptr), ptr(rowval), ptr(nzval), 0, c64(z.real, z.imag), float(tau1),
+                              float(tau2), float(alpha), int(lsize), int(rsize), ptr(p), cap, ptr(lcolptr),
+                              ptr(lrow), ptr(lval), ptr(invp), C.byref(shift)), None)
+    nl = int(lcolptr[n])
+    L = sp.csc_matrix((lval[:nl], lrow[:nl], lcolptr), shape=(n, n))
+    return L, invp, shift.value
+
+
+def get_hsl_LLTP(Cm, z, tau1, tau2, alpha, lsize, rsize, p, engine: "Engine" = None) -> "SparseLLTP":
+    """get_hsl_LLTP(C, z, tau1, tau2, α, lsize, rsize, p) (hsl_preconditioner.jl:159-252) with C
+    passed as Cm: the IC factor built on the host (ic_factor), uploaded to the device as a
+    SparseLLTP."""
+    L, invp, _ = ic_factor(Cm, z, tau1, tau2, alpha, lsize, rsize, p)
+    return SparseLLTP(L, p, invp, engine)
+
+
 class SparseLLTP:
     """SparseLLTP (src/preconditioner/RLSPreconditioner.jl:8-26) on the device: the IC factor
     L (sparse; only its lower triangle is used), the permutation p and its stored inverse
