@@ -84,7 +84,7 @@ def test_sparse_upload_rejects_bad_indices(cuda_device):
     nzval = np.ones(2, dtype=np.complex128)
     with pytest.raises(DimensionMismatch):
         check(lib().rls_sparse_upload_csc(e._h, 3, 2, ptr(colptr), ptr(rowval), ptr(nzval), 0), e._h)
+    X, Y = np.ones(2, dtype=np.complex128), np.ones(3, dtype=np.complex128)
     with pytest.raises(R.RLSError):
-        check(lib().rls_spmm_shifted(e._h, c64(0, 0), 0, 1, ptr(np.ones(2, dtype=np.complex128)), 2,
-                                     ptr(np.ones(3, dtype=np.complex128)), 3), e._h)
+        check(lib().rls_spmm_shifted(e._h, c64(0, 0), 0, 1, ptr(X), 2, ptr(Y), 3), e._h)
     e.close()

@@ -105,9 +105,9 @@ def _raw(Cm, p, base=0, lsize=3, rsize=2, cap=None, rows=None):
     cap = n + lsz * n if cap is None else cap
     out = (np.zeros(n + 1, dtype=np.int64), np.zeros(max(cap, 1), dtype=np.int64),
            np.zeros(max(cap, 1), dtype=np.complex128), np.zeros(n, dtype=np.int64))
+    pb = np.ascontiguousarray(p, dtype=np.int64) + base       # named: the library reads it
     st = lib().rls_ic_factor(n, ptr(colptr), ptr(rowval), ptr(nzval), base, c64(0.1, 0.0), 1e-3, 1e-4, 0.0, lsize,
-                             rsize, ptr(np.ascontiguousarray(p, dtype=np.int64) + base), cap, ptr(out[0]), ptr(out[1]),
-                             ptr(out[2]), ptr(out[3]), None)
+                             rsize, ptr(pb), cap, ptr(out[0]), ptr(out[1]), ptr(out[2]), ptr(out[3]), None)
     return st, out
 
 
@@ -145,3 +145,28 @@ def test_errors():
         check(_raw(Cm, p, rows=rows)[0], None)
     with pytest.raises(DimensionMismatch):
         R.ic_factor(sp.random(5, 6, density=0.5, format="csc"), 0.0, 1e-3, 1e-4, 0.0, 2, 1, np.arange(5))
+
+
+def test_small_and_clamped_sizes():
+    """n = 1; lsize beyond n − 1 (clamped as ichsd does) equals lsize = n − 1; the factor's
+    pattern alone (NULL entry outputs) comes back from the pointers."""
+    one = sp.csc_matrix(np.array([[2.0 + 1.0j]]))
+    L, invp, a = R.ic_factor(one, 0.5, 1e-3, 1e-4, 0.0, 5, 0, [0])
+    assert L.shape == (1, 1) and invp.tolist() == [0] and a == 0.0
+    assert np.isclose(L[0, 0], abs(2.0 + 1.0j - 0.5))
+    Cm = _case("random", 40, seed=5)
+    p = np.random.default_rng(5).permutation(40)
+    La = R.ic_factor(Cm, 0.1, 1e-3, 1e-4, 0.0, 39, 3, p)[0]
+    Lb = R.ic_factor(Cm, 0.1, 1e-3, 1e-4, 0.0, 500, 3, p)[0]
+    assert np.array_equal(La.indptr, Lb.indptr) and np.array_equal(La.data, Lb.data)
+    A = sp.csc_matrix(Cm, dtype=np.complex128)
+    A.sort_indices()
+    lp = np.zeros(41, dtype=np.int64)
+    ip = np.zeros(40, dtype=np.int64)
+    colptr = np.ascontiguousarray(A.indptr, dtype=np.int64)   # named: the library reads them
+    rowval = np.ascontiguousarray(A.indices, dtype=np.int64)
+    nzval = np.ascontiguousarray(A.data)
+    p64 = np.ascontiguousarray(p, dtype=np.int64)
+    check(lib().rls_ic_factor(40, ptr(colptr), ptr(rowval), ptr(nzval), 0, c64(0.1, 0.0), 1e-3, 1e-4, 0.0, 39, 3,
+                              ptr(p64), 40 * 40, ptr(lp), None, None, ptr(ip), None), None)
+    assert np.array_equal(lp, La.indptr)

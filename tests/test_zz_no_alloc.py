@@ -46,7 +46,8 @@ def qr_engine(cuda_device):
 def reference_r(e, A):
     m, k = A.shape
     R = np.zeros((k, k), dtype=np.complex128, order="F")
-    check(lib().rls_test_qr(e._h, m, k, ptr(np.asfortranarray(A)), ptr(R), None), e._h)
+    Af = np.asfortranarray(A)          # named, so that it outlives the call that reads it
+    check(lib().rls_test_qr(e._h, m, k, ptr(Af), ptr(R), None), e._h)
     return R
 
 
