@@ -18,10 +18,12 @@ from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_g
 from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
                       SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
+from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
     "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
-    "psTriRecy", "ic_factor", "get_hsl_LLTP", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException",
+    "psTriRecy", "ic_factor", "get_hsl_LLTP", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
+    "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException",
 ]

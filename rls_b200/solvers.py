@@ -424,6 +424,10 @@ class SparseLLTP:
               self.engine._h)
         self.shape = (n, n)
 
+    def adjoint(self) -> "SparseLLTP":
+        """P·L·Lᴴ·Pᴴ is Hermitian, and so is its inverse."""
+        return self
+
     def ldiv(self, B, out=None):
         B = np.asarray(B)
         vec = B.ndim == 1
