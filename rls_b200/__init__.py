@@ -16,14 +16,14 @@ from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_g
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
 from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
-                      SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP)
+                      SparseLLTP_AD, SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
-from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat
+from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
     "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
-    "psTriRecy", "ic_factor", "get_hsl_LLTP", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
+    "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
     "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException",
 ]

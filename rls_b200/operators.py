@@ -170,3 +170,14 @@ class _FilledAdjoint:
 
     def adjoint(self):
         return self.F
+
+
+def mul_coupled(M, S, V):
+    """(M·V, S·V) (mul_coupled_ms!, RLSPreconditioner.jl:38-76): when M = M₀·F and S = S₀·F are
+    two-factor chains sharing the same F object, F·V is formed once."""
+    V = np.asarray(V)
+    if (isinstance(M, MulChainMat) and isinstance(S, MulChainMat) and len(M.factors) == 2
+            and len(S.factors) == 2 and M.factors[1] is S.factors[1]):
+        FV = np.asarray(M.factors[1] @ V)
+        return np.asarray(M.factors[0] @ FV), np.asarray(S.factors[0] @ FV)
+    return np.asarray(M @ V), np.asarray(S @ V)

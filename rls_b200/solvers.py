@@ -444,6 +444,48 @@ class SparseLLTP:
         return res
 
 
+class SparseLLTP_AD:
+    """SparseLLTP_AD (RLSPreconditioner.jl:160-290), the two-level preconditioner of the pred
+    stage: ``ldiv(B)`` = K⁻¹B + E·(GramE⁻¹·(Eᴴ·B)), with K a SparseLLTP (its two sparse
+    triangular solves on the device) and E (n × ks) with the Cholesky factor of
+    GramE = (CE)ᴴ(CE) on the host (ks ≤ 40: two tall-skinny products and a ks × ks solve per
+    apply).  The factorisation is plain upper Cholesky, as rls_cholesky! (RLSLinearAlgebra.jl:15-21)
+    is; a GramE that is not positive definite raises numpy.linalg.LinAlgError."""
+
+    def __init__(self, K, E, GramE):
+        import scipy.linalg as sla
+        self.K = K
+        self.E = np.array(E, dtype=np.complex128, order="F")
+        self.GramE = np.array(GramE, dtype=np.complex128, order="F")
+        if self.E.shape[0] != K.shape[0] or self.GramE.shape != (self.E.shape[1], self.E.shape[1]):
+            raise DimensionMismatch(-2, f"SparseLLTP_AD: E {self.E.shape}, GramE {self.GramE.shape}, K {K.shape}")
+        self.F = sla.cho_factor(self.GramE, lower=False)
+        self.shape = K.shape
+
+    def update_basis(self, X, CX):
+        """update_sparse_lldiv_ad_basis! (:208-226): E = X, GramE = CXᴴ·CX, refactored."""
+        import scipy.linalg as sla
+        X = np.asarray(X)
+        CX = np.asarray(CX)
+        if X.shape != self.E.shape:
+            raise DimensionMismatch(-2, f"update_basis: X {X.shape}, E {self.E.shape}")
+        self.E[...] = X
+        self.GramE = np.asfortranarray(CX.conj().T @ CX)
+        self.F = sla.cho_factor(self.GramE, lower=False)
+
+    def ldiv(self, B):
+        import scipy.linalg as sla
+        B = np.asarray(B, dtype=np.complex128)
+        coeff = sla.cho_solve(self.F, self.E.conj().T @ B)
+        proj = self.E @ coeff
+        X = np.asarray(self.K.ldiv(B))
+        return X + proj
+
+    def adjoint(self) -> "SparseLLTP_AD":
+        """Both terms are Hermitian."""
+        return self
+
+
 class Lanes:
     """Concurrent grid lanes on one GPU (rls_pstrirecy_schur_lanes_range): one Engine per
     lane, each with the Schur factor uploaded; the traversal is split into near-equal parts

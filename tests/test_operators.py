@@ -85,3 +85,69 @@ def test_preconditioned_chain_of_the_pred_stage():
     D = Cz.toarray() @ Pd @ np.linalg.inv(L.toarray().conj().T)
     assert np.allclose(M @ X, D @ X)
     assert np.allclose(M.adjoint() @ X, D.conj().T @ X)
+
+
+class _HostK:
+    """A SparseLLTP stand-in whose solve is the CPU restatement (the device solve has its own
+    parity tests); only the composition around it is under test here."""
+
+    def __init__(self, L, p, invp):
+        self.L, self.p, self.invp = L, p, invp
+        self.shape = L.shape
+
+    def ldiv(self, B):
+        from oracle.precond import lltp_ldiv
+        return lltp_ldiv(self.L, self.p, self.invp, B)
+
+
+def test_two_level_preconditioner():
+    """SparseLLTP_AD: K⁻¹B + E·(GramE⁻¹·(Eᴴ·B)), and update_basis with GramE = (CX)ᴴ(CX)."""
+    from rls_b200.examples import ic_factor_banded
+    rng = np.random.default_rng(5)
+    n, ks = 80, 4
+    L = ic_factor_banded(n, 12, 0.5, seed=5)
+    p = rng.permutation(n)
+    invp = np.argsort(p)
+    K = _HostK(L, p, invp)
+    E = _c(rng, n, ks)
+    CX = _c(rng, n + 3, ks)
+    G = CX.conj().T @ CX
+    Kad = R.SparseLLTP_AD(K, E, G)
+    B = _c(rng, n, 3)
+    Ld = L.toarray()
+    Pd = np.zeros((n, n))
+    Pd[p, np.arange(n)] = 1.0
+    Kinv = Pd @ np.linalg.inv(Ld @ Ld.conj().T) @ Pd.T
+    ref = Kinv @ B + E @ np.linalg.solve(G, E.conj().T @ B)
+    assert np.allclose(Kad.ldiv(B), ref, rtol=1e-10, atol=1e-12)
+    X2, CX2 = _c(rng, n, ks), _c(rng, n + 3, ks)
+    Kad.update_basis(X2, CX2)
+    G2 = CX2.conj().T @ CX2
+    ref2 = Kinv @ B + X2 @ np.linalg.solve(G2, X2.conj().T @ B)
+    assert np.allclose(Kad.ldiv(B), ref2, rtol=1e-10, atol=1e-12)
+    with pytest.raises(R.DimensionMismatch):
+        R.SparseLLTP_AD(K, E[:-1], G)
+    with pytest.raises(np.linalg.LinAlgError):
+        R.SparseLLTP_AD(K, E, -np.eye(ks))
+
+
+def test_mul_coupled_shares_the_common_factor():
+    rng = np.random.default_rng(6)
+    calls = []
+
+    class Counted:
+        def __init__(self, A):
+            self.A, self.shape = A, A.shape
+
+        def __matmul__(self, X):
+            calls.append(1)
+            return self.A @ X
+
+    F = Counted(_c(rng, 5, 4))
+    M0, S0 = _c(rng, 6, 5), _c(rng, 3, 5)
+    V = _c(rng, 4, 2)
+    MV, SV = R.mul_coupled(MulChainMat(M0, F), MulChainMat(S0, F), V)
+    assert len(calls) == 1
+    assert np.allclose(MV, M0 @ F.A @ V) and np.allclose(SV, S0 @ F.A @ V)
+    MV, SV = R.mul_coupled(MulChainMat(M0, F), MulChainMat(S0, Counted(F.A)), V)
+    assert len(calls) == 3 and np.allclose(SV, S0 @ F.A @ V)
