@@ -171,17 +171,18 @@ std::vector<double> l2_scaling(int64_t n, const Csc& A) {
   return s;
 }
 
-// Partial partition of ix[0, n) by |w[ix]|: afterwards positions ncut..n (1-based) hold the
-// n − ncut + 1 largest (a quickselect with the last element as pivot, larger values moved
-// to the right end; the scheme of split2!, ictkl3.jl:9-44).
-void partition_largest(int64_t n, int64_t ncut, std::vector<int64_t>& ix, const std::vector<cd>& w) {
+// Partial partition of ix[0, n) by mag[ix] (each candidate's |w|, computed once per column):
+// afterwards positions ncut..n (1-based) hold the n − ncut + 1 largest (a quickselect with
+// the last element as pivot, larger values moved to the right end; the scheme of split2!,
+// ictkl3.jl:9-44).
+void partition_largest(int64_t n, int64_t ncut, std::vector<int64_t>& ix, const std::vector<double>& mag) {
   if (n <= 1 || ncut <= 0 || ncut > n) return;
   int64_t first = 1, last = n;
   while (first < last) {
     int64_t mid = last;
-    const double pivot = std::abs(w[(size_t)ix[(size_t)mid - 1]]);
+    const double pivot = mag[(size_t)ix[(size_t)mid - 1]];
     for (int64_t j = last - 1; j >= first; --j)
-      if (std::abs(w[(size_t)ix[(size_t)j - 1]]) > pivot) {
+      if (mag[(size_t)ix[(size_t)j - 1]] > pivot) {
         --mid;
         std::swap(ix[(size_t)mid - 1], ix[(size_t)j - 1]);
       }
@@ -211,6 +212,7 @@ int64_t ic_attempt(int64_t n, const Csc& A, const std::vector<double>& scale, st
   std::vector<int64_t> headl((size_t)n, -1), nextl((size_t)n, -1), headr((size_t)n, -1), nextr((size_t)n, -1);
   std::vector<int64_t> posl((size_t)n, 0), posr((size_t)n, 0);
   std::vector<cd> w((size_t)n, cd(0.0, 0.0));
+  std::vector<double> mag((size_t)n, 0.0);
   std::vector<char> mark((size_t)n, 0);
   std::vector<int64_t> lst;
   lst.reserve((size_t)n);
@@ -278,19 +280,20 @@ int64_t ic_attempt(int64_t n, const Csc& A, const std::vector<double>& scale, st
     const int64_t nw = (int64_t)lst.size();
     for (int64_t k : lst) {
       w[(size_t)k] = w[(size_t)k] * djt;
+      mag[(size_t)k] = std::abs(w[(size_t)k]);
       mark[(size_t)k] = 0;
     }
     const int64_t jsize = std::min(lsize + saved, nw);
     saved += lsize - jsize;
     const int64_t largep = nw - jsize + 1;   // 1-based start of the kept candidates
     if (nw >= 1) {
-      partition_largest(nw, largep, lst, w);
+      partition_largest(nw, largep, lst, mag);
       std::sort(lst.begin() + (largep - 1), lst.end());
       int64_t indr = largep;
       for (int64_t pos = largep; pos <= nw; ++pos) {
         const int64_t k = lst[(size_t)pos - 1];
         const cd t = w[(size_t)k];
-        const double m = std::abs(t);
+        const double m = mag[(size_t)k];
         if (m >= tau1) {
           d[(size_t)k] -= t.real() * t.real() + t.imag() * t.imag();
           if (d[(size_t)k] <= kSmall && k > j) return -(j + 1);
@@ -303,14 +306,14 @@ int64_t ic_attempt(int64_t n, const Csc& A, const std::vector<double>& scale, st
       }
       const int64_t radd = std::min(indr - 1, rsize + savedr);
       const int64_t larger = (indr - 1) - radd + 1;
-      partition_largest(indr - 1, larger, lst, w);
+      partition_largest(indr - 1, larger, lst, mag);
       savedr += rsize - radd;
       seg.clear();
       for (int64_t pos = larger; pos <= indr - 1; ++pos) {
         const int64_t k = lst[(size_t)pos - 1];
         const cd t = w[(size_t)k];
         w[(size_t)k] = cd(0.0, 0.0);
-        if (tau2 == 0.0 || std::abs(t) > tau2) seg.emplace_back(k, t);
+        if (tau2 == 0.0 || mag[(size_t)k] > tau2) seg.emplace_back(k, t);
       }
       for (int64_t pos = 1; pos < larger; ++pos) w[(size_t)lst[(size_t)pos - 1]] = cd(0.0, 0.0);
       std::sort(seg.begin(), seg.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
