@@ -58,7 +58,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         cmd[1:1] = ["-Xptxas", "-v"]
     _run(cmd)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, ic_o, "-lcudart"])
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, ic_o, "-lcudart", "-lpthread"])
     os.replace(tmp, LIB)
     return LIB
 

@@ -24,6 +24,7 @@
 #include <complex>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rls_b200.h"
@@ -82,35 +83,56 @@ Csc normal_lower(int64_t n, const Csc& C, cd z) {
       h.row[(size_t)at] = j;
       h.val[(size_t)at] = std::conj(cz.val[(size_t)q]);
     }
-  Csc a;
-  a.ptr.assign((size_t)n + 1, 0);
-  std::vector<int64_t> seen((size_t)n, -1);
-  std::vector<cd> x((size_t)n);
-  std::vector<int64_t> touched;
-  for (int64_t j = 0; j < n; ++j) {
-    touched.clear();
-    for (int64_t qb = cz.ptr[(size_t)j]; qb < cz.ptr[(size_t)j + 1]; ++qb) {
-      const int64_t k = cz.row[(size_t)qb];
-      const cd b = cz.val[(size_t)qb];
-      for (int64_t qa = h.ptr[(size_t)k]; qa < h.ptr[(size_t)k + 1]; ++qa) {
-        const int64_t i = h.row[(size_t)qa];
-        const cd t = h.val[(size_t)qa] * b;
-        if (seen[(size_t)i] != j) {
-          seen[(size_t)i] = j;
-          x[(size_t)i] = t;
-          touched.push_back(i);
-        } else {
-          x[(size_t)i] += t;
+  // columns are independent: contiguous column ranges on host threads, each column summed in
+  // the same order as a single thread would, then concatenated
+  const int64_t nthreads = std::max<int64_t>(1, std::min<int64_t>((int64_t)std::thread::hardware_concurrency(),
+                                                                  std::min<int64_t>(16, n / 256 + 1)));
+  std::vector<Csc> part((size_t)nthreads);
+  auto run = [&](int64_t t) {
+    const int64_t j0 = n * t / nthreads, j1 = n * (t + 1) / nthreads;
+    Csc& a = part[(size_t)t];
+    a.ptr.assign((size_t)(j1 - j0) + 1, 0);
+    std::vector<int64_t> seen((size_t)n, -1);
+    std::vector<cd> x((size_t)n);
+    std::vector<int64_t> touched;
+    for (int64_t j = j0; j < j1; ++j) {
+      touched.clear();
+      for (int64_t qb = cz.ptr[(size_t)j]; qb < cz.ptr[(size_t)j + 1]; ++qb) {
+        const int64_t k = cz.row[(size_t)qb];
+        const cd b = cz.val[(size_t)qb];
+        for (int64_t qa = h.ptr[(size_t)k]; qa < h.ptr[(size_t)k + 1]; ++qa) {
+          const int64_t i = h.row[(size_t)qa];
+          const cd t2 = h.val[(size_t)qa] * b;
+          if (seen[(size_t)i] != j) {
+            seen[(size_t)i] = j;
+            x[(size_t)i] = t2;
+            touched.push_back(i);
+          } else {
+            x[(size_t)i] += t2;
+          }
         }
       }
+      std::sort(touched.begin(), touched.end());
+      for (int64_t i : touched)
+        if (i >= j) {
+          a.row.push_back(i);
+          a.val.push_back(x[(size_t)i]);
+        }
+      a.ptr[(size_t)(j - j0) + 1] = (int64_t)a.row.size();
     }
-    std::sort(touched.begin(), touched.end());
-    for (int64_t i : touched)
-      if (i >= j) {
-        a.row.push_back(i);
-        a.val.push_back(x[(size_t)i]);
-      }
-    a.ptr[(size_t)j + 1] = (int64_t)a.row.size();
+  };
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < nthreads; ++t) pool.emplace_back(run, t);
+  run(0);
+  for (auto& th : pool) th.join();
+  Csc a;
+  a.ptr.assign((size_t)n + 1, 0);
+  for (int64_t t = 0; t < nthreads; ++t) {
+    const int64_t j0 = n * t / nthreads, j1 = n * (t + 1) / nthreads;
+    const int64_t base = (int64_t)a.row.size();
+    a.row.insert(a.row.end(), part[(size_t)t].row.begin(), part[(size_t)t].row.end());
+    a.val.insert(a.val.end(), part[(size_t)t].val.begin(), part[(size_t)t].val.end());
+    for (int64_t j = j0; j < j1; ++j) a.ptr[(size_t)j + 1] = base + part[(size_t)t].ptr[(size_t)(j - j0) + 1];
   }
   return a;
 }

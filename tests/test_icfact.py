@@ -16,7 +16,8 @@ from rls_b200.examples import skewlap3d, sprand
 
 def _case(kind, n, seed):
     if kind == "random":
-        return (sp.random(n, n, density=0.08, random_state=seed, format="csc") + sp.identity(n) * 0.3).tocsc()
+        dens = 0.08 if n < 200 else 6.0 / n
+        return (sp.random(n, n, density=dens, random_state=seed, format="csc") + sp.identity(n) * 0.3).tocsc()
     if kind == "complex":
         A = sp.random(n, n, density=0.06, random_state=seed, format="csc")
         B = sp.random(n, n, density=0.03, random_state=seed + 1, format="csc")
@@ -37,6 +38,7 @@ CASES = [
     ("stencil", 64, 12.5 - 3j, 1e-3, 1e-4, 0.0, 8, 4),
     ("stencil", 125, -40.0, 1e-2, 1e-3, 0.0, 5, 5),
     ("sprand", 120, 0.5 + 0.05j, 1e-3, 1e-4, 0.0, 20, 10),
+    ("random", 600, 0.1 - 0.2j, 1e-2, 1e-3, 0.0, 6, 4),     # the normal product on several threads
 ]
 
 
