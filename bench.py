@@ -517,10 +517,11 @@ def run_ours(args):
                                   sigma[timed[:args.steps * s]]))}
     # roofline of the dominant profiled kernel
     names = {0: "k_trsm_half (R⁻¹/R⁻ᴴ on T−zI, block-row scaled factor)", 1: "k_heev_rr (projected eigensolve)",
-             2: "k_gemm_rows (recycle X/W product)", 3: "k_trmm_partial+reduce (T·V, Tᴴ·[J5 V])"}
+             2: "recycle step span (k_batch_czx .. k_batch_xw, or k_gemm_rows per point)", 3: "k_trmm_partial+reduce (T·V, Tᴴ·[J5 V])"}
     peaks = {}
     try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
     except (OSError, ValueError):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))

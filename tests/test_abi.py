@@ -13,7 +13,8 @@ HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.j
 def declared():
     names = set()
     for h in HEADERS:
-        src = open(h).read()
+        with open(h) as f:
+            src = f.read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(rls_\w+)\s*\(", src, flags=re.M):
             names.add(m.group(1))

@@ -41,7 +41,10 @@ def test_column_shares_and_max_over_ranks(tmp_path, world):
     import torch.multiprocessing as mp
     mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
-    res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
+    res = []
+    for r in range(world):
+        with open(tmp_path / f"rank{r}.json") as f:
+            res.append(json.load(f))
     x_st, x_ed, y_st, y_ed, n_x, n_y, k = bench.GRID
     offs = [r["off"] for r in res]
     assert offs[0] == 0
