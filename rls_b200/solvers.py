@@ -23,6 +23,21 @@ from .grid import Recursion
 EPS = float(np.finfo(np.float64).eps)
 
 
+def _checked(arr, dtype, min_len: int, name: str, writable: bool = False):
+    """arr as a C-contiguous array of dtype holding at least min_len values, for the library to
+    read (or, with writable, write in place: then arr must already be such an array)."""
+    if writable:
+        if not isinstance(arr, np.ndarray) or arr.dtype != dtype or not arr.flags.c_contiguous or \
+                not arr.flags.writeable:
+            raise ArgumentError(-1, f"{name} must be a writable C-contiguous {np.dtype(dtype).name} array")
+        a = arr
+    else:
+        a = np.ascontiguousarray(arr, dtype=dtype)
+    if a.size < min_len:
+        raise DimensionMismatch(-2, f"{name} holds {a.size} values, {min_len} needed")
+    return a
+
+
 @dataclass
 class PsTriRecyControl:
     """psTriRecy.jl:350-370 (same fields, same defaults; shift = normC²·eps·100)."""
@@ -164,6 +179,8 @@ class Engine:
 
     def set_schur(self, T: np.ndarray):
         T = np.asfortranarray(np.asarray(T, dtype=np.complex128))
+        if T.ndim != 2 or T.shape[0] != T.shape[1]:
+            raise DimensionMismatch(-2, f"the Schur factor must be square, got shape {T.shape}")
         n = T.shape[0]
         check(lib().rls_set_schur(self._h, n, ptr(T), n), self._h)
         self._T_id = id(T)
@@ -222,7 +239,8 @@ class Engine:
                         cst, X0=None):
         """Continues (or, with i_begin == 0, starts) a psTriRecy run over rec.Z[i_begin:i_end];
         sigma/st are the run's full-length outputs, cst the C view of st (stats_struct)."""
-        Z = rec.Z
+        Z = _checked(rec.Z, np.complex128, 0, "rec.Z")
+        sigma = _checked(sigma, np.float64, len(Z), "sigma", writable=True)
         x0 = None
         if X0 is not None and i_begin == 0:
             x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
@@ -550,6 +568,8 @@ class Lanes:
                         cst, X0=None):
         """Lane-local points j_begin..j_end-1 of every lane (j_begin == 0 starts the lanes);
         sigma/st are the full-length outputs, cst their C view (Engine.stats_struct)."""
+        Z = _checked(rec.Z, np.complex128, 0, "rec.Z")
+        sigma = _checked(sigma, np.float64, len(Z), "sigma", writable=True)
         x0 = None
         if X0 is not None and j_begin == 0:
             x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
@@ -557,7 +577,7 @@ class Lanes:
                 raise DimensionMismatch(-2, f"X0 must be {(self.n, control.r)}, got {x0.shape}")
         g = rec.c_grid()
         cc = control.c_struct()
-        check(lib().rls_pstrirecy_schur_lanes_range(self._arr, len(self.engines), ptr(rec.Z), len(rec.Z), C.byref(g),
+        check(lib().rls_pstrirecy_schur_lanes_range(self._arr, len(self.engines), ptr(Z), len(Z), C.byref(g),
                                                     C.byref(cc), ptr(x0), int(j_begin), int(j_end), ptr(sigma),
                                                     C.byref(cst)), self.engines[0]._h)
         for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
