@@ -2202,11 +2202,16 @@ int lltp_check_csc(int64_t n, const int64_t* colptr, const int64_t* rowval, cons
       why = "column pointers decrease at column " + std::to_string(c + 1);
       return RLS_ERR_DIM;
     }
-  for (int64_t e = 0; e < nnz; ++e)
+  for (int64_t e = 0; e < nnz; ++e) {
     if (rowval[e] - base < 0 || rowval[e] - base >= n) {
       why = "row index " + std::to_string(rowval[e] - base + 1) + " out of range 1.." + std::to_string(n);
       return RLS_ERR_DIM;
     }
+    if (!std::isfinite(nzval[e].re) || !std::isfinite(nzval[e].im)) {
+      why = "non-finite entry at position " + std::to_string(e + 1);
+      return RLS_ERR_ARG;
+    }
+  }
   return RLS_OK;
 }
 

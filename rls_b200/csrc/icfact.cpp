@@ -374,6 +374,11 @@ extern "C" int rls_ic_factor(int64_t n, const int64_t* colptr, const int64_t* ro
     rls_host_error("rls_ic_factor: invalid arguments");
     return RLS_ERR_ARG;
   }
+  if (!std::isfinite(z.re) || !std::isfinite(z.im) || !std::isfinite(alpha) || !std::isfinite(tau1) ||
+      !std::isfinite(tau2)) {
+    rls_host_error("rls_ic_factor: the shift z, α and the drop tolerances must be finite");
+    return RLS_ERR_ARG;
+  }
   if (rsize < 0 || (n > 1 && lsize < 1)) {
     rls_host_error("rls_ic_factor: lsize must be at least 1 and rsize at least 0 (lsize=" + std::to_string(lsize) +
                    ", rsize=" + std::to_string(rsize) + ")");
@@ -403,6 +408,10 @@ extern "C" int rls_ic_factor(int64_t n, const int64_t* colptr, const int64_t* ro
       if (q > C.ptr[(size_t)j] && r <= C.row[(size_t)q - 1]) {
         rls_host_error("rls_ic_factor: row indices of column " + std::to_string(j + 1) +
                        " are not strictly increasing (SparseMatrixCSC order)");
+        return RLS_ERR_ARG;
+      }
+      if (!std::isfinite(nzval[q].re) || !std::isfinite(nzval[q].im)) {
+        rls_host_error("rls_ic_factor: non-finite entry in column " + std::to_string(j + 1));
         return RLS_ERR_ARG;
       }
       C.row[(size_t)q] = r;

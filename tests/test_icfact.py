@@ -172,3 +172,20 @@ def test_small_and_clamped_sizes():
     check(lib().rls_ic_factor(40, ptr(colptr), ptr(rowval), ptr(nzval), 0, c64(0.1, 0.0), 1e-3, 1e-4, 0.0, 39, 3,
                               ptr(p64), 40 * 40, ptr(lp), None, None, ptr(ip), None), None)
     assert np.array_equal(lp, La.indptr)
+
+
+@pytest.mark.parametrize("bad", ["z", "alpha", "tau1", "entry"])
+def test_non_finite_inputs_are_argument_errors(bad):
+    """A non-finite shift, tolerance or matrix entry is rejected before any work."""
+    Cm = _case("random", 30, seed=7).tolil()
+    z, alpha, tau1 = 0.1 + 0.0j, 0.0, 1e-3
+    if bad == "z":
+        z = complex(np.nan, 0.0)
+    elif bad == "alpha":
+        alpha = np.inf
+    elif bad == "tau1":
+        tau1 = np.nan
+    else:
+        Cm[3, 3] = np.nan
+    with pytest.raises(ArgumentError):
+        R.ic_factor(Cm.tocsc(), z, tau1, 1e-4, alpha, 3, 2, np.arange(30))

@@ -123,3 +123,14 @@ def test_plan_invariants_on_the_af23560_shaped_factor():
         check(lib().rls_test_lltp_plan_dense(23560, ptr(colptr), ptr(rowval), ptr(nzval), 0, op, None,
                                              C.byref(sing), C.byref(lev)), None)
         assert sing.value == 0 and lev.value == -(-23560 // 32)      # one chain through every block row
+
+
+def test_plan_rejects_non_finite_entries():
+    """The checks rls_lltp_upload shares with the plan: a non-finite factor entry is an error."""
+    from rls_b200._lib import ArgumentError
+    colptr = np.array([0, 2, 3], dtype=np.int64)
+    rowval = np.array([0, 1, 1], dtype=np.int64)
+    nzval = np.array([1.0, np.nan, 2.0], dtype=np.complex128)
+    D = np.zeros((2, 2), dtype=np.complex128)
+    with pytest.raises(ArgumentError):
+        check(lib().rls_test_lltp_plan_dense(2, ptr(colptr), ptr(rowval), ptr(nzval), 0, 0, ptr(D), None, None), None)
