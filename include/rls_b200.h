@@ -6,10 +6,13 @@
  * project).  Conventions, shared by all calls:
  *   - complex values are rls_c64 {re, im} (layout of Julia ComplexF64 and of
  *     C99 double complex); matrices are column-major with a leading dimension;
- *   - grid indices and permutations are 1-based, as in the Julia API;
- *   - calls are synchronous (rls_tsqr_r_noalloc only enqueues; see there); no
- *     exceptions cross the ABI; a negative return is an rls_status and
- *     rls_last_error() gives the message;
+ *   - grid indices and permutations are 1-based, as in the Julia API; the
+ *     sparse entry points take a base argument (0 or 1) for their CSC arrays;
+ *   - calls are synchronous (rls_tsqr_r_noalloc and rls_spmm_shifted_dev only
+ *     enqueue; see there); no exceptions cross the ABI; a negative return is an
+ *     rls_status and rls_last_error() gives the message (rls_last_error(NULL)
+ *     for the calls that take no context: the grid, rls_lane_offsets,
+ *     rls_ic_factor);
  *   - the library never frees or retains caller memory.
  */
 #ifndef RLS_B200_H
