@@ -11,8 +11,8 @@
  *   - calls are synchronous (rls_tsqr_r_noalloc and rls_spmm_shifted_dev only
  *     enqueue; see there); no exceptions cross the ABI; a negative return is an
  *     rls_status and rls_last_error() gives the message (rls_last_error(NULL)
- *     for the calls that take no context: the grid, rls_lane_offsets,
- *     rls_ic_factor);
+ *     for rls_lane_offsets and rls_ic_factor, which take no context; the grid
+ *     calls return the status alone);
  *   - the library never frees or retains caller memory.
  */
 #ifndef RLS_B200_H
