@@ -78,7 +78,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmm", action="store_true", help="skip the sparse shifted product measurement")
     ap.add_argument("--no-ic", action="store_true", help="skip the IC preconditioner apply measurement")
-    ap.add_argument("--plain-steps", type=int, default=1, help="steps timed on the unbatched per-point path")
+    ap.add_argument("--plain-steps", type=int, default=5, help="steps timed on the unbatched per-point path")
+    ap.add_argument("--accuracy-points", type=int, default=64,
+                    help="timed points checked against the FP64 truth after the timed region (0: skip)")
     ap.add_argument("--ncu-window", default=None,
                     help="WARM,COUNT: run WARM points, then COUNT points inside cudaProfilerStart/Stop, and exit "
                          "(for ncu --profile-from-start off); no timing output")
@@ -473,6 +475,28 @@ def run_ours(args):
     sigma, timed, refines, prof, waits, clk = (main["sig"], main["timed"], main["refines"], main["prof"],
                                                main["waits"], main["clk"])
 
+    # accuracy of the timed run itself (after the timed region): σ at sampled timed points of
+    # every lane against an FP64 truth (block inverse iteration with cuBLAS triangular solves
+    # on the same Schur factor, independent of the engine's kernels; tests/truth.py)
+    accuracy = None
+    if args.accuracy_points > 0:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from truth import sigma_min_schur
+        pick = np.unique(np.concatenate([
+            timed[np.linspace(0, len(timed) - 1, args.accuracy_points).astype(np.int64)],
+            timed[np.argsort(sigma[timed])[:16]]]))                # plus the 16 smallest σ
+        t0 = time.perf_counter()
+        truth, bound, its = sigma_min_schur(T, sub.Z[pick])
+        err = np.abs(sigma[pick] - truth)
+        lane_of = np.searchsorted(main["offs"], pick, side="right") - 1
+        accuracy = {"points": int(pick.size), "lanes_covered": int(np.unique(lane_of).size),
+                    "max_abs_err": float(err.max()), "max_abs_err_over_normC": float(err.max() / NORMC),
+                    "bar": "1e-4·normC", "within_bar": bool(err.max() <= 1e-4 * NORMC),
+                    "max_rel_err": float(np.max(err / truth)),
+                    "truth_max_err_bound": float(bound.max()), "truth_iterations_max": int(its.max()),
+                    "truth": "block inverse subspace iteration on (T−zI)ᴴ(T−zI), cuBLAS FP64 triangular solves",
+                    "seconds": time.perf_counter() - t0}
+
     # end to end through the public API on fresh contexts: host buffers, T uploaded to every lane
     e2e = None
     if not args.no_e2e:
@@ -530,7 +554,7 @@ def run_ours(args):
     cnt, tot_ms, work = prof[top]
     achieved = (work / cnt) / (tot_ms / cnt / 1e3) / 1e9 if cnt else 0.0
     # DRAM bytes per launch of the TRSM from one ncu capture of this workload (n = 4000, k = 6):
-    # dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_trsm_half_sprand4000.md
+    # dram__bytes_read.sum + dram__bytes_write.sum of k_trsm_half<6>
     traffic = NCU_TRSM_TRAFFIC if (top == 0 and args.n == N_MAT) else None
     out["roofline"] = {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": hbm_peak,
                        "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
@@ -560,6 +584,8 @@ def run_ours(args):
                                            args.cpu_sample_s)
     if e2e is not None:
         out["e2e"] = e2e
+    if accuracy is not None:
+        out["accuracy"] = accuracy
     if plain is not None:
         out["plain_per_point"] = plain
         a0 = args.warmup * s   # lane 0 starts at the rank's first point, as the plain run does

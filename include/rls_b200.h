@@ -234,7 +234,8 @@ int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const 
  * full-length arrays; the stats scalars are summed over lanes.  The _range form runs,
  * in every lane, the lane-local points j_begin..j_end-1 (a call with j_begin > 0
  * continues each lane's run).  A log sink set on a context is called from that lane's
- * thread. */
+ * thread.  Every lane needs a context of its own: a context listed twice returns
+ * RLS_ERR_ARG before any work, with the message in rls_last_error(NULL). */
 int rls_lane_offsets(const rls_grid* g, int64_t nZ, int nlanes, int64_t* offsets /* nlanes+1 */);
 int rls_pstrirecy_schur_lanes(rls_ctx* const* ctxs, int nlanes, const rls_c64* Z, int64_t nZ,
                               const rls_grid* g, const rls_pstrirecy_control* control,
@@ -341,7 +342,10 @@ int rls_sigma_grad(rls_ctx* ctx, rls_c64 z, const rls_c64* v0, int refine_steps,
  *     reached that point.
  *   - The first call on a device, with that device current, looks up the
  *     array's address there (cudaGetSymbolAddress); make that first call before
- *     any stream capture begins on the device.
+ *     any stream capture begins on the device.  A device reset (cudaDeviceReset,
+ *     or a reset of the primary context by the application) unloads the array;
+ *     the first call made in the new context looks its address up again, so that
+ *     call too belongs before any stream capture.
  *   - All calls on a device share the one array, and it keeps the last call's
  *     contents (nothing in it needs to start at zero).  Calls whose work
  *     overlaps on the GPU — issued on different streams, or from several host

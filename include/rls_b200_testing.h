@@ -3,7 +3,8 @@
  * parity tests.  They have no counterpart in the reference: each runs one device
  * routine of the engine on host inputs so that it can be compared with the
  * LAPACK routine the reference calls at that point.  Host pointers, column-major.
- * All but rls_test_lltp_plan_dense need rls_set_schur() and rls_test_setup() first.
+ * All but rls_test_lltp_plan_dense and rls_test_recip need rls_set_schur() and
+ * rls_test_setup() first.
  */
 #ifndef RLS_B200_TESTING_H
 #define RLS_B200_TESTING_H
@@ -42,6 +43,10 @@ int rls_test_svd_rr(rls_ctx* ctx, int nS, int r, int sideL, int lq, const rls_c6
  * may be NULL) receives the SM clock at the kernel's phase boundaries. */
 int rls_test_heev_rr(rls_ctx* ctx, int pr, int r, const rls_c64* H1, const rls_c64* H2, rls_c64 z,
                      double shift, double tau, int* rr, double* lam, rls_c64* G, long long* clk);
+
+/* The eigensolver's reciprocal (hardware estimate refined by two Newton steps) and CUDA's
+ * 1.0/q on the same n inputs (host arrays).  Needs a context only. */
+int rls_test_recip(rls_ctx* ctx, int64_t n, const double* q, double* r_nr, double* r_div);
 
 /* updateRecycledSpace! (recySpace.jl:160-223) with X (n × r) on the device space
  * (r_sub = 1).  Compare the CPU restatement. */

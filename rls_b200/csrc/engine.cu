@@ -2438,6 +2438,16 @@ extern "C" int rls_pstrirecy_schur_lanes_range(rls_ctx* const* ctxs, int nlanes,
     return RLS_ERR_ARG;
   for (int l = 0; l < nlanes; ++l)
     if (!ctxs[l]) return RLS_ERR_ARG;
+  // one host thread per lane drives its context's stream and workspaces: a context listed
+  // twice would be driven by two threads at once.  Checked before any context is touched,
+  // so the message goes to rls_last_error(NULL).
+  for (int l = 0; l < nlanes; ++l)
+    for (int q = 0; q < l; ++q)
+      if (ctxs[q] == ctxs[l]) {
+        g_create_err = "rls_pstrirecy_schur_lanes: lanes " + std::to_string(q) + " and " + std::to_string(l) +
+                       " share one context; every lane needs its own";
+        return RLS_ERR_ARG;
+      }
   std::vector<int64_t> off((size_t)nlanes + 1);
   int rc = rls_lane_offsets(g, nZ, nlanes, off.data());
   if (rc != RLS_OK) {
@@ -2581,7 +2591,28 @@ static __device__ __align__(256) cplx g_noalloc_tsqr_scratch[RLS_NOALLOC_STACK0 
 
 namespace {
 std::mutex g_noalloc_mu;
+// Address of the array per device, with the driver context it was looked up in: a device
+// reset (cudaDeviceReset, or the host application resetting the primary context) unloads
+// the module, and the next call, made in the new context, looks the address up again.
 cplx* g_noalloc_ptr[RLS_NOALLOC_MAX_DEVICES] = {};
+void* g_noalloc_ctx[RLS_NOALLOC_MAX_DEVICES] = {};
+
+// The driver's cuCtxGetCurrent through the runtime, so that the library needs no link to
+// libcuda (it must load on hosts without a driver).  Returns nullptr when unavailable.
+void* current_driver_context() {
+  using Fn = int (*)(void**);
+  static Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (Fn) nullptr;
+    return reinterpret_cast<Fn>(p);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 void noalloc_fail(const char* fmt, ...) {
   char buf[512];
@@ -2616,9 +2647,11 @@ extern "C" int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int 
   }
   cplx* scratch;
   {
-    // set-up, once per device, with that device current: the scratch array's address
+    // set-up, once per device and driver context, with that device current: the scratch
+    // array's address
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    void* drv = current_driver_context();
+    if (!g_noalloc_ptr[dev] || drv != g_noalloc_ctx[dev]) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_tsqr_scratch);
       if (e != cudaSuccess || !p) {
@@ -2627,6 +2660,7 @@ extern "C" int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int 
         return RLS_ERR_CUDA;
       }
       g_noalloc_ptr[dev] = static_cast<cplx*>(p);
+      g_noalloc_ctx[dev] = drv;
     }
     scratch = g_noalloc_ptr[dev];
   }

@@ -300,3 +300,30 @@ extern "C" int rls_test_recycle(rls_ctx* ctx, rls_c64 z, double shift, double ga
                          cudaMemcpyDeviceToHost, ctx->stream));
   return sync_and_check(ctx);
 }
+
+namespace {
+__global__ void k_test_recip(int64_t n, const double* q, double* r_nr, double* r_div) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    r_nr[i] = recip_nr(q[i]);
+    r_div[i] = 1.0 / q[i];
+  }
+}
+}  // namespace
+
+// recip_nr (the Sturm-count reciprocal: hardware estimate + two Newton steps) beside CUDA's
+// correctly rounded 1.0/q, for the same inputs.
+extern "C" int rls_test_recip(rls_ctx* ctx, int64_t n, const double* q, double* r_nr, double* r_div) {
+  if (!ctx || n < 1 || !q || !r_nr || !r_div) return RLS_ERR_ARG;
+  DevTmp t(ctx);
+  double* dq = t.alloc<double>((size_t)n);
+  double* d1 = t.alloc<double>((size_t)n);
+  double* d2 = t.alloc<double>((size_t)n);
+  if (!dq || !d1 || !d2) return RLS_ERR_NOMEM;
+  CK(cudaMemcpyAsync(dq, q, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, 1024);
+  k_test_recip<<<blocks, 256, 0, ctx->stream>>>(n, dq, d1, d2);
+  RET(check_launch(ctx, "k_test_recip"));
+  CK(cudaMemcpyAsync(r_nr, d1, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(r_div, d2, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
+}

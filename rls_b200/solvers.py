@@ -257,6 +257,11 @@ class Engine:
         """Speculative recycle batch size (1 = plain per-point path)."""
         check(lib().rls_ctx_set_batch(self._h, int(max_points)), self._h)
 
+    def set_ritz_basis(self, g1_always: bool):
+        """Recycle-step Ritz basis when r_ == p·r: V·G1·G2 (True, default) or the
+        reference's V·G2 (False, fastRaylRitz.jl:199-202)."""
+        check(lib().rls_ctx_set_ritz_basis(self._h, int(bool(g1_always))), self._h)
+
     def set_trsm_ctas(self, ctas: int):
         """CTAs per triangular solve (0: one per half block row, the single-traversal
         optimum; fewer leave SMs to concurrent lanes)."""

@@ -49,3 +49,19 @@ def test_status_strings_and_null_context(built_lib):
     from rls_b200._lib import rls_grid
     g = rls_grid(0.0, 1.0, 0.0, 1.0, 1, 4, 1)
     assert L.rls_grid_zigzag(C.byref(g), None) == -1
+
+
+def test_lanes_reject_a_context_listed_twice(built_lib):
+    """Each lane's host thread drives its own context; a context listed twice is an
+    ArgumentError found before any context is touched (the pointers here are never read)."""
+    from rls_b200._lib import lib, rls_grid, rls_pstrirecy_control
+    L = lib()
+    fake = C.create_string_buffer(64)                     # stands in for one context handle
+    ctxs = (C.c_void_p * 3)(C.addressof(fake), C.addressof(fake) + 16, C.addressof(fake))
+    g = rls_grid(0.0, 1.0, 0.0, 1.0, 4, 4, 2)
+    Z = (C.c_double * 32)()
+    sig = (C.c_double * 16)()
+    ctl = rls_pstrirecy_control()
+    st = L.rls_pstrirecy_schur_lanes(ctxs, 3, Z, 16, C.byref(g), C.byref(ctl), None, sig, None)
+    assert st == -1
+    assert b"share one context" in L.rls_last_error(None)

@@ -188,3 +188,71 @@ def test_heev_rr_matches_zheevr(eng_T, pr, r, tau):
     # residual of the Ritz pairs
     res = np.linalg.norm(Hz @ Gk - Gk * w[:k][None, :]) / scale
     assert res < 1e-10
+
+
+@pytest.fixture(scope="module")
+def eng_T60(cuda_device):
+    """A space of up to 60 blocks of 6 columns: the projected problem reaches pr = 360, the
+    size psTriRecy's p = 60, r = 6 allow."""
+    rng = np.random.default_rng(17)
+    n = 400
+    T = np.triu(crand(rng, n, n)) / np.sqrt(n) + np.eye(n)
+    e = Engine(cuda_device)
+    e.set_schur(T)
+    check(lib().rls_test_setup(e._h, 6, 60), e._h)
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("pr,tau", [(180, 1e-10), (240, 1e-12), (360, 1e-10), (360, 1e10)])
+def test_heev_rr_full_size_matches_zheevr(eng_T60, pr, tau):
+    """find_rr_dim! at the sizes the p = 60 space reaches (the eigensolver keeps Hz in global
+    memory beyond its shared-memory limit).  τ = 1e10 makes the gap rule run through several
+    growing index ranges."""
+    e = eng_T60
+    r = 6
+    rng = np.random.default_rng(pr + 11)
+    H1, H2 = _hz_pair(rng, pr)
+    z = -0.3 + 0.2j
+    shift = 1e-13
+    rr = C.c_int(0)
+    lam = np.zeros(pr)
+    G = np.zeros((pr, pr), dtype=np.complex128, order="F")
+    check(lib().rls_test_heev_rr(e._h, pr, r, ptr(H1), ptr(H2), c64(z.real, z.imag), shift, tau, C.byref(rr),
+                                 ptr(lam), ptr(G), None), e._h)
+    Hz = affine_combine(z, H1, H2, H2.conj().T, np.eye(pr), shift=shift)
+    Hz = np.triu(Hz) + np.triu(Hz, 1).conj().T
+    Hz[np.diag_indices(pr)] = Hz.diagonal().real
+    rr_ref, G_ref = find_rr_dim(Hz, r, tau)
+    assert rr.value == rr_ref
+    w = np.linalg.eigvalsh(Hz)
+    scale = abs(w).max()
+    assert abs(lam[pr - 1] - w[-1]) <= 1e-12 * scale
+    k = rr.value
+    assert np.allclose(lam[:min(k, pr - 1)], w[:min(k, pr - 1)], atol=1e-12 * scale, rtol=0)
+    Gk = G[:, :k]
+    assert np.linalg.norm(Gk.conj().T @ Gk - np.eye(k)) < 1e-10
+    res = np.linalg.norm(Hz @ Gk - Gk * w[:k][None, :]) / scale
+    assert res < 1e-10
+
+
+def test_recip_nr_against_cuda_division(cuda_device):
+    """The eigensolver's Sturm counts divide by the pivot through recip_nr (rcp.approx.ftz.f64
+    estimate + two Newton–Raphson steps).  Its stated bound: within 2 ulp (relative error
+    ≤ 2⁻⁵¹) of CUDA's correctly rounded 1.0/q for normal q whose reciprocal is normal, both
+    signs, across the exponent range."""
+    rng = np.random.default_rng(3)
+    mant = 1.0 + rng.random(20000)
+    expo = rng.integers(-1000, 1000, size=20000)
+    q = np.ldexp(mant, expo) * np.where(rng.random(20000) < 0.5, -1.0, 1.0)
+    q = np.concatenate([q, [1.0, -1.0, 3.0, 0.1, 1e-300, -1e300, 2.0 ** -1020, 2.0 ** 1020]])
+    n = q.size
+    r_nr = np.zeros(n)
+    r_div = np.zeros(n)
+    e = Engine(cuda_device)
+    check(lib().rls_test_recip(e._h, n, ptr(q), ptr(r_nr), ptr(r_div)), e._h)
+    e.close()
+    assert np.array_equal(r_div, 1.0 / q)           # CUDA's division is IEEE round-to-nearest
+    rel = np.abs(r_nr - r_div) / np.abs(r_div)
+    assert np.all(np.isfinite(r_nr))
+    assert rel.max() <= 2.0 ** -51, rel.max()

@@ -103,3 +103,18 @@ def test_generators_shapes():
     assert Ld.shape == (64, 64)
     # Landau operator is complex symmetric
     assert np.allclose(Ld, Ld.T)
+
+
+def test_fp64_truth_matches_dense_svd():
+    """The parity tests' FP64 truth (block inverse iteration on the Schur factor, tests/truth.py)
+    against LAPACK's dense SVD of C − zI, here on the host (torch CPU)."""
+    import scipy.linalg as sla
+    from rls_b200.examples import sprand
+    from truth import sigma_min_schur
+    C = sprand(150).toarray()
+    T = np.triu(sla.schur(C, output="complex")[0])
+    zs = [0.5 + 0.05j, 0.45 + 0.0j, 0.3 - 0.2j, 2.0 + 1.0j]
+    sig, bound, its = sigma_min_schur(T, zs, device="cpu")
+    ref = np.array([sla.svdvals(C - z * np.eye(150))[-1] for z in zs])
+    assert np.all(bound <= 1e-10)
+    assert np.max(np.abs(sig - ref)) <= 1e-12 * 3.2

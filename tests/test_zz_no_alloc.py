@@ -85,6 +85,10 @@ def test_two_calls_in_a_row_match_engine_qr(qr_engine):
         assert np.all(np.isfinite(R))
         assert np.allclose(np.tril(R, -1), 0)
         assert np.linalg.norm(R - Rref) <= RTOL * nA, (m, k, np.linalg.norm(R - Rref) / nA)
+        # independent of the shared TSQR kernel: RᴴR reproduces AᴴA, and |diag R| matches
+        # LAPACK's Householder QR
+        assert np.linalg.norm(R.conj().T @ R - A.conj().T @ A) <= RTOL * nA ** 2
+        assert np.allclose(np.abs(np.diag(R)), np.abs(np.diag(sla.qr(A, mode="r")[0])), rtol=1e-9, atol=0)
 
 
 def test_largest_block_gives_gram_factor(cuda_device):
