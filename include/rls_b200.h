@@ -105,6 +105,64 @@ typedef struct {
   int64_t conv_first, conv_last;
 } rls_lobpcg_control;
 
+/* Mirrors `PsPrecRecyControl` (src/core/psPrecRecy.jl:220-261), fields in order.  Julia
+ * Symbol pred_orth_type: 0 = :lapack, 1 = :shiftchol.  pred_conv_range (Union{Nothing,
+ * UnitRange}) is the 1-based pair pred_conv_first..pred_conv_last, with pred_conv_first < 1
+ * for `nothing`.  shift's default depends on main_normC, so callers pass it explicitly.
+ * inner_verbose_override < 0 stands for `nothing`.  Bool fields are uint8 with explicit
+ * padding. */
+typedef struct {
+  double tol;
+  double lobpcg_tol_scale;
+  double main_normC;
+  double main_tau;
+  double shift;
+  double gap_tau;
+  double recycle_fail_dist_thresh;   /* NaN or Inf = default (one grid step × 1.01) */
+  double tol_pred;
+  double lobpcg_pred_tol_scale;
+  int64_t pred_conv_first, pred_conv_last;
+  double pred_tau;
+  double idx_cutoff_pred;
+  int32_t pred_orth_type;
+  int32_t _pad0;
+  int64_t pred_conv_thresh_type;
+  double lambda_lower_min;
+  double lambda_upper_max;
+  int64_t r_main, p_main, p_min_main;
+  uint8_t main_implict_update, main_implict_recycle, _pad1[6];
+  int64_t r_pred, p_pred, p_min_pred;
+  uint8_t pred_implict_update, pred_implict_recycle, _pad2[6];
+  double hsl_tol, hsl_cntl_1, hsl_cntl_2;
+  int64_t hsl_icntl_1, hsl_icntl_2;
+  double gamma_tol, lambda_n_tol;
+  int64_t inner_verbose_override;
+  uint8_t collect_timing, _pad3[7];
+} rls_psprecrecy_control;
+
+/* Mirrors `PsPrecRecyStats` (src/core/psPrecRecy.jl:318-341), fields in order.  Array members
+ * are caller-allocated with length nZ and may be NULL; main_refine_it and pred_refine_it are
+ * additions (LOBPCG iterations of each stage per point). */
+typedef struct {
+  int64_t* p_count;
+  int64_t* pred_p_count;
+  int64_t* r_recy;
+  rls_c64* pts;
+  rls_c64* pred_pts;
+  rls_c64* precond_rebuild_pts;
+  int64_t* main_M_vec_apps;
+  int64_t* main_M_vec_apps_no_recycle;
+  int64_t* main_L_vec_apps;
+  int64_t* pred_M_vec_apps;
+  int64_t* pred_L_vec_apps;
+  uint64_t main_recycle_time_ns, main_refine_time_ns, main_update_time_ns;
+  uint64_t pred_recycle_time_ns, pred_refine_time_ns, pred_update_time_ns;
+  uint64_t precond_time_ns;
+  int64_t n_it, n_pred_it, n_pts, n_pred_pts, n_precond_rebuild_pts;
+  int64_t* main_refine_it;
+  int64_t* pred_refine_it;
+} rls_psprecrecy_stats;
+
 /* Optional per-point log sink (the reference prints the same lines to `io`). */
 typedef void (*rls_log_fn)(const char* line, void* user);
 
@@ -254,6 +312,30 @@ int rls_lobpcg_svd_invtri(rls_ctx* ctx, rls_c64 z, const rls_c64* X0,
                           const rls_lobpcg_control* control, rls_c64* X_out,
                           double* sigma_r, double* sigma, int64_t* it);
 
+/* Operators of rls_lobpcg_svd, each built from what the context holds:
+ *   RLS_OP_INV_SCHUR  InvMat(adjoint(T − zI)) on the Schur factor (rls_set_schur), as
+ *                     psTriRecy calls it (psTriRecy.jl:797);
+ *   RLS_OP_SHIFTED    ShiftedMat(C, −z) = C − zI on the sparse C (rls_sparse_upload_csc), as
+ *                     psPrecRecy's main stage (psPrecRecy.jl:926);
+ *   RLS_OP_PRED       MulChainMat(ShiftedMat(C, −z), invF), invF = P·L⁻ᴴ of the uploaded
+ *                     SparseLLTP (rls_lltp_upload), the prediction stage's operator and
+ *                     _compute_λ_n's (psPrecRecy.jl:27-41, :405-422);
+ *   RLS_OP_INV_L      InvMat(L) of the uploaded factor, _compute_γ's operator (:388-402).
+ * Preconditioners: RLS_PREC_NONE (IdentityMat) or RLS_PREC_LLTP (the uploaded SparseLLTP). */
+enum { RLS_OP_INV_SCHUR = 0, RLS_OP_SHIFTED = 1, RLS_OP_PRED = 2, RLS_OP_INV_L = 3 };
+enum { RLS_PREC_NONE = 0, RLS_PREC_LLTP = 1 };
+
+/* lobpcgSvd(C, X0, K, keep, control) (src/core/lobpcgSvd.jl:365-477) on the operator `op` at
+ * shift z (ignored by RLS_OP_INV_L), with K = `prec`: side 'L' (largest singular values of
+ * C, returned inverted in keep.σ) or 'S' (smallest), orth_type :lapack or :shiftchol,
+ * conv_thresh_type 0 or 1 and conv_range as LobpcgSvdControl holds them; 1 <= r <= 40.
+ * X0 (n × r, may be NULL: the fixed uniform [0,1) fill) stands for the caller's X0 or rand!.
+ * X_out (n × r, may be NULL) receives keep.S[:, 1:r], sigma_r (r, may be NULL) keep.σ[1:r],
+ * *sigma the returned σ (side 'S': σ[1]; side 'L': 1/σ[1]) and *it the iteration count. */
+int rls_lobpcg_svd(rls_ctx* ctx, int op, rls_c64 z, int prec, const rls_c64* X0,
+                   const rls_lobpcg_control* control, rls_c64* X_out, double* sigma_r, double* sigma,
+                   int64_t* it);
+
 /* ---- sparse shifted product ------------------------------------------------------ */
 
 /* Uploads a sparse m × n C in the layout of Julia's SparseMatrixCSC (colptr n+1, rowval and
@@ -309,6 +391,37 @@ int rls_ic_factor(int64_t n, const int64_t* colptr, const int64_t* rowval, const
                   const int64_t* p, int64_t cap, int64_t* lcolptr, int64_t* lrowval, rls_c64* lnzval,
                   int64_t* invp, double* shift_used);
 int rls_lltp_ldiv_dev(rls_ctx* ctx, int b, const rls_c64* B, int64_t ldb, rls_c64* X, int64_t ldx);
+
+/* ---- psPrecRecy -------------------------------------------------------------------- */
+
+/* psPrecRecy(C, rec; control) (src/core/psPrecRecy.jl:617-1033) on the device: C is n × n in
+ * the reference's CSC layout (colptr n+1, rowval and nzval nnz; indices base 0 or 1, as
+ * SparseMatrixCSC holds them with base = 1).  p is the column order the reference takes from
+ * SPQR (qr(C).cpiv, psPrecRecy.jl:625), passed in by the caller (base as the CSC; NULL: the
+ * identity).  The IC preconditioner is built on the host (get_hsl_LLTP, rls_ic_factor) at
+ * rec.Z[1] and at every rebuild; everything per grid point runs on the GPU.  X0_main (n ×
+ * r_main), X0_pred (n × r_pred) and X0_bound (n × 1) stand for the reference's rand! draws of
+ * the two stages' start blocks (:547, :586; X0_pred again at every rebuild, :849) and of the
+ * Ritz-bound estimates γ and λ_n (:388-422); NULL fills them on the device with a fixed
+ * uniform [0, 1) sequence.  sigma_min receives nZ values in Z order.  Supported: the
+ * configuration of the reference's drivers (main_implict_recycle = true, main_implict_update
+ * = false, pred_implict_recycle = true, pred_implict_update = true), 1 <= r_main <= 8,
+ * 1 <= r_pred <= 40, p_pred·r_pred <= 800; other settings return RLS_ERR_ARG.  A context
+ * holding a Schur operator of another order returns RLS_ERR_STATE. */
+int rls_psprecrecy(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval, const rls_c64* nzval,
+                   int base, const int64_t* p, const rls_c64* Z, int64_t nZ, const rls_grid* g,
+                   const rls_psprecrecy_control* control, const rls_c64* X0_main, const rls_c64* X0_pred,
+                   const rls_c64* X0_bound, double* sigma_min, rls_psprecrecy_stats* stats);
+
+/* The same loop over points i_begin..i_end-1 (0-based, end exclusive): i_begin = 0 starts a
+ * run (C uploaded, preconditioner built, spaces reset); i_begin > 0 continues the run whose
+ * previous call ended there, with C, p and the X0 arguments ignored.  No reference
+ * counterpart: it lets a caller stream a long grid in pieces. */
+int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                         const rls_c64* nzval, int base, const int64_t* p, const rls_c64* Z, int64_t nZ,
+                         const rls_grid* g, const rls_psprecrecy_control* control, const rls_c64* X0_main,
+                         const rls_c64* X0_pred, const rls_c64* X0_bound, int64_t i_begin, int64_t i_end,
+                         double* sigma_min, rls_psprecrecy_stats* stats);
 
 /* ---- gradient -------------------------------------------------------------------- */
 

@@ -157,3 +157,78 @@ def block_rot_rmul_adj(A, U, i1, i2, r):
     A2 = A[:, c2].copy()
     A[:, c1] = A1 @ Ua[:r, :r] + A2 @ Ua[r:, :r]
     A[:, c2] = A1 @ Ua[:r, r:] + A2 @ Ua[r:, r:]
+
+
+def qr_shiftchol_inplace(X: np.ndarray, R: np.ndarray | None = None, itmax: int = 3):
+    """_rls_qr_shiftchol! (RLSLinearAlgebra.jl:725-796): shifted Cholesky-QR.
+
+    X (m×n) ← orthonormal basis; R (when given) ← R_k ⋯ R_1.  On a failed Cholesky of the
+    Gram matrix, 11(mn + n(n+1))·eps·max_j‖X_j‖² is added to its diagonal (cumulatively)
+    and the factorisation is retried; a sweep stops once ‖XᴴX − I‖_F < 2√n·eps.  Returns
+    True when it converged within itmax sweeps (the reference warns otherwise).
+    """
+    m, n = X.shape
+    assert m >= n, "shifted Cholesky-QR requires m >= n"
+    if n == 0:
+        return True
+    conv_tol = 2 * np.sqrt(float(n)) * EPS
+    work = X.conj().T @ X
+    it = 1
+    retries = 0
+    while it <= itmax:
+        c, info = lapack.zpotrf(work.copy(), lower=0, clean=1)
+        if info == 0:
+            Rc = np.triu(c)
+            if it == 1 and R is not None:
+                R[:n, :n] = np.eye(n)
+            if R is not None:
+                R[:n, :n] = Rc @ R[:n, :n]
+            X[:, :] = sla_solve_right_upper(X, Rc)
+            work = X.conj().T @ X
+            if np.linalg.norm(work - np.eye(n)) < conv_tol:
+                return True
+            it += 1
+        else:
+            retries += 1
+            if retries > 1000:
+                raise RuntimeError("shifted Cholesky-QR: no shift made the Gram matrix factorable")
+            gnorm = max(np.linalg.norm(X[:, j]) ** 2 for j in range(n))
+            work = work + 11 * (m * n + n * (n + 1)) * EPS * gnorm * np.eye(n)
+    return False
+
+
+def sla_solve_right_upper(X, Rc):
+    """X · Rc⁻¹ for upper-triangular Rc (the reference forms trtri(Rc) then trmm; the same
+    product to rounding)."""
+    import scipy.linalg as sla
+    Rinv = sla.solve_triangular(Rc, np.eye(Rc.shape[0], dtype=np.complex128), lower=False)
+    return X @ Rinv
+
+
+def qr_typed(V: np.ndarray, R: np.ndarray | None = None, typ: str = "lapack"):
+    """rls_qr!(V, R; type) (RLSLinearAlgebra.jl:584-596)."""
+    if typ == "lapack":
+        return qr_inplace(V, R)
+    if typ == "shiftchol":
+        qr_shiftchol_inplace(V, R)
+        return None
+    raise ValueError(f"unsupported rls_qr! type: {typ}")
+
+
+def orth_typed(V, X, W=None, R=None, typ="lapack"):
+    """rls_orth!(V, X, W, R; type) (RLSLinearAlgebra.jl:1127-1160)."""
+    if typ == "lapack":
+        return orth_inplace(V, X, W, R)
+    nX = X.shape[1]
+    W1 = V.conj().T @ X
+    X -= V @ W1
+    R1 = np.zeros((nX, nX), dtype=np.complex128)
+    qr_typed(X, R1, typ)
+    W2 = V.conj().T @ X
+    X -= V @ W2
+    R2 = np.zeros((nX, nX), dtype=np.complex128)
+    qr_typed(X, R2, typ)
+    if W is not None:
+        W[:, :] = W2 @ R1 + W1
+    if R is not None:
+        R[:, :] = R2 @ R1

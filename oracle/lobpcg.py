@@ -10,7 +10,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .linalg import EPS, qr_inplace, svd_inplace, lq_rows_inplace, orth_inplace
+from .linalg import EPS, qr_inplace, qr_typed, svd_inplace, lq_rows_inplace, orth_inplace, orth_typed
 
 
 @dataclass
@@ -53,10 +53,10 @@ class LobpcgSvdKeep:
         self.lam = np.zeros(3 * r)
 
 
-def svd_rayl_ritz(CS, R_view, G_view, sigma, lam, r, side):
+def svd_rayl_ritz(CS, R_view, G_view, sigma, lam, r, side, orth_type="lapack"):
     """svdRaylRitz! (lobpcgSvd.jl:126-184)."""
     nS = CS.shape[1]
-    qr_inplace(CS, R_view)
+    qr_typed(CS, R_view, orth_type)
     R_work = R_view[:nS, :nS].copy()
     svd_inplace(R_work, sigma, G_view, ascending=(side != "L"))
     if side == "L":
@@ -138,26 +138,27 @@ def lobpcg_svd(C, X0, K, keep: LobpcgSvdKeep, ctl: LobpcgSvdControl, rng=None):
     else:
         rng = rng or np.random.default_rng()
         X[:, :] = rng.random(X.shape) + 1j * rng.random(X.shape)
-    qr_inplace(X)
+    ot = ctl.orth_type
+    qr_typed(X, None, ot)
     CX[:, :] = C.mul(X)
-    svd_rayl_ritz(CX, R_r, G_r_r, sigma, lam, r, side)
+    svd_rayl_ritz(CX, R_r, G_r_r, sigma, lam, r, side, ot)
     basis_update(X, CX, X, CX, R_r, G_r_r)
     residual(C, X, CX, P, lam_r, side)
     check_conv_svd(P, sigma, ctl.tol, side, ctl.normC, ctl.conv_range, ctl.conv_thresh_type)
     ldiv(P)
-    orth_inplace(X, P)
+    orth_typed(X, P, typ=ot)
     CP[:, :] = C.mul(P)
     for i in range(1, ctl.maxit + 1):
         if i == 1:
-            svd_rayl_ritz(CXP, R_2r, G_2r_2r, sigma, lam, r, side)
+            svd_rayl_ritz(CXP, R_2r, G_2r_2r, sigma, lam, r, side, ot)
             basis_update(XP, CXP, XP, CXP, R_2r, G_2r_2r)
         else:
-            svd_rayl_ritz(CS, R_3r, G_3r_3r, sigma, lam, r, side)
+            svd_rayl_ritz(CS, R_3r, G_3r_3r, sigma, lam, r, side, ot)
             basis_update(XP, CXP, S, CS, R_3r, G_3r_2r)
         residual(C, X, CX, W, lam_r, side)
         if check_conv_svd(W, sigma, ctl.tol, side, ctl.normC, ctl.conv_range, ctl.conv_thresh_type):
             return (sigma[0] if side == "S" else 1.0 / sigma[0]), i
         ldiv(W)
-        orth_inplace(XP, W)
+        orth_typed(XP, W, typ=ot)
         CW[:, :] = C.mul(W)
     return (sigma[0] if side == "S" else 1.0 / sigma[0]), ctl.maxit

@@ -1,7 +1,7 @@
-"""B200 σ_min(C − zI) grid engine — the psTriRecy hot path of kuandeng/rls on sm_100a.
+"""B200 σ_min(C − zI) grid engine — the psTriRecy / psPrecRecy hot path of kuandeng/rls on sm_100a.
 
 Public names mirror the reference (src/core/recuGrid.jl, src/core/psTriRecy.jl,
-src/core/lobpcgSvd.jl).  All per-grid-point work runs in librls_b200.so; there is
+src/core/psPrecRecy.jl, src/core/lobpcgSvd.jl).  All per-grid-point work runs in librls_b200.so; there is
 no CPU fallback.
 """
 import os as _os
@@ -16,7 +16,8 @@ from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_g
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
 from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
-                      SparseLLTP_AD, SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP)
+                      SparseLLTP_AD, SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP, PsPrecRecyControl,
+                      PsPrecRecyStats, PrecRecyRun, psPrecRecy)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
 
@@ -25,5 +26,6 @@ __all__ = [
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
     "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
     "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
-    "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException",
+    "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException", "PsPrecRecyControl",
+    "PsPrecRecyStats", "PrecRecyRun", "psPrecRecy",
 ]

@@ -46,6 +46,35 @@ class rls_lobpcg_control(C.Structure):
                 ("conv_thresh_type", C.c_int32), ("conv_first", C.c_int64), ("conv_last", C.c_int64)]
 
 
+class rls_psprecrecy_control(C.Structure):
+    _fields_ = [("tol", C.c_double), ("lobpcg_tol_scale", C.c_double), ("main_normC", C.c_double),
+                ("main_tau", C.c_double), ("shift", C.c_double), ("gap_tau", C.c_double),
+                ("recycle_fail_dist_thresh", C.c_double), ("tol_pred", C.c_double),
+                ("lobpcg_pred_tol_scale", C.c_double), ("pred_conv_first", C.c_int64), ("pred_conv_last", C.c_int64),
+                ("pred_tau", C.c_double), ("idx_cutoff_pred", C.c_double), ("pred_orth_type", C.c_int32),
+                ("_pad0", C.c_int32), ("pred_conv_thresh_type", C.c_int64), ("lambda_lower_min", C.c_double),
+                ("lambda_upper_max", C.c_double), ("r_main", C.c_int64), ("p_main", C.c_int64),
+                ("p_min_main", C.c_int64), ("main_implict_update", C.c_uint8), ("main_implict_recycle", C.c_uint8),
+                ("_pad1", C.c_uint8 * 6), ("r_pred", C.c_int64), ("p_pred", C.c_int64), ("p_min_pred", C.c_int64),
+                ("pred_implict_update", C.c_uint8), ("pred_implict_recycle", C.c_uint8), ("_pad2", C.c_uint8 * 6),
+                ("hsl_tol", C.c_double), ("hsl_cntl_1", C.c_double), ("hsl_cntl_2", C.c_double),
+                ("hsl_icntl_1", C.c_int64), ("hsl_icntl_2", C.c_int64), ("gamma_tol", C.c_double),
+                ("lambda_n_tol", C.c_double), ("inner_verbose_override", C.c_int64), ("collect_timing", C.c_uint8),
+                ("_pad3", C.c_uint8 * 7)]
+
+
+class rls_psprecrecy_stats(C.Structure):
+    _fields_ = [(f, C.POINTER(C.c_int64)) for f in ("p_count", "pred_p_count", "r_recy")] + \
+               [(f, C.POINTER(c64)) for f in ("pts", "pred_pts", "precond_rebuild_pts")] + \
+               [(f, C.POINTER(C.c_int64)) for f in ("main_M_vec_apps", "main_M_vec_apps_no_recycle", "main_L_vec_apps",
+                                                    "pred_M_vec_apps", "pred_L_vec_apps")] + \
+               [(f, C.c_uint64) for f in ("main_recycle_time_ns", "main_refine_time_ns", "main_update_time_ns",
+                                          "pred_recycle_time_ns", "pred_refine_time_ns", "pred_update_time_ns",
+                                          "precond_time_ns")] + \
+               [(f, C.c_int64) for f in ("n_it", "n_pred_it", "n_pts", "n_pred_pts", "n_precond_rebuild_pts")] + \
+               [(f, C.POINTER(C.c_int64)) for f in ("main_refine_it", "pred_refine_it")]
+
+
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 P = C.c_void_p
 
@@ -71,6 +100,7 @@ SIGNATURES = {
     "rls_pstrirecy_schur_range": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P,
                                             C.c_int64, C.c_int64, P, C.POINTER(rls_pstrirecy_stats)]),
     "rls_lobpcg_svd_invtri": (C.c_int, [P, c64, P, C.POINTER(rls_lobpcg_control), P, P, P, P]),
+    "rls_lobpcg_svd": (C.c_int, [P, C.c_int, c64, C.c_int, P, C.POINTER(rls_lobpcg_control), P, P, P, P]),
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_tsqr_r_noalloc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int, P, P]),
     "rls_sigma_grad": (C.c_int, [P, c64, P, C.c_int, P, P, P, P, P]),
@@ -88,6 +118,11 @@ SIGNATURES = {
     "rls_pstrirecy_schur_lanes_range": (C.c_int, [P, C.c_int, P, C.c_int64, C.POINTER(rls_grid),
                                                   C.POINTER(rls_pstrirecy_control), P, C.c_int64, C.c_int64, P,
                                                   C.POINTER(rls_pstrirecy_stats)]),
+    "rls_psprecrecy": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P, P, C.c_int64, C.POINTER(rls_grid),
+                                 C.POINTER(rls_psprecrecy_control), P, P, P, P, C.POINTER(rls_psprecrecy_stats)]),
+    "rls_psprecrecy_range": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P, P, C.c_int64, C.POINTER(rls_grid),
+                                       C.POINTER(rls_psprecrecy_control), P, P, P, C.c_int64, C.c_int64, P,
+                                       C.POINTER(rls_psprecrecy_stats)]),
     "rls_ctx_launches": (C.c_int64, [P]),
     "rls_ctx_set_ritz_basis": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_batch": (C.c_int, [P, C.c_int]),

@@ -125,6 +125,7 @@ enum {
   DEVERR_NONFINITE = 2,
   DEVERR_SIZE = 4,
   DEVERR_BREAKDOWN = 8,
+  DEVERR_POSDEF = 16,     // a Cholesky factorisation without a shift rule met a non-positive pivot
 };
 
 // Spin limit for dataflow waits: far above any legitimate wait (a wait of this

@@ -25,6 +25,7 @@
 #include "small.cuh"
 #include "sparse.cuh"
 #include "sptrsv.cuh"
+#include "pred.cuh"
 #include "host_err.h"
 
 namespace {
@@ -38,6 +39,9 @@ struct DevBuf {
 };
 
 }  // namespace
+
+struct PrecState;                 // psPrecRecy's run state (precrecy.cuh)
+void prec_state_delete(PrecState* s);
 
 struct rls_ctx {
   int device = 0;
@@ -170,6 +174,13 @@ struct rls_ctx {
     int epoch = 0;
     int64_t singular_at = 0;     // first 1-based index with a zero diagonal, 0 if none
   } lltp;
+
+  // psPrecRecy: the main recycled space above runs on the sparse C (op_sparse: the space's
+  // products M·V and Mᴴ·[J5 V] use the uploaded CSR instead of the Schur tiles); the
+  // prediction stage, the preconditioner and the run state live in `prec`.
+  bool op_sparse = false;
+  int scratch_cols = 0;            // minimum column count the shared scratch serves (setup_space)
+  PrecState* prec = nullptr;
 
   std::vector<DevBuf> owned;
 };
@@ -311,6 +322,10 @@ int sync_and_check(rls_ctx* ctx) {
     }
     if (h & DEVERR_NONFINITE) {
       set_err(ctx, "non-finite values in a device factorization (singular shifted factor?)");
+      return RLS_ERR_BREAKDOWN;
+    }
+    if (h & DEVERR_POSDEF) {
+      set_err(ctx, "PosDefException: a Gram matrix of the two-level preconditioner is not positive definite");
       return RLS_ERR_BREAKDOWN;
     }
     // DEVERR_BREAKDOWN: Cholesky needed its shift; reported but not fatal (the reference warns).
@@ -722,7 +737,7 @@ void release_space(rls_ctx* ctx) {
 }
 
 int setup_space(rls_ctx* ctx, int r, int p_max) {
-  if (ctx->r == r && ctx->p_max == p_max && ctx->V) {
+  if (ctx->r == r && ctx->p_max == p_max && ctx->V && ctx->small_dim >= std::max(ctx->scratch_cols, 1)) {
     ctx->p = 0;
     ctx->pts.assign(p_max, rls_c64{0, 0});
     return RLS_OK;
@@ -761,23 +776,23 @@ int setup_space(rls_ctx* ctx, int r, int p_max) {
   RET(dalloc_t(ctx, &ctx->Rk, (size_t)9 * r * r));
   RET(dalloc_t(ctx, &ctx->sig, (size_t)3 * r));
   RET(dalloc_t(ctx, &ctx->lam, (size_t)3 * r));
-  ctx->tall_tmp_cols = std::max(prm, 2 * r);
+  ctx->tall_tmp_cols = std::max(std::max(prm, 2 * r), ctx->scratch_cols);
   RET(dalloc_t(ctx, &ctx->tall_tmp, (size_t)np * ctx->tall_tmp_cols));
-  const int kmax = std::max(prm, 3 * r);
+  const int kmax = std::max(std::max(prm, 3 * r), ctx->scratch_cols);
   ctx->gram_part_elems = (size_t)((np + 63) / 64) * kmax * 32;
   RET(dalloc_t(ctx, &ctx->gram_part, ctx->gram_part_elems));
   ctx->tsqr_stack_elems = (size_t)((np + 63) / 64 + 2) * 64 * 64;
   RET(dalloc_t(ctx, &ctx->tsqr_stack[0], ctx->tsqr_stack_elems));
   RET(dalloc_t(ctx, &ctx->tsqr_stack[1], ctx->tsqr_stack_elems));
-  RET(dalloc_t(ctx, &ctx->house_tau, (size_t)2 * prm + 64));
+  RET(dalloc_t(ctx, &ctx->house_tau, (size_t)2 * kmax + 64));
   ctx->small_dim = kmax;
   for (int i = 0; i < 8; ++i) RET(dalloc_t(ctx, &ctx->small[i], (size_t)kmax * std::max(kmax, 64) + 64));
-  RET(dalloc_t(ctx, &ctx->owW, (size_t)prm * 8 + 64));
+  RET(dalloc_t(ctx, &ctx->owW, (size_t)kmax * 64 + 64));
   RET(dalloc_t(ctx, &ctx->owR, (size_t)64 * 64));
-  RET(dalloc_t(ctx, &ctx->svdA, (size_t)prm * prm));
-  RET(dalloc_t(ctx, &ctx->svdV, (size_t)prm * prm));
-  ctx->gemm_tmp_cols = 64;
-  RET(dalloc_t(ctx, &ctx->gemm_tmp, (size_t)np * 64));
+  RET(dalloc_t(ctx, &ctx->svdA, (size_t)kmax * kmax));
+  RET(dalloc_t(ctx, &ctx->svdV, (size_t)kmax * kmax));
+  ctx->gemm_tmp_cols = ctx->scratch_cols > 64 ? 128 : 64;
+  RET(dalloc_t(ctx, &ctx->gemm_tmp, (size_t)np * ctx->gemm_tmp_cols));
   {  // speculative batch workspaces (BATCH_MAX points)
     const size_t BM = BATCH_MAX;
     RET(dalloc_t(ctx, &ctx->bz, BM));
@@ -916,6 +931,8 @@ __global__ void k_conj_transpose(int m, int n, const cplx* A, int lda, cplx* B, 
   }
 }
 
+int spmm_dev(rls_ctx* ctx, cplx s, int adj, int b, const cplx* X, int64_t ldx, cplx* Y, int64_t ldy);
+
 int add_blocks(rls_ctx* ctx, const cplx* Xin, cplx z) {  // _add_blocks! (recySpace.jl:344-453)
   const int p = ctx->p, r = ctx->r, pr = p * r;
   const int64_t np = ctx->n_pad;
@@ -939,12 +956,18 @@ int add_blocks(rls_ctx* ctx, const cplx* Xin, cplx z) {  // _add_blocks! (recySp
                          cudaMemcpyDeviceToDevice, ctx->stream));
   }
   // J5 = M V_new; [J1 J2] = Mᴴ [J5 V_new]   (mul_coupled_ms!, recySpace.jl:368-380)
-  RET(trmm(ctx, 0, Vn, J5n, np, r));
-  RET(copy_cols(ctx, J5n, ctx->tall_tmp, r));
-  RET(copy_cols(ctx, Vn, ctx->tall_tmp + (int64_t)r * np, r));
-  RET(trmm(ctx, 1, ctx->tall_tmp, ctx->tall_tmp, np, 2 * r));
-  RET(copy_cols(ctx, ctx->tall_tmp, J1n, r));
-  RET(copy_cols(ctx, ctx->tall_tmp + (int64_t)r * np, J2n, r));
+  if (ctx->op_sparse) {          // M = C sparse (psPrecRecy's main stage, psPrecRecy.jl:642-644)
+    RET(spmm_dev(ctx, czero(), 0, r, Vn, np, J5n, np));
+    RET(spmm_dev(ctx, czero(), 1, r, J5n, np, J1n, np));
+    RET(spmm_dev(ctx, czero(), 1, r, Vn, np, J2n, np));
+  } else {
+    RET(trmm(ctx, 0, Vn, J5n, np, r));
+    RET(copy_cols(ctx, J5n, ctx->tall_tmp, r));
+    RET(copy_cols(ctx, Vn, ctx->tall_tmp + (int64_t)r * np, r));
+    RET(trmm(ctx, 1, ctx->tall_tmp, ctx->tall_tmp, np, 2 * r));
+    RET(copy_cols(ctx, ctx->tall_tmp, J1n, r));
+    RET(copy_cols(ctx, ctx->tall_tmp + (int64_t)r * np, J2n, r));
+  }
   // H blocks (recySpace.jl:392-417)
   RET(gram(ctx, np, Vn, np, r, J1n, np, r, ctx->H1 + (int64_t)pr * ld + pr, ld));
   RET(gram(ctx, np, Vn, np, r, J2n, np, r, ctx->H2 + (int64_t)pr * ld + pr, ld));
@@ -1293,6 +1316,8 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_blockrot_coeffs, optin));
   RET(allow_big_smem(ctx, k_chol_inv, optin));
   RET(allow_big_smem(ctx, k_trtri, optin));
+  RET(allow_big_smem(ctx, k_blockrot_apply_g, optin));
+  RET(allow_big_smem(ctx, k_blockrot_left_g, optin));
   return RLS_OK;
 }
 
@@ -1367,6 +1392,8 @@ extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->owned) cudaFree(b.p);
   ctx->owned.clear();
+  prec_state_delete(ctx->prec);
+  ctx->prec = nullptr;
   ctx->T_buf.reset();
   ctx->T = nullptr;
   if (ctx->wait_ev) cudaEventDestroy(ctx->wait_ev);
@@ -1406,6 +1433,7 @@ int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<c
     dfree(ctx, q);
   ctx->grad_ws = nullptr;
   release_space(ctx);
+  ctx->op_sparse = false;
   ctx->n = n;
   ctx->nb = (int)((n + TILE - 1) / TILE);
   ctx->n_pad = (int64_t)ctx->nb * TILE;
@@ -1679,6 +1707,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
   rls_pstrirecy_stats dummy{};
   if (!st) st = &dummy;
   if (i_begin == 0) {
+    ctx->op_sparse = false;     // the space's products use the Schur tiles
     RET(setup_space(ctx, r, (int)ctl->p));
     RET(upload_x0(ctx, X0, r));
     // recycle_fail_dist_thresh (recySpace.jl:22-38)
@@ -2698,5 +2727,6 @@ extern "C" int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int 
   return RLS_OK;
 }
 
+#include "precrecy.cuh"
 #include "../../include/rls_b200_testing.h"
 #include "testing.cuh"

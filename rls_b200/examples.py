@@ -100,3 +100,34 @@ def ic_factor_banded(n: int, band: int, fill: float, seed: int, complex_values: 
     off = sp.csr_matrix((v, (r, c)), shape=(n, n), dtype=np.complex128)
     diag = 1.0 + np.asarray(abs(off).sum(axis=1)).ravel()
     return (off + sp.diags(diag.astype(np.complex128))).tocsc()
+
+
+AF23560_NORMC = 645.74                                 # af23560_psPrecRecy.jl (normC of af23560.jl)
+AF23560_GRID = dict(x_st=-1.6, x_ed=0.8, y_st=-1.55, y_ed=1.55, n_x=200, n_y=200, k=20)
+
+
+def af23560_shaped(n: int = 23560, per_row: int = 20, half_width: int = 300, normC: float = AF23560_NORMC,
+                   seed: int = SEED) -> sp.csc_matrix:
+    """Synthetic stand-in for the af23560 matrix of example/af23560/af23560.jl (not distributed):
+    real unsymmetric, `per_row` − 1 off-diagonal N(0,1) entries per row at uniform offsets within
+    ±`half_width` of the diagonal (coinciding entries summed), and a weakly dominant diagonal
+    d_i = Σ_j |c_ij| over the row, so that the spectrum lies in the closed right half-plane and
+    reaches towards the origin, where the af23560 grid [-1.6, 0.8] × [-1.55, 1.55] sits.  The
+    whole matrix is scaled to ‖C‖₂ = normC (largest singular value by ARPACK).  complex128 CSC
+    with sorted indices."""
+    import scipy.sparse.linalg as spla
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n, dtype=np.int64), per_row - 1)
+    off = rng.integers(1, half_width + 1, size=rows.size) * np.where(rng.random(rows.size) < 0.5, -1, 1)
+    cols = rows + off
+    ok = (cols >= 0) & (cols < n)
+    rows, cols = rows[ok], cols[ok]
+    vals = rng.standard_normal(rows.size)
+    B = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    B.sum_duplicates()
+    d = np.asarray(abs(B).sum(axis=1)).ravel()
+    A = (B + sp.diags(d)).tocsc()
+    s1 = spla.svds(A, k=1, return_singular_vectors=False, random_state=seed)[0]
+    C = (A * (normC / s1)).astype(np.complex128).tocsc()
+    C.sort_indices()
+    return C

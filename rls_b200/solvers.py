@@ -302,6 +302,27 @@ class Engine:
                                           C.byref(s), C.byref(it)), self._h)
         return s.value, it.value, X, sr
 
+    OPS = {"inv_schur": 0, "shifted": 1, "pred": 2, "inv_l": 3}
+
+    def lobpcg_svd(self, op: str, z: complex, control: LobpcgSvdControl, prec: str = None, X0=None):
+        """lobpcgSvd(C, X0, K, keep, control) (lobpcgSvd.jl:365-477) on one of the context's
+        operators: "inv_schur" InvMat(adjoint(T − zI)), "shifted" ShiftedMat(C, −z), "pred"
+        ShiftedMat(C, −z)·invF, "inv_l" InvMat(L); K = None or "lltp" (the uploaded SparseLLTP).
+        Returns (σ, it, X = keep.S[:, 1:r], keep.σ[1:r])."""
+        r = control.r
+        n = control.n
+        x0 = None
+        if X0 is not None:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128).reshape(n, -1))
+        X = np.zeros((n, r), dtype=np.complex128, order="F")
+        sr = np.zeros(r)
+        s = C.c_double()
+        it = C.c_int64()
+        cc = control.c_struct()
+        check(lib().rls_lobpcg_svd(self._h, self.OPS[op], c64(z.real, z.imag), 0 if prec is None else 1, ptr(x0),
+                                   C.byref(cc), ptr(X), ptr(sr), C.byref(s), C.byref(it)), self._h)
+        return s.value, it.value, X, sr
+
     def sparse_upload(self, C):
         """Uploads a sparse C (SciPy sparse, any format) for spmm_shifted / ShiftedMat."""
         import scipy.sparse as sp
@@ -670,6 +691,204 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
             io.write("Total refine time for singular value problem: %.6f seconds\n" % (st.refine_time_ns / 1e9))
             io.write("Total update time for singular value problem: %.6f seconds\n" % (st.update_time_ns / 1e9))
         io.write(f"Total R vec apps for singular value problem: {int(st.R_vec_apps.sum())}\n")
+        io.write(f"Total it for singular value problem: {st.n_it}\n")
+        io.write(f"Total pt for singular value problem: {st.n_pts}\n")
+    return sigma, st
+
+
+# ---- psPrecRecy (src/core/psPrecRecy.jl) -------------------------------------------------------
+
+@dataclass
+class PsPrecRecyControl:
+    """psPrecRecy.jl:220-261 (same fields, same defaults; shift = main_normC²·eps·100).  The Greek
+    field names λ_lower_min, λ_upper_max, γ_tol and λ_n_tol are spelt lambda_lower_min,
+    lambda_upper_max, gamma_tol and lambda_n_tol; pred_orth_type is "lapack" or "shiftchol" for
+    the Symbols :lapack / :shiftchol; pred_conv_range is None or a 1-based (first, last)."""
+    tol: float = 1e-3
+    lobpcg_tol_scale: float = 0.1
+    main_normC: float = 10.0
+    main_tau: float = 1.666
+    shift: float = None
+    gap_tau: float = 1e-10
+    recycle_fail_dist_thresh: float = float("nan")
+    tol_pred: float = 1e-3
+    lobpcg_pred_tol_scale: float = 1.0
+    pred_conv_range: tuple = None
+    pred_tau: float = 1.666
+    idx_cutoff_pred: float = 1e-2
+    pred_orth_type: str = "lapack"
+    pred_conv_thresh_type: int = 0
+    lambda_lower_min: float = 0.1
+    lambda_upper_max: float = 30.0
+    r_main: int = 6
+    p_main: int = 60
+    p_min_main: int = 1
+    main_implict_update: bool = False
+    main_implict_recycle: bool = False
+    r_pred: int = 20
+    p_pred: int = 20
+    p_min_pred: int = 1
+    pred_implict_update: bool = True
+    pred_implict_recycle: bool = True
+    hsl_tol: float = 1e-3
+    hsl_cntl_1: float = 1e-6
+    hsl_cntl_2: float = 1e-5
+    hsl_icntl_1: int = 200
+    hsl_icntl_2: int = 200
+    gamma_tol: float = 1e-3
+    lambda_n_tol: float = 1e-3
+    inner_verbose_override: int = None
+    collect_timing: bool = True
+
+    def __post_init__(self):
+        if self.shift is None:
+            self.shift = self.main_normC ** 2 * EPS * 100
+        if self.pred_orth_type not in ("lapack", "shiftchol"):
+            raise ArgumentError(-1, f"pred_orth_type={self.pred_orth_type} must be :lapack or :shiftchol")
+
+    def c_struct(self) -> "rls_psprecrecy_control":
+        from ._lib import rls_psprecrecy_control
+        c = rls_psprecrecy_control()
+        for f in ("tol", "lobpcg_tol_scale", "main_normC", "main_tau", "shift", "gap_tau", "recycle_fail_dist_thresh",
+                  "tol_pred", "lobpcg_pred_tol_scale", "pred_tau", "idx_cutoff_pred", "lambda_lower_min",
+                  "lambda_upper_max", "hsl_tol", "hsl_cntl_1", "hsl_cntl_2", "gamma_tol", "lambda_n_tol"):
+            setattr(c, f, float(getattr(self, f)))
+        for f in ("pred_conv_thresh_type", "r_main", "p_main", "p_min_main", "r_pred", "p_pred", "p_min_pred",
+                  "hsl_icntl_1", "hsl_icntl_2"):
+            setattr(c, f, int(getattr(self, f)))
+        for f in ("main_implict_update", "main_implict_recycle", "pred_implict_update", "pred_implict_recycle",
+                  "collect_timing"):
+            setattr(c, f, int(bool(getattr(self, f))))
+        if self.pred_conv_range is None:
+            c.pred_conv_first, c.pred_conv_last = -1, -1
+        else:
+            c.pred_conv_first, c.pred_conv_last = int(self.pred_conv_range[0]), int(self.pred_conv_range[1])
+        c.pred_orth_type = 0 if self.pred_orth_type == "lapack" else 1
+        c.inner_verbose_override = -1 if self.inner_verbose_override is None else int(self.inner_verbose_override)
+        return c
+
+
+class PsPrecRecyStats:
+    """psPrecRecy.jl:318-350 (+ main_refine_it, pred_refine_it: LOBPCG iterations per point)."""
+    _I = ("p_count", "pred_p_count", "r_recy", "main_M_vec_apps", "main_M_vec_apps_no_recycle", "main_L_vec_apps",
+          "pred_M_vec_apps", "pred_L_vec_apps", "main_refine_it", "pred_refine_it")
+    _Z = ("pts", "pred_pts", "precond_rebuild_pts")
+    _S = ("main_recycle_time_ns", "main_refine_time_ns", "main_update_time_ns", "pred_recycle_time_ns",
+          "pred_refine_time_ns", "pred_update_time_ns", "precond_time_ns", "n_it", "n_pred_it", "n_pts", "n_pred_pts",
+          "n_precond_rebuild_pts")
+
+    def __init__(self, nZ):
+        for f in self._I:
+            setattr(self, f, np.zeros(nZ, dtype=np.int64))
+        for f in self._Z:
+            setattr(self, f, np.zeros(nZ, dtype=np.complex128))
+        for f in self._S:
+            setattr(self, f, 0)
+
+    def c_struct(self):
+        from ._lib import rls_psprecrecy_stats
+        c = rls_psprecrecy_stats()
+        for f in self._I:
+            setattr(c, f, getattr(self, f).ctypes.data_as(C.POINTER(C.c_int64)))
+        for f in self._Z:
+            setattr(c, f, getattr(self, f).ctypes.data_as(C.POINTER(c64)))
+        return c
+
+    def read_scalars(self, c):
+        for f in self._S:
+            setattr(self, f, int(getattr(c, f)))
+
+
+class PrecRecyRun:
+    """One psPrecRecy run on an Engine, resumable over index ranges (rls_psprecrecy_range)."""
+
+    def __init__(self, engine: Engine, C_, rec: Recursion, control: PsPrecRecyControl, p=None, X0_main=None,
+                 X0_pred=None, X0_bound=None):
+        import scipy.sparse as sp
+        A = sp.csc_matrix(C_, dtype=np.complex128)
+        A.sum_duplicates()
+        A.sort_indices()
+        n = A.shape[0]
+        if A.shape != (n, n):
+            raise DimensionMismatch(-2, f"psPrecRecy needs a square C, got size {A.shape}")
+        self.e, self.rec, self.control, self.n = engine, rec, control, n
+        self.colptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        self.rowval = np.ascontiguousarray(A.indices, dtype=np.int64)
+        self.nzval = np.ascontiguousarray(A.data, dtype=np.complex128)
+        self.p = None if p is None else np.ascontiguousarray(p, dtype=np.int64)
+        if self.p is not None and self.p.shape != (n,):
+            raise DimensionMismatch(-2, f"p has length {self.p.size}, expected {n}")
+
+        def block(X, k, name):
+            if X is None:
+                return None
+            X = np.asfortranarray(np.asarray(X, dtype=np.complex128).reshape(n, -1))
+            if X.shape != (n, k):
+                raise DimensionMismatch(-2, f"{name} must be {(n, k)}, got {X.shape}")
+            return X
+        self.x0 = (block(X0_main, control.r_main, "X0_main"), block(X0_pred, control.r_pred, "X0_pred"),
+                   block(X0_bound, 1, "X0_bound"))
+        self.Z = _checked(rec.Z, np.complex128, 0, "rec.Z")
+        nZ = len(self.Z)
+        self.sigma = np.full(nZ, np.nan)
+        self.st = PsPrecRecyStats(nZ)
+        self._cst = self.st.c_struct()
+        self._cc = control.c_struct()
+        self._g = rec.c_grid()
+
+    def run(self, i_begin=0, i_end=None):
+        i_end = len(self.Z) if i_end is None else i_end
+        a, b, c = self.x0
+        check(lib().rls_psprecrecy_range(self.e._h, self.n, ptr(self.colptr), ptr(self.rowval), ptr(self.nzval), 0,
+                                         ptr(self.p), ptr(self.Z), len(self.Z), C.byref(self._g), C.byref(self._cc),
+                                         ptr(a), ptr(b), ptr(c), int(i_begin), int(i_end), ptr(self.sigma),
+                                         C.byref(self._cst)), self.e._h)
+        self.st.read_scalars(self._cst)
+        return self.sigma, self.st
+
+
+def psPrecRecy(C_, rec: Recursion, control: PsPrecRecyControl = None, verbose: int = 1, io=None, p=None,
+               X0_main=None, X0_pred=None, X0_bound=None, device: int = 0):
+    """psPrecRecy (psPrecRecy.jl:617-623; a dense C is made sparse, :1036-1042) →
+    (σ_min in rec.Z order, PsPrecRecyStats).
+
+    ``p`` is the column order the reference takes from SPQR (``qr(C).cpiv``, :625), which needs
+    SuiteSparse; None here takes reverse Cuthill–McKee of C + Cᵀ as the stand-in fill-reducing
+    order.  ``X0_main`` (n × r_main), ``X0_pred`` (n × r_pred) and ``X0_bound`` (n × 1) stand in
+    for the reference's rand! draws; None draws fixed uniform [0,1) blocks on the device.
+    """
+    import scipy.sparse as sp
+    control = control or PsPrecRecyControl()
+    io = io if io is not None else sys.stdout
+    A = sp.csc_matrix(C_, dtype=np.complex128)
+    if p is None:
+        from scipy.sparse.csgraph import reverse_cuthill_mckee
+        S = abs(A) + abs(A.T)
+        p = np.ascontiguousarray(reverse_cuthill_mckee(S.tocsr(), symmetric_mode=True), dtype=np.int64)
+    if verbose >= 1:
+        io.write("[psPrecRecy] rec: x_range=[%.6f, %.6f], y_range=[%.6f, %.6f], n_x=%d, n_y=%d, k=%d, n_pts=%d\n"
+                 % (rec.x_st, rec.x_ed, rec.y_st, rec.y_ed, rec.n_x, rec.n_y, rec.k, rec.n_x * rec.n_y))
+        io.write("[psPrecRecy] control:\n")
+        for f in control.__dataclass_fields__:
+            io.write(f"  {f} = {getattr(control, f)!r}\n")
+    eng = _engine(device)
+    if verbose >= 1:
+        eng.set_log(lambda line: io.write(line + "\n"), verbose)
+    else:
+        eng.set_log(None)
+    try:
+        run = PrecRecyRun(eng, A, rec, control, p=p, X0_main=X0_main, X0_pred=X0_pred, X0_bound=X0_bound)
+        sigma, st = run.run()
+    finally:
+        eng.set_log(None)
+    if verbose >= 1:
+        io.write(f"Total M vec apps for pred singular value problem: {int(st.pred_M_vec_apps.sum())}\n")
+        io.write(f"Total L vec apps for pred singular value problem: {int(st.pred_L_vec_apps.sum())}\n")
+        io.write(f"Total it for pred singular value problem: {st.n_pred_it}\n")
+        io.write(f"Total pt for pred singular value problem: {st.n_pred_pts}\n")
+        io.write(f"Total preconditioner points: {st.n_precond_rebuild_pts}\n")
+        io.write(f"Total M vec apps for singular value problem: {int(st.main_M_vec_apps.sum())}\n")
+        io.write(f"Total L vec apps for singular value problem: {int(st.main_L_vec_apps.sum())}\n")
         io.write(f"Total it for singular value problem: {st.n_it}\n")
         io.write(f"Total pt for singular value problem: {st.n_pts}\n")
     return sigma, st
