@@ -71,7 +71,11 @@ typedef struct {
 
 /* Mirrors `PsTriRecyStats` (src/core/psTriRecy.jl:257-272).  Array members are
  * caller-allocated with length nZ and may be NULL; refine_it is an addition
- * (LOBPCG iterations per point, 0 when the point was recycled). */
+ * (LOBPCG iterations per point, 0 when the point was recycled), and so are the trailing
+ * dsdx and dsdy: ∂σ/∂Re z and ∂σ/∂Im z at every point from the point's own singular pair
+ * (the accepted Ritz pair of a recycled point; LOBPCG's converged pair of a refined one),
+ * −Re(uᴴv) and Im(uᴴv) with u = (T − zI)v/σ.  Their accuracy is first order in the residual
+ * the solver accepted; rls_sigma_grad refines one point further. */
 typedef struct {
   int64_t* p_count;
   int64_t* r_recy;
@@ -89,6 +93,8 @@ typedef struct {
   uint8_t _pad0[7];
   int64_t n_it;
   int64_t n_pts;
+  double* dsdx;
+  double* dsdy;
 } rls_pstrirecy_stats;
 
 /* Mirrors `LobpcgSvdControl` (src/core/lobpcgSvd.jl:1-13).  orth_type: 0 =
@@ -435,6 +441,18 @@ int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colptr, const i
  * Re(conj((Qu)_i) (Qv)_j).  Host memory. */
 int rls_sigma_grad(rls_ctx* ctx, rls_c64 z, const rls_c64* v0, int refine_steps, double* sigma,
                    double* dsdx, double* dsdy, rls_c64* u_out, rls_c64* v_out);
+
+/* Uploads the Schur vectors Q of C = Q T Qᴴ (n × n, column-major, leading dimension ldq; host
+ * memory) to the context that holds T, for rls_sigma_grad_pattern.  No reference counterpart. */
+int rls_set_schur_vectors(rls_ctx* ctx, const rls_c64* Q, int64_t ldq);
+
+/* ∂σ/∂C_ij = Re(conj((Qu)_i)·(Qv)_j) on the nnz index pairs (rows[k], cols[k]) (base 0 or 1) of
+ * a sparsity pattern, from the Schur-basis singular pair u, v of T − zI (host vectors of n
+ * values, e.g. rls_sigma_grad's u_out and v_out), on the device: Q·[u v] against the uploaded
+ * Q, then one gather per nonzero.  dsdC (nnz values, host) receives the gradient.  No
+ * counterpart in the reference. */
+int rls_sigma_grad_pattern(rls_ctx* ctx, const rls_c64* u, const rls_c64* v, int64_t nnz, const int64_t* rows,
+                           const int64_t* cols, int base, double* dsdC);
 
 /* ---- allocation-free utility ---------------------------------------------------- */
 

@@ -37,7 +37,7 @@ class rls_pstrirecy_stats(C.Structure):
                 ("preprocess_time_ns", C.c_uint64), ("recycle_time_ns", C.c_uint64), ("qr_time_ns", C.c_uint64),
                 ("refine_time_ns", C.c_uint64), ("update_time_ns", C.c_uint64),
                 ("mv_stats_available", C.c_uint8), ("_pad0", C.c_uint8 * 7), ("n_it", C.c_int64),
-                ("n_pts", C.c_int64)]
+                ("n_pts", C.c_int64), ("dsdx", C.POINTER(C.c_double)), ("dsdy", C.POINTER(C.c_double))]
 
 
 class rls_lobpcg_control(C.Structure):
@@ -104,6 +104,8 @@ SIGNATURES = {
     "rls_ctx_stream": (C.c_void_p, [P]),
     "rls_tsqr_r_noalloc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int, P, P]),
     "rls_sigma_grad": (C.c_int, [P, c64, P, C.c_int, P, P, P, P, P]),
+    "rls_set_schur_vectors": (C.c_int, [P, P, C.c_int64]),
+    "rls_sigma_grad_pattern": (C.c_int, [P, P, P, C.c_int64, P, P, C.c_int, P]),
     "rls_sparse_upload_csc": (C.c_int, [P, C.c_int64, C.c_int64, P, P, P, C.c_int]),
     "rls_spmm_shifted": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),
     "rls_spmm_shifted_dev": (C.c_int, [P, c64, C.c_int, C.c_int, P, C.c_int64, P, C.c_int64]),

@@ -242,3 +242,25 @@ __global__ void k_batch_w0(BatchDesc d) {
   s = block_sum(s, red);
   if (threadIdx.x == 0) d.w0sq[b] = batch_ok(d, b) ? s : -1.0;
 }
+
+// Quadratic form q_b = g_bᴴ·H2·g_b of each point's leading Ritz coefficient vector g_b =
+// G_total_b[:, 0] (pr values, ld pr, point b at G + b·gstride) with the space's
+// H2 = J5ᴴV (pr × pr, ld ldh).  vᴴ(M − zS)v of the recycled singular vector v = V·g_b is
+// conj(q_b) − z (Vᴴ J5 = H2ᴴ, ‖v‖ = 1): the gradient of σ with respect to z at recycled
+// points.  One CTA per point, deterministic.
+__global__ void k_batch_quad(int pr, const cplx* __restrict__ G, int64_t gstride, const cplx* __restrict__ H2,
+                             int ldh, const int* __restrict__ rr, cplx* out) {
+  __shared__ cplx red[32];
+  const int b = blockIdx.x;
+  const cplx* g = G + (int64_t)b * gstride;
+  cplx s = czero();
+  if (!rr || (rr[b] >= 1 && rr[b] <= BATCH_KMAX)) {
+    for (int i = threadIdx.x; i < pr; i += blockDim.x) {
+      cplx hg = czero();
+      for (int j = 0; j < pr; ++j) hg = cfma(H2[(int64_t)j * ldh + i], g[j], hg);
+      s = cfmac(g[i], hg, s);
+    }
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[b] = s;
+}

@@ -143,6 +143,8 @@ struct rls_ctx {
   size_t heev_smem_avail = 0;      // dynamic shared memory k_heev_rr may use
   // speculative batched recycle (rls_ctx_set_batch)
   int spec_max = 16, spec_cur = 8;
+  bool grad_on = false;            // the current run writes ∂σ/∂z per point (stats dsdx/dsdy)
+  cplx* bquad = nullptr;           // BATCH_MAX: g_bᴴ·H2·g_b of the batched recycle steps
   cplx *bz = nullptr, *bG = nullptr, *bheevA = nullptr, *bczx = nullptr, *bstack0 = nullptr, *bstack1 = nullptr;
   cplx *bRb = nullptr, *bG2 = nullptr, *bGtot = nullptr, *bXW = nullptr;
   double *btau = nullptr, *bheevLU = nullptr, *bsig = nullptr, *bcolpart = nullptr, *bw0 = nullptr;
@@ -721,7 +723,8 @@ void release_space(rls_ctx* ctx) {
                    &ctx->Ulist, &ctx->heev.A, &ctx->Gheev, &ctx->CzX, &ctx->Gtot, &ctx->S, &ctx->CS, &ctx->Gk,
                    &ctx->Rk, &ctx->tall_tmp, &ctx->gram_part, &ctx->tsqr_stack[0], &ctx->tsqr_stack[1],
                    &ctx->house_tau, &ctx->zdev, &ctx->owW, &ctx->owR, &ctx->svdA, &ctx->svdV, &ctx->gemm_tmp, &ctx->bz, &ctx->bG, &ctx->bheevA,
-                   &ctx->bczx, &ctx->bstack0, &ctx->bstack1, &ctx->bRb, &ctx->bG2, &ctx->bGtot, &ctx->bXW};
+                   &ctx->bczx, &ctx->bstack0, &ctx->bstack1, &ctx->bRb, &ctx->bG2, &ctx->bGtot, &ctx->bXW,
+                   &ctx->bquad};
   for (cplx** b : bufs) { dfree(ctx, *b); *b = nullptr; }
   double** dbufs[] = {&ctx->heev.lu, &ctx->lam_dev, &ctx->taudev, &ctx->sig_rec, &ctx->sig, &ctx->lam,
                       &ctx->btau, &ctx->bheevLU, &ctx->bsig, &ctx->bcolpart, &ctx->bw0};
@@ -813,6 +816,7 @@ int setup_space(rls_ctx* ctx, int r, int p_max) {
     RET(dalloc_t(ctx, &ctx->bXW, BM * 2 * np * r));
     RET(dalloc_t(ctx, &ctx->bcolpart, BM * (np / 32 + 1)));
     RET(dalloc_t(ctx, &ctx->bw0, BM));
+    RET(dalloc_t(ctx, &ctx->bquad, BM));
   }
   return RLS_OK;
 }
@@ -1056,6 +1060,7 @@ struct RecycleResult {
   int rr;
   double sigma0;
   double w0norm;
+  cplx quad;      // g₁ᴴ·H2·g₁ of the leading Ritz vector (when ctx->grad_on)
 };
 
 int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResult* out) {
@@ -1122,8 +1127,19 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
   prof_end(ctx, KP_RECYCLE_GEMM, e0g, 16.0 * ((double)ctx->n * pr * 4 + 2.0 * ctx->n * r));
   k_sum<<<1, 256, 0, ctx->stream>>>(ctx->colpart, nparts, ctx->dscal);
   RET(check_launch(ctx, "k_sum"));
+  if (ctx->grad_on) {
+    k_batch_quad<<<1, 256, 0, ctx->stream>>>(pr, ctx->Gtot, 0, ctx->H2, ctx->pr_max, nullptr, ctx->bquad);
+    RET(check_launch(ctx, "k_batch_quad"));
+  }
   double w2 = 0.0, s0 = 0.0;
-  RET(d2h2(ctx, &w2, ctx->dscal, 1, &s0, ctx->sig_rec, 1));
+  out->quad = czero();
+  {
+    D2HBatch rd(ctx);
+    RET(rd.add(&w2, ctx->dscal, 1));
+    RET(rd.add(&s0, ctx->sig_rec, 1));
+    if (ctx->grad_on) RET(rd.add(&out->quad, ctx->bquad, 1));
+    RET(rd.finish());
+  }
   out->rr = rr;
   out->sigma0 = s0;
   out->w0norm = std::sqrt(w2);
@@ -1134,7 +1150,7 @@ int recycle_step(rls_ctx* ctx, cplx z, double shift, double gap_tau, RecycleResu
 // return rr[b] (0 when the batch path skipped the point: Ritz dimension > BATCH_KMAX),
 // sig0[b] and w0[b] = |W_b[:,1]| for b < B; X_b, W_b stay in ctx->bXW.
 int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, double shift, int* rr, double* sig0,
-                  double* w0) {
+                  double* w0, cplx* quad) {
   const int r = ctx->r, pr = ctx->p * r;
   const int64_t np = ctx->n_pad;
   CK(cudaMemcpyAsync(ctx->bz, zs, sizeof(cplx) * B, cudaMemcpyHostToDevice, ctx->stream));
@@ -1208,12 +1224,18 @@ int recycle_batch(rls_ctx* ctx, int B, const cplx* zs, const double* taus, doubl
   prof_end(ctx, KP_RECYCLE_GEMM, e1, B * 16.0 * ((double)ctx->n * pr * 6 + 2.0 * ctx->n * r));
   k_batch_w0<<<B, 256, 0, ctx->stream>>>(d);
   RET(check_launch(ctx, "k_batch_w0"));
+  if (ctx->grad_on && quad) {
+    k_batch_quad<<<B, 256, 0, ctx->stream>>>(pr, ctx->bGtot, (int64_t)ctx->pr_max * r, ctx->H2, ctx->pr_max,
+                                             ctx->brr, ctx->bquad);
+    RET(check_launch(ctx, "k_batch_quad"));
+  }
   std::vector<double> hs((size_t)B * BATCH_KMAX), hw0(B);
   {
     D2HBatch rd(ctx);
     RET(rd.add(rr, ctx->brr, (size_t)B));
     RET(rd.add(hs.data(), ctx->bsig, (size_t)B * BATCH_KMAX));
     RET(rd.add(hw0.data(), ctx->bw0, (size_t)B));
+    if (ctx->grad_on && quad) RET(rd.add(quad, ctx->bquad, (size_t)B));
     RET(rd.finish());
   }
   for (int b = 0; b < B; ++b) {
@@ -1736,10 +1758,20 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     return RLS_ERR_STATE;
   }
   const double lob_tol = ctl->lobpcg_tol_scale * ctl->tol;
+  ctx->grad_on = st->dsdx || st->dsdy;
   auto thresh_ok = [&](double w0, double s0) {   // _residual_norm_ok (psTriRecy.jl:237-245)
     return w0 < ctl->normC * std::max(s0 * ctl->tol, ctl->normC * std::sqrt(2.0) * kEps);
   };
-  auto accept = [&](int64_t i, double s0, int r_svdrr) {
+  // ∂σ/∂z at a recycled point from q = gᴴH2g: vᴴ(T − zI)v = conj(q) − z, uᴴv = conj(vᴴRv)/σ
+  auto grad_recycled = [&](int64_t i, double s0, cplx q) {
+    if (!ctx->grad_on) return;
+    const double re = q.x - Z[i].re, im = -q.y - Z[i].im;       // vᴴ R v
+    const double gx = (s0 > 0.0) ? -re / s0 : 0.0, gy = (s0 > 0.0) ? -im / s0 : 0.0;
+    if (st->dsdx) st->dsdx[i] = gx;
+    if (st->dsdy) st->dsdy[i] = gy;
+  };
+  auto accept = [&](int64_t i, double s0, int r_svdrr, cplx q) {
+    grad_recycled(i, s0, q);
     sigma_min[i] = s0;
     if (st->M_vec_apps) st->M_vec_apps[i] = 0;
     if (st->M_vec_apps_no_recycle) st->M_vec_apps_no_recycle[i] = 0;
@@ -1756,7 +1788,15 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     LobpcgResult lres{};
     RET(lobpcg_invtri(ctx, z, r, 2000, lob_tol, true, &lres));
     double s0 = 0.0;
-    RET(d2h(ctx, &s0, ctx->sig, 1));
+    if (ctx->grad_on) {   // uᴴv = σ·(CX[:,1])ᴴX[:,1] (CX = R⁻ᴴX = u/σ at convergence)
+      RET(gram(ctx, ctx->n_pad, ctx->CS, ctx->n_pad, 1, ctx->S, ctx->n_pad, 1, ctx->small[7], 1));
+      cplx w{0, 0};
+      RET(d2h2(ctx, &s0, ctx->sig, 1, &w, ctx->small[7], 1));
+      if (st->dsdx) st->dsdx[i] = -s0 * w.x;
+      if (st->dsdy) st->dsdy[i] = s0 * w.y;
+    } else {
+      RET(d2h(ctx, &s0, ctx->sig, 1));
+    }
     sigma_min[i] = s0;  // keep.σ[1] (psTriRecy.jl:809)
     const int64_t it = lres.it;
     int64_t m_apps = 0, r_apps = 0;
@@ -1806,15 +1846,16 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
       // Speculative batch: the recycle steps of points i..i+B-1 against the current space.
       // Accepted points leave the space unchanged, so the results up to the first
       // rejection are exactly those of the sequential loop.
-      cplx zs[BATCH_MAX];
+      cplx zs[BATCH_MAX], quad[BATCH_MAX];
       double taus[BATCH_MAX], sig0[BATCH_MAX], w0[BATCH_MAX];
       int rr[BATCH_MAX];
       for (int b = 0; b < B; ++b) {
         zs[b] = cmk(Z[i + b].re, Z[i + b].im);
         taus[b] = gap_tau_at(std::max(run.remaining - b, 0));
+        quad[b] = czero();
       }
       const uint64_t t0 = now_ns();
-      RET(recycle_batch(ctx, B, zs, taus, ctl->shift, rr, sig0, w0));
+      RET(recycle_batch(ctx, B, zs, taus, ctl->shift, rr, sig0, w0, quad));
       st->recycle_time_ns += now_ns() - t0;
       int b = 0;
       bool failed = false;
@@ -1824,7 +1865,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
         if (st->r_recy) st->r_recy[i + b] = rr[b];
         if (st->refine_it) st->refine_it[i + b] = 0;
         if (thresh_ok(w0[b], sig0[b])) {
-          accept(i + b, sig0[b], rr[b]);
+          accept(i + b, sig0[b], rr[b], quad[b]);
           continue;
         }
         failed = true;
@@ -1854,7 +1895,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
           run.remaining = run.remaining > 0 ? run.remaining - 1 : 0;
           st->recycle_time_ns += now_ns() - t1;
           if (st->r_recy) st->r_recy[i] = rres.rr;
-          if (thresh_ok(rres.w0norm, rres.sigma0)) accept(i, rres.sigma0, rres.rr);
+          if (thresh_ok(rres.w0norm, rres.sigma0)) accept(i, rres.sigma0, rres.rr, rres.quad);
           else RET(refine(i, rres.rr));
           ++i;
         }
@@ -1872,7 +1913,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
       st->recycle_time_ns += now_ns() - t0;
       if (st->r_recy) st->r_recy[i] = rres.rr;
       if (thresh_ok(rres.w0norm, rres.sigma0)) {
-        accept(i, rres.sigma0, rres.rr);
+        accept(i, rres.sigma0, rres.rr, rres.quad);
       } else {
         if (ctx->verbose >= 2)
           emit_log(ctx, "  recycle rejected: |W[:,1]|=%.3e σ_recy=%.6e r_svdrr=%d pr=%d", rres.w0norm, rres.sigma0,
@@ -2497,6 +2538,8 @@ extern "C" int rls_pstrirecy_schur_lanes_range(rls_ctx* const* ctxs, int nlanes,
     ls.M_vec_apps_no_recycle = (st && st->M_vec_apps_no_recycle) ? st->M_vec_apps_no_recycle + o : nullptr;
     ls.R_vec_apps = (st && st->R_vec_apps) ? st->R_vec_apps + o : nullptr;
     ls.refine_it = (st && st->refine_it) ? st->refine_it + o : nullptr;
+    ls.dsdx = (st && st->dsdx) ? st->dsdx + o : nullptr;
+    ls.dsdy = (st && st->dsdy) ? st->dsdy + o : nullptr;
     status[l] = rls_pstrirecy_schur_range(c, Z + o, len, g, ctl, X0, b, e, sigma_min + o, &ls);
   };
   if (nlanes == 1) {

@@ -53,6 +53,9 @@ struct PrecState {
   int64_t l_np = 0;
   cplx *lS = nullptr, *lCS = nullptr, *lG = nullptr, *lR = nullptr;
   double *lsig = nullptr, *llam = nullptr;
+  // Schur vectors Q (n_pad × n_pad, rls_set_schur_vectors) and [u v Qu Qv] for ∂σ/∂C
+  cplx *Qdev = nullptr, *Qws = nullptr;
+  int64_t Q_np = 0, Q_n = 0;
   // host copy of C (for the IC rebuilds) and the column order
   std::vector<int64_t> colptr, rowval, p0;
   std::vector<rls_c64> nzval;
@@ -70,6 +73,29 @@ struct PrecState {
 void prec_state_delete(PrecState* s) { delete s; }
 
 namespace {
+
+// A device buffer owned by one host call: freed (after the stream drains) when it goes out
+// of scope.  For per-call inputs whose size the call's arguments fix.
+template <class T>
+struct DevTmpBuf {
+  rls_ctx* ctx;
+  T* p = nullptr;
+  explicit DevTmpBuf(rls_ctx* c) : ctx(c) {}
+  int alloc(size_t count) {
+    if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      set_err(ctx, "device allocation of %zu bytes failed", std::max<size_t>(count, 1) * sizeof(T));
+      return RLS_ERR_NOMEM;
+    }
+    return RLS_OK;
+  }
+  ~DevTmpBuf() {
+    if (p) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaFree(p);
+    }
+  }
+};
 
 // ---- small building blocks ---------------------------------------------------------------
 
@@ -787,6 +813,7 @@ extern "C" int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colp
   }
   RET(check_prec_control(ctx, c));
   CK(cudaSetDevice(ctx->device));
+  ctx->grad_on = false;
   const int rm = (int)c->r_main, rp = (int)c->r_pred;
   rls_psprecrecy_stats dummy{};
   if (!st) st = &dummy;
@@ -1105,7 +1132,7 @@ extern "C" int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colp
         zs[b] = cmk(Z[i + b].re, Z[i + b].im);
         taus[b] = c->gap_tau;
       }
-      RET(recycle_batch(ctx, B, zs, taus, c->shift, rr, sig0, w0));
+      RET(recycle_batch(ctx, B, zs, taus, c->shift, rr, sig0, w0, nullptr));
       nb = B;
     }
     st->main_recycle_time_ns += now_ns() - t0;
@@ -1292,4 +1319,89 @@ extern "C" int rls_lobpcg_svd(rls_ctx* ctx, int op, rls_c64 z, int prec, const r
   if (sigma) *sigma = s;
   if (it) *it = its;
   return RLS_OK;
+}
+
+// ---- ∂σ/∂C on a sparsity pattern (the adjoint of σ with respect to C's entries) ------------
+
+namespace {
+// out[k] = Re(conj(Qu[rows[k]]) · Qv[cols[k]])  (Qu, Qv columns of QUV, ld ldq)
+__global__ void k_grad_pattern(int64_t nnz, const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
+                               int base, const cplx* __restrict__ Qu, const cplx* __restrict__ Qv, int64_t n,
+                               double* out, int* err) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = rows[k] - base, j = cols[k] - base;
+    if (i < 0 || i >= n || j < 0 || j >= n) {
+      atomicOr(err, DEVERR_SIZE);
+      out[k] = 0.0;
+      continue;
+    }
+    const cplx a = Qu[i], b = Qv[j];
+    out[k] = a.x * b.x + a.y * b.y;          // Re(conj(a)·b)
+  }
+}
+}  // namespace
+
+extern "C" int rls_set_schur_vectors(rls_ctx* ctx, const rls_c64* Q, int64_t ldq) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->T) {
+    set_err(ctx, "no Schur factor uploaded (call rls_set_schur first)");
+    return RLS_ERR_STATE;
+  }
+  if (!Q || ldq < ctx->n) {
+    set_err(ctx, "rls_set_schur_vectors: Q must be n × n with ldq >= n");
+    return RLS_ERR_ARG;
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->prec) ctx->prec = new PrecState();
+  PrecState& ps = *ctx->prec;
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  if (ps.Q_np != np) {
+    dfree(ctx, ps.Qdev);
+    dfree(ctx, ps.Qws);
+    ps.Qdev = ps.Qws = nullptr;
+    RET(dalloc_t(ctx, &ps.Qdev, (size_t)np * np));
+    RET(dalloc_t(ctx, &ps.Qws, (size_t)4 * np));
+    ps.Q_np = np;
+  }
+  CK(cudaMemsetAsync(ps.Qdev, 0, sizeof(cplx) * np * np, ctx->stream));
+  CK(cudaMemcpy2DAsync(ps.Qdev, np * sizeof(cplx), Q, ldq * sizeof(cplx), n * sizeof(cplx), n,
+                       cudaMemcpyHostToDevice, ctx->stream));
+  ps.Q_n = n;
+  return sync_and_check(ctx);
+}
+
+extern "C" int rls_sigma_grad_pattern(rls_ctx* ctx, const rls_c64* u, const rls_c64* v, int64_t nnz,
+                                      const int64_t* rows, const int64_t* cols, int base, double* dsdC) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->prec || !ctx->prec->Qdev || ctx->prec->Q_n != ctx->n) {
+    set_err(ctx, "no Schur vectors uploaded (call rls_set_schur_vectors first)");
+    return RLS_ERR_STATE;
+  }
+  if (!u || !v || nnz < 0 || (nnz > 0 && (!rows || !cols || !dsdC)) || (base != 0 && base != 1)) {
+    set_err(ctx, "rls_sigma_grad_pattern: invalid arguments");
+    return RLS_ERR_ARG;
+  }
+  if (nnz == 0) return RLS_OK;
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->V) RET(setup_space(ctx, 1, 1));
+  PrecState& ps = *ctx->prec;
+  const int64_t np = ctx->n_pad, n = ctx->n;
+  cplx* UV = ps.Qws;            // [u v] (Schur basis)
+  cplx* QUV = ps.Qws + 2 * np;  // [Q u, Q v]
+  CK(cudaMemsetAsync(UV, 0, sizeof(cplx) * 2 * np, ctx->stream));
+  CK(cudaMemcpyAsync(UV, u, sizeof(cplx) * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(UV + np, v, sizeof(cplx) * n, cudaMemcpyHostToDevice, ctx->stream));
+  RET(gemm_rows(ctx, np, one_src(ps.Qdev), np, (int)n, UV, np, 2, QUV, np));
+  DevTmpBuf<int64_t> dr(ctx), dc(ctx);
+  DevTmpBuf<double> dout(ctx);
+  RET(dr.alloc((size_t)nnz));
+  RET(dc.alloc((size_t)nnz));
+  RET(dout.alloc((size_t)nnz));
+  CK(cudaMemcpyAsync(dr.p, rows, sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dc.p, cols, sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+  const unsigned blocks = (unsigned)std::min<int64_t>((nnz + 255) / 256, 148 * 8);
+  k_grad_pattern<<<blocks, 256, 0, ctx->stream>>>(nnz, dr.p, dc.p, base, QUV, QUV + np, n, dout.p, ctx->derr);
+  RET(check_launch(ctx, "k_grad_pattern"));
+  CK(cudaMemcpyAsync(dsdC, dout.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync_and_check(ctx);
 }

@@ -88,11 +88,17 @@ class PsTriRecyStats:
     mv_stats_available: bool = True
     n_it: int = 0
     n_pts: int = 0
+    dsdx: np.ndarray = None      # ∂σ/∂Re z per point (grad=True)
+    dsdy: np.ndarray = None      # ∂σ/∂Im z per point
 
     @classmethod
-    def alloc(cls, nZ):
+    def alloc(cls, nZ, grad: bool = False):
         z = lambda: np.zeros(nZ, dtype=np.int64)
-        return cls(z(), z(), np.zeros(nZ, dtype=np.complex128), z(), z(), z(), z())
+        st = cls(z(), z(), np.zeros(nZ, dtype=np.complex128), z(), z(), z(), z())
+        if grad:
+            st.dsdx = np.full(nZ, np.nan)
+            st.dsdy = np.full(nZ, np.nan)
+        return st
 
 
 @dataclass
@@ -164,6 +170,7 @@ class Engine:
         self._h = h
         self._log_cb = None
         self._T_id = None
+        self._Q_id = None
         self.n = 0
 
     def close(self):
@@ -184,6 +191,7 @@ class Engine:
         n = T.shape[0]
         check(lib().rls_set_schur(self._h, n, ptr(T), n), self._h)
         self._T_id = id(T)
+        self._Q_id = None
         self.n = n
 
     def set_log(self, fn, verbose=1):
@@ -195,20 +203,14 @@ class Engine:
         self._log_cb = cb
         check(lib().rls_ctx_set_log(self._h, cb, None, int(verbose)), self._h)
 
-    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None):
+    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None, grad: bool = False):
+        """psTriRecy on the uploaded Schur factor → (σ, stats); with grad, stats.dsdx and
+        stats.dsdy hold ∂σ/∂Re z and ∂σ/∂Im z at every point."""
         nZ = len(rec.Z)
         Z = np.ascontiguousarray(rec.Z, dtype=np.complex128)
         sigma = np.full(nZ, np.nan)
-        st = PsTriRecyStats.alloc(nZ)
-        cst = rls_pstrirecy_stats()
-        i64 = C.POINTER(C.c_int64)
-        cst.p_count = st.p_count.ctypes.data_as(i64)
-        cst.r_recy = st.r_recy.ctypes.data_as(i64)
-        cst.pts = st.pts.ctypes.data_as(C.POINTER(c64))
-        cst.M_vec_apps = st.M_vec_apps.ctypes.data_as(i64)
-        cst.M_vec_apps_no_recycle = st.M_vec_apps_no_recycle.ctypes.data_as(i64)
-        cst.R_vec_apps = st.R_vec_apps.ctypes.data_as(i64)
-        cst.refine_it = st.refine_it.ctypes.data_as(i64)
+        st = PsTriRecyStats.alloc(nZ, grad)
+        cst = self.stats_struct(st)
         x0 = None
         if X0 is not None:
             x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
@@ -233,6 +235,11 @@ class Engine:
         cst.M_vec_apps_no_recycle = st.M_vec_apps_no_recycle.ctypes.data_as(i64)
         cst.R_vec_apps = st.R_vec_apps.ctypes.data_as(i64)
         cst.refine_it = st.refine_it.ctypes.data_as(i64)
+        f64 = C.POINTER(C.c_double)
+        if st.dsdx is not None:
+            cst.dsdx = st.dsdx.ctypes.data_as(f64)
+        if st.dsdy is not None:
+            cst.dsdy = st.dsdy.ctypes.data_as(f64)
         return cst
 
     def pstrirecy_range(self, rec: Recursion, control: PsTriRecyControl, i_begin: int, i_end: int, sigma, st,
@@ -356,9 +363,10 @@ class Engine:
         v0 (n values) approximates the right singular vector of T − zI (e.g. the first
         Ritz vector of lobpcg_svd_invtri).  Returns a dict with sigma, dsdx = ∂σ/∂Re z,
         dsdy = ∂σ/∂Im z and the Schur-basis singular vectors u, v.  With the Schur vectors
-        Q of C (C = Q T Qᴴ, from pre_process) it adds uC = Q u, vC = Q v and dsdC =
-        Re(conj(uC_i) vC_j): on the (rows, cols) index arrays of ``pattern`` when given
-        (the nnz of a sparse C), else the dense n × n matrix.
+        Q of C (C = Q T Qᴴ, from pre_process; uploaded once per Q) it adds dsdC =
+        Re(conj((Qu)_i) (Qv)_j), computed on the device (rls_sigma_grad_pattern): on the
+        (rows, cols) index arrays of ``pattern`` when given (the nnz of a sparse C), else the
+        dense n × n matrix.
         """
         v0 = np.ascontiguousarray(np.asarray(v0, dtype=np.complex128).reshape(-1))
         if v0.shape[0] != self.n:
@@ -370,13 +378,20 @@ class Engine:
                                    C.byref(dx), C.byref(dy), ptr(u), ptr(v)), self._h)
         out = {"sigma": sg.value, "dsdx": dx.value, "dsdy": dy.value, "u": u, "v": v}
         if Q is not None:
-            uC, vC = Q @ u, Q @ v
-            out["uC"], out["vC"] = uC, vC
+            if self._Q_id != id(Q):
+                Qf = np.asfortranarray(np.asarray(Q, dtype=np.complex128))
+                check(lib().rls_set_schur_vectors(self._h, ptr(Qf), Qf.shape[0]), self._h)
+                self._Q_id = id(Q)
             if pattern is not None:
-                rows, cols = pattern
-                out["dsdC"] = np.real(np.conj(uC[rows]) * vC[cols])
+                rows = np.ascontiguousarray(pattern[0], dtype=np.int64)
+                cols = np.ascontiguousarray(pattern[1], dtype=np.int64)
             else:
-                out["dsdC"] = np.real(np.outer(np.conj(uC), vC))
+                rows = np.ascontiguousarray(np.tile(np.arange(self.n, dtype=np.int64), self.n))
+                cols = np.ascontiguousarray(np.repeat(np.arange(self.n, dtype=np.int64), self.n))
+            g = np.zeros(rows.size)
+            check(lib().rls_sigma_grad_pattern(self._h, ptr(u), ptr(v), rows.size, ptr(rows), ptr(cols), 0, ptr(g)),
+                  self._h)
+            out["dsdC"] = g if pattern is not None else g.reshape(self.n, self.n, order="F")
         return out
 
 
@@ -609,10 +624,10 @@ class Lanes:
         for f in ("recycle_time_ns", "qr_time_ns", "refine_time_ns", "update_time_ns", "n_it", "n_pts"):
             setattr(st, f, int(getattr(cst, f)))
 
-    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None):
+    def pstrirecy(self, rec: Recursion, control: PsTriRecyControl, X0=None, grad: bool = False):
         nZ = len(rec.Z)
         sigma = np.full(nZ, np.nan)
-        st = PsTriRecyStats.alloc(nZ)
+        st = PsTriRecyStats.alloc(nZ, grad)
         cst = self.engines[0].stats_struct(st)
         self.pstrirecy_range(rec, control, 0, nZ, sigma, st, cst, X0=X0)
         st.mv_stats_available = True
@@ -644,13 +659,15 @@ def _print_startup(io, rec, control):
 
 
 def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int = 1, io=None, X0=None,
-              device: int = 0, lanes: int = 1):
+              device: int = 0, lanes: int = 1, grad: bool = False):
     """psTriRecy (psTriRecy.jl:889-913) → (σ_min in rec.Z order, PsTriRecyStats).
 
     ``X0`` (n × r) stands in for the reference's ``rand!(X)``; None draws a
     deterministic uniform [0,1) complex block on the device.  ``lanes`` > 1 splits the
     traversal on column boundaries into concurrent lanes on the same GPU (class Lanes);
-    1 keeps the reference's single traversal.
+    1 keeps the reference's single traversal.  ``grad`` fills stats.dsdx / stats.dsdy with
+    ∂σ/∂Re z and ∂σ/∂Im z at every point from its own singular pair (no reference
+    counterpart).
     """
     control = control or PsTriRecyControl()
     io = io if io is not None else sys.stdout
@@ -666,7 +683,7 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
     if lanes > 1:
         ls = Lanes(lanes, device, T)
         try:
-            sigma, st = ls.pstrirecy(rec, control, X0=X0)
+            sigma, st = ls.pstrirecy(rec, control, X0=X0, grad=grad)
         finally:
             ls.close()
         st.preprocess_time_ns = pre_ns
@@ -678,7 +695,7 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
     else:
         eng.set_log(None)
     try:
-        sigma, st = eng.pstrirecy(rec, control, X0=X0)
+        sigma, st = eng.pstrirecy(rec, control, X0=X0, grad=grad)
     finally:
         eng.set_log(None)
     st.preprocess_time_ns = pre_ns

@@ -76,3 +76,32 @@ def test_engine_gradient_rejects_bad_input(cuda_device):
     with pytest.raises(ArgumentError):
         e.sigma_grad(0.5, np.zeros(120))
     e.close()
+
+
+@pytest.mark.gpu
+def test_grid_gradient_every_point(cuda_device):
+    """∂σ/∂z at every grid point from the loop's own singular pairs (stats dsdx, dsdy): the
+    accepted Ritz pair at recycled points (quadratic form on the cached H2), LOBPCG's pair at
+    refined ones.  Against the dense-SVD gradient: these come from pairs the solver accepted at
+    its tolerance, so they agree to first order in the accepted residual (|uᴴv| ≤ 1, bound
+    1e-3), and the same values come out of single-lane and laned runs."""
+    import rls_b200 as R
+    C = sprand(240).toarray().astype(np.complex128)
+    T = R.pre_process(C)
+    grid = (0.45, 0.55, 0.0, 0.1, 8, 6, 3)
+    rec = R.recursion_grid(*grid)
+    n = 240
+    rng = np.random.default_rng(8)
+    X0 = rng.random((n, 6)) + 1j * rng.random((n, 6))
+    ctl = R.PsTriRecyControl(normC=3.2, tol=1e-4, p=20, recy_tau=1.6)
+    sig, st = R.psTriRecy(R.SchurFactor(T), rec, ctl, verbose=0, X0=X0, grad=True)
+    assert np.all(np.isfinite(st.dsdx)) and np.all(np.isfinite(st.dsdy))
+    ref = np.array([dense_sigma_grad(C, z)[1:3] for z in rec.Z])
+    err = np.maximum(np.abs(st.dsdx - ref[:, 0]), np.abs(st.dsdy - ref[:, 1]))
+    rec_pts = st.refine_it == 0
+    print(f"grid gradient: max error recycled {err[rec_pts].max() if rec_pts.any() else 0:.2e}, "
+          f"refined {err[~rec_pts].max():.2e}")
+    assert rec_pts.any() and (~rec_pts).any()
+    assert err.max() <= 1e-3, err.max()
+    sig2, st2 = R.psTriRecy(R.SchurFactor(T), rec, ctl, verbose=0, X0=X0, grad=False)
+    assert st2.dsdx is None and np.array_equal(sig, sig2)
