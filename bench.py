@@ -59,6 +59,26 @@ GRID = (0.45, 0.55, 0.0, 0.1, 200, 200, 20)
 N_MAT = 4000
 NORMC = 3.2
 NCU_TRSM_TRAFFIC = 132.54e6 + 3.81e6   # DRAM bytes per k_trsm_half launch (ncu, n = 4000, k = 6)
+WORKLOAD = "sprand4000"
+# The dense Schur-factor workloads of psTriRecy (the default is the sprand case on its full grid;
+# laser5000 is the dense Landau laser operator, example/laser/laser.jl:15-57, normC = 1,
+# laser_psTriRecy.jl:28-36).  af23560 (psPrecRecy) has its own leg (run_precrecy).
+WORKLOADS = {
+    "sprand4000": dict(metric=METRIC, grid=GRID, n=4000, normC=3.2,
+                       desc="psTriRecy sprand N=4000 dense-Schur, 200x200 grid [0.45,0.55]x[0,0.1], k=20, "
+                            "tol=1e-4, p=60, r=6, recy_tau=1.6"),
+    "laser5000": dict(metric="σ_min grid pts/s (psTriRecy, laser N=5000, 200×200 grid, k=20, tol 1e-4)",
+                      grid=(-1.1, 1.2, -1.1, 1.1, 200, 200, 20), n=5000, normC=1.0,
+                      desc="psTriRecy laser (Landau, F=40π) N=5000 dense-Schur, 200x200 grid [-1.1,1.2]x[-1.1,1.1], "
+                           "k=20, tol=1e-4, p=60, r=6, recy_tau=1.6"),
+}
+
+
+def select_workload(name):
+    """Rebinds the workload constants (the dense psTriRecy workloads)."""
+    global METRIC, GRID, N_MAT, NORMC, WORKLOAD
+    w = WORKLOADS[name]
+    METRIC, GRID, N_MAT, NORMC, WORKLOAD = w["metric"], w["grid"], w["n"], w["normC"], name
 
 
 def parse():
@@ -67,14 +87,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sprand4000", choices=["sprand4000", "laser5000", "af23560"],
+                    help="sprand4000 (default, the headline), laser5000 (dense laser operator), af23560 "
+                         "(psPrecRecy on the af23560-shaped synthetic matrix)")
     ap.add_argument("--chunk", type=int, default=200,
                     help="grid points per lane per step (at most; lowered to fit the lane's share of the grid)")
     ap.add_argument("--lanes", type=int, default=20, help="concurrent grid lanes per GPU")
     ap.add_argument("--trsm-ctas", type=int, default=0,
                     help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
+    ap.add_argument("--pp-chunk", type=int, default=10, help="grid points per step of the af23560 (psPrecRecy) leg")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
-    ap.add_argument("--n", type=int, default=N_MAT)
+    ap.add_argument("--n", type=int, default=None, help="matrix order (default: the workload's)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmm", action="store_true", help="skip the sparse shifted product measurement")
     ap.add_argument("--no-ic", action="store_true", help="skip the IC preconditioner apply measurement")
@@ -93,9 +117,9 @@ def control():
 
 
 def build_inputs(n):
-    from rls_b200.examples import sprand
+    from rls_b200.examples import sprand, landau
     from rls_b200.solvers import pre_process
-    C = sprand(n).toarray()
+    C = landau(n) if WORKLOAD == "laser5000" else sprand(n).toarray()
     t0 = time.perf_counter()
     T = pre_process(C)
     return C, np.asfortranarray(T), time.perf_counter() - t0
@@ -311,9 +335,9 @@ def cpu_baseline(T, rec, ctl, X0, budget_s, min_pts=2):
 def base_line(args, n_gpus):
     return {"metric": METRIC, "unit": "pts/s", "n_gpus": n_gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
-            "data": "synthetic (sprand generator, NumPy PCG64 seed 20260318)",
-            "config": {"workload": "psTriRecy sprand N=4000 dense-Schur, 200x200 grid [0.45,0.55]x[0,0.1], k=20, "
-                                   "tol=1e-4, p=60, r=6, recy_tau=1.6",
+            "data": ("synthetic (sprand generator, NumPy PCG64 seed 20260318)" if WORKLOAD == "sprand4000" else
+                     "synthetic (laser.jl's Landau operator, Gauss-Legendre nodes by Golub-Welsch)"),
+            "config": {"workload": WORKLOADS[WORKLOAD]["desc"],
                        "n": args.n, "grid": list(GRID), "points_per_step": None,
                        "l2": "inputs larger than L2 (Schur tiles 132 MB and each lane's scaled copy 132 MB, "
                               "streamed every step; L2 126 MB)"}}
@@ -625,6 +649,12 @@ def run_ncu_window(args):
 
 def main():
     args = parse()
+    if args.workload == "af23560":
+        run_precrecy(args)
+        return
+    select_workload(args.workload)
+    if args.n is None:
+        args.n = N_MAT
     if args.ncu_window:
         run_ncu_window(args)
         return
@@ -632,6 +662,208 @@ def main():
         run_reference(args)
     else:
         run_ours(args)
+
+
+
+# ---- psPrecRecy on the af23560-shaped matrix --------------------------------------------------
+
+AF_GRID = (-1.6, 0.8, -1.55, 1.55, 200, 200, 20)
+
+
+def af_controls(mod, normC):
+    """af23560_psPrecRecy.jl:16-46 as PsPrecRecyControl of `mod` (rls_b200.solvers or the oracle)."""
+    return mod.PsPrecRecyControl(
+        tol=1e-4, main_normC=normC, main_tau=1.6, gap_tau=1e-10, tol_pred=1e-3, lobpcg_pred_tol_scale=1.0,
+        pred_tau=1.6, idx_cutoff_pred=0.01, pred_orth_type="shiftchol", pred_conv_thresh_type=1,
+        lambda_lower_min=0.01, lambda_upper_max=30.0, r_main=6, p_main=60, p_min_main=1, main_implict_update=False,
+        main_implict_recycle=True, r_pred=40, p_pred=20, p_min_pred=1, pred_implict_update=True,
+        pred_implict_recycle=True, hsl_tol=1e-3, hsl_cntl_1=1e-6, hsl_icntl_1=200, hsl_icntl_2=500,
+        hsl_cntl_2=1e-6, gamma_tol=1e-3, lambda_n_tol=1e-3)
+
+
+def af_inputs(n):
+    from rls_b200.examples import af23560_shaped, AF23560_NORMC
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    C = af23560_shaped(n)
+    # psPrecRecy orders by SPQR's column pivoting (qr(C).cpiv, psPrecRecy.jl:625), which needs
+    # SuiteSparse; reverse Cuthill-McKee of |C| + |Cᵀ| stands in for that fill-reducing order
+    p = np.ascontiguousarray(reverse_cuthill_mckee((abs(C) + abs(C.T)).tocsr(), symmetric_mode=True),
+                             dtype=np.int64)
+    return C, AF23560_NORMC, p
+
+
+def sparse_truth(C, zs, block=4, maxit=200, rtol=1e-13):
+    """FP64 σ_min(C − zI) by block inverse iteration on (C − zI)ᴴ(C − zI) with SciPy's sparse LU
+    (host; independent of the engine), and the residual bound |σ − σ_true| ≤ ‖Av − σ²v‖/σ."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    n = C.shape[0]
+    rng = np.random.default_rng(0)
+    out, bnd = [], []
+    for z in zs:
+        A = (C - z * sp.identity(n, format="csc", dtype=np.complex128)).tocsc()
+        lu = spla.splu(A)
+        Y = np.linalg.qr(rng.standard_normal((n, block)) + 1j * rng.standard_normal((n, block)))[0]
+        prev, s = np.inf, np.inf
+        for _ in range(maxit):
+            Y = lu.solve(lu.solve(Y, trans="H"))
+            Y = np.linalg.qr(Y)[0]
+            _, sv, Vh = np.linalg.svd(A @ Y, full_matrices=False)
+            Y = Y @ Vh.conj().T
+            s = sv[-1]
+            if abs(prev - s) <= rtol * s:
+                break
+            prev = s
+        v = Y[:, -1]
+        res = A.conj().T @ (A @ v) - s * s * v
+        out.append(s)
+        bnd.append(np.linalg.norm(res) / s)
+    return np.array(out), np.array(bnd)
+
+
+def run_precrecy(args):
+    """psPrecRecy (af23560-shaped, 200x200 grid, k=20): the prefix of the traversal in steps of
+    --pp-chunk points, device time of the timed steps on the engine stream."""
+    n = args.n or 23560
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    C, normC, p = af_inputs(n)
+    s = args.pp_chunk
+    nst = args.warmup + args.steps
+    out = {"metric": "σ_min grid pts/s (psPrecRecy, af23560-shaped N=23560, 200×200 grid, k=20, tol 1e-4)",
+           "unit": "pts/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+           "data": "synthetic af23560-shaped matrix (rls_b200.examples.af23560_shaped, NumPy PCG64 seed 20260318)",
+           "config": {"workload": "psPrecRecy af23560-shaped N=%d (~20 nnz/row, band ±300, ‖C‖₂=645.74), 200x200 "
+                                  "grid [-1.6,0.8]x[-1.55,1.55], k=20, tol=1e-4, r_main=6, p_main=60, r_pred=40, "
+                                  "p_pred=20, IC lsize=200 rsize=500, RCM column order" % n,
+                      "n": n, "nnz": int(C.nnz), "grid": list(AF_GRID), "points_per_step": s,
+                      "span": f"traversal points {args.warmup * s}..{nst * s - 1} after {args.warmup * s} "
+                              f"warm-up points (the run's first preconditioner build is in the warm-up)"}}
+    if args.impl == "reference":
+        from oracle import recugrid as G
+        from oracle.psprecrecy import PsPrecRecyRun
+        import oracle.psprecrecy as OP
+        from rls_b200.solvers import ic_factor as ic_host
+        rng = np.random.default_rng(1)
+        run = PsPrecRecyRun(C, G.recursion_grid(*AF_GRID), af_controls(OP, normC), p,
+                            rng.random((n, 6)) + 1j * rng.random((n, 6)), rng.random((n, 40)) + 1j * rng.random((n, 40)),
+                            bound_x0=rng.random((n, 1)) + 1j * rng.random((n, 1)), ic=ic_host)
+        rs = args.ref_chunk
+        for w in range(args.warmup):
+            run.run(w * rs, (w + 1) * rs)
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            a = (args.warmup + k) * rs
+            run.run(a, a + rs)
+        el = time.perf_counter() - t0
+        v = args.steps * rs / el
+        out.update({"impl": "reference", "value": v, "ms_per_step": el * 1e3 / args.steps,
+                    "cpu_baseline": {"value": v, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+                                     "sample": f"{rs} points per step after {args.warmup} warm-up steps; CPU "
+                                               "restatement of psPrecRecy (SciPy sparse solves and LAPACK, all host "
+                                               "threads; IC factor by the C++ host build)"},
+                    "e2e": {"value": v, "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        out["config"]["points_per_step"] = rs
+        out["config"]["span"] = (f"traversal points {args.warmup * rs}..{(args.warmup + args.steps) * rs - 1} after "
+                                 f"{args.warmup * rs} warm-up points")
+        print(json.dumps(out), flush=True)
+        return
+    import torch
+    import rls_b200 as R
+    from rls_b200.solvers import Engine, PrecRecyRun
+    torch.cuda.set_device(0)
+    rec = R.recursion_grid(*AF_GRID)
+    ctl = af_controls(R, normC)
+    rng = np.random.default_rng(1)
+    X0m = rng.random((n, 6)) + 1j * rng.random((n, 6))
+    X0p = rng.random((n, 40)) + 1j * rng.random((n, 40))
+    xb = rng.random((n, 1)) + 1j * rng.random((n, 1))
+    e = Engine(0)
+    t0 = time.perf_counter()
+    run = PrecRecyRun(e, C, rec, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb)
+    run.run(0, args.warmup * s)
+    torch.cuda.synchronize()
+    t_warm = time.perf_counter() - t0
+    e.set_profile(True)
+    stream = torch.cuda.ExternalStream(e.stream_ptr())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(0 if "CUDA_VISIBLE_DEVICES" not in os.environ else os.environ["CUDA_VISIBLE_DEVICES"].split(",")[0])
+    clk.start()
+    time.sleep(0.3)
+    l0 = e.launches()
+    ev0.record(stream)
+    t1 = time.perf_counter()
+    sig, st = run.run(args.warmup * s, nst * s)
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - t1
+    l1 = e.launches()
+    clk.stop()
+    ms = ev0.elapsed_time(ev1)
+    prof = {k: e.profile(k) for k in (1, 4, 5, 6)}
+    e.close()
+    timed = np.arange(args.warmup * s, nst * s)
+    v = args.steps * s / (ms / 1e3)
+    out.update({"value": v, "ms_per_step": ms / args.steps, "gpu_launches": int(l1 - l0), "clocks": clk.summary(),
+                "e2e": {"value": nst * s / (t_warm + wall), "unit": "pts/s",
+                        "h2d_bytes_per_step": int((C.nnz * 32 + n * 8 + nst * s * 16) / nst),
+                        "d2h_bytes_per_step": int(s * 8),
+                        "span": "PrecRecyRun through the public API from host buffers: C uploaded, preconditioner "
+                                f"built at z†, steps 0..{nst - 1}, wall clock"},
+                "wall_pts_per_s": args.steps * s / wall})
+    out["stats"] = {"main_refines_timed": int(np.sum(st.main_refine_it[timed] > 0)),
+                    "pred_refines_timed": int(np.sum(st.pred_refine_it[timed] > 0)),
+                    "precond_builds": st.n_precond_rebuild_pts, "precond_s": st.precond_time_ns / 1e9,
+                    "main_refine_s": st.main_refine_time_ns / 1e9, "pred_refine_s": st.pred_refine_time_ns / 1e9,
+                    "pred_update_s": st.pred_update_time_ns / 1e9, "main_recycle_s": st.main_recycle_time_ns / 1e9,
+                    "pred_recycle_s": st.pred_recycle_time_ns / 1e9, "main_update_s": st.main_update_time_ns / 1e9}
+    names = {1: "pred-stage eigensolve (tridiagonalisation + Sturm + inverse iteration)", 4: "host waits",
+             5: "k_spmm_shifted (C − zI and its adjoint)", 6: "IC preconditioner solves (k_sptrsv_blocks)"}
+    out["kernel_time_ms"] = {names[k]: {"launches": c, "ms": m} for k, (c, m, w) in prof.items() if k != 4}
+    out["host_waits"] = {"count": prof[4][0], "ms": prof[4][1]}
+    cnt, tot, work = prof[6]
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    if cnt:
+        ach = (work / cnt) / (tot / cnt / 1e3) / 1e9
+        out["roofline"] = {"bound": "hbm", "kernel": names[6], "achieved": ach, "peak": hbm, "unit": "GB/s",
+                           "frac": ach / hbm, "traffic": None,
+                           "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "launches": cnt,
+                           "avg_us": tot / cnt * 1e3}
+    # accuracy of the timed points against the FP64 sparse-LU truth (after the timed region)
+    pick = timed[np.linspace(0, len(timed) - 1, min(args.accuracy_points, len(timed), 8)).astype(np.int64)]
+    if args.accuracy_points > 0:
+        truth, bound = sparse_truth(C, rec.Z[pick])
+        err = np.abs(sig[pick] - truth)
+        out["accuracy"] = {"points": int(pick.size), "max_abs_err": float(err.max()),
+                           "max_abs_err_over_normC": float(err.max() / normC),
+                           "within_bar": bool(err.max() <= 1e-4 * normC), "truth_max_err_bound": float(bound.max()),
+                           "truth": "block inverse iteration on (C−zI)ᴴ(C−zI), SciPy sparse LU (host)"}
+    if args.cpu_sample_s > 0:
+        from oracle import recugrid as G
+        from oracle.psprecrecy import PsPrecRecyRun
+        import oracle.psprecrecy as OP
+        from rls_b200.solvers import ic_factor as ic_host
+        runo = PsPrecRecyRun(C, G.recursion_grid(*AF_GRID), af_controls(OP, normC), p, X0m, X0p, bound_x0=xb,
+                             ic=ic_host)
+        t0 = time.perf_counter()
+        i = 0
+        while i < nst * s and (i < 2 or time.perf_counter() - t0 < args.cpu_sample_s):
+            runo.run(i, i + 1)
+            i += 1
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": i / el, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"first {i} points of the traversal (preconditioner build included), CPU "
+                                         f"restatement (SciPy sparse solves, LAPACK; IC by the C++ host build), "
+                                         f"{el:.1f} s"}
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

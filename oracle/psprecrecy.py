@@ -189,7 +189,8 @@ def _pred_idx(lam, r_pred, cutoff):
 class PsPrecRecyRun:
     """psPrecRecy (psPrecRecy.jl:617-1033) on a sparse square C, resumable over index ranges."""
 
-    def __init__(self, C, rec, ctl: PsPrecRecyControl, p, X0_main, X0_pred, bound_x0=None, log=None):
+    def __init__(self, C, rec, ctl: PsPrecRecyControl, p, X0_main, X0_pred, bound_x0=None, log=None, ic=None):
+        self.ic = ic or ic_factor        # get_hsl_LLTP's factorisation (the restatement by default)
         self.C = sp.csc_matrix(C, dtype=np.complex128)
         n = self.C.shape[0]
         self.n, self.rec, self.ctl, self.log = n, rec, ctl, log
@@ -231,8 +232,8 @@ class PsPrecRecyRun:
     # _get_pred_precond! (psPrecRecy.jl:436-462)
     def _precond(self, z):
         ctl, n = self.ctl, self.n
-        L, invp, _ = ic_factor(self.C, z, ctl.hsl_tol, ctl.hsl_cntl_1, ctl.hsl_cntl_2, ctl.hsl_icntl_1,
-                               ctl.hsl_icntl_2, self.p)
+        L, invp, _ = self.ic(self.C, z, ctl.hsl_tol, ctl.hsl_cntl_1, ctl.hsl_cntl_2, ctl.hsl_icntl_1,
+                             ctl.hsl_icntl_2, self.p)
         self.F = LowerFactor(L, self.p, invp)
         self.invF = InvF(self.F)
         x0 = self.bound_x0

@@ -2302,7 +2302,7 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
     return RLS_ERR_SINGULAR;
   }
   const int64_t nblk = F.op[0].nblk;
-  const unsigned grid = (unsigned)std::min<int64_t>((nblk + SPT_WARPS - 1) / SPT_WARPS, 148 * 16);
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk, 148 * 4);
   const unsigned gg = (unsigned)((F.n + 255) / 256);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ctx->profile) {
@@ -2322,9 +2322,9 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
     cplx* Xc = X + (int64_t)c0 * ldx;
 #define RLS_SPT_CASE(K)                                                                                            \
   case K:                                                                                                          \
-    k_sptrsv_blocks<K, false><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(F.op[0], Bc, ldb, F.p, F.w1, F.n,          \
-                                                                        F.ticket, F.flags, F.epoch, ctx->derr);   \
-    k_sptrsv_blocks<K, true><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(                                           \
+    k_sptrsv_wide<K, false><<<grid, 32 * SPW_WARPS, 0, ctx->stream>>>(F.op[0], Bc, ldb, F.p, F.w1, F.n,            \
+                                                                      F.ticket, F.flags, F.epoch, ctx->derr);     \
+    k_sptrsv_wide<K, true><<<grid, 32 * SPW_WARPS, 0, ctx->stream>>>(                                             \
         F.op[1], F.w1, F.n, nullptr, F.w2, F.n, F.ticket + 1, F.flags + nblk * SPT_FLAG_STRIDE, F.epoch, ctx->derr); \
     k_gather_rows<K><<<gg, 256, 0, ctx->stream>>>(F.n, F.invp, F.w2, F.n, Xc, ldx);                                \
     break;
@@ -2333,7 +2333,7 @@ int lltp_ldiv_dev(rls_ctx* ctx, int b, const cplx* B, int64_t ldb, cplx* X, int6
       RLS_SPT_CASE(5) RLS_SPT_CASE(6) RLS_SPT_CASE(7) RLS_SPT_CASE(8)
     }
 #undef RLS_SPT_CASE
-    RET(check_launch(ctx, "k_sptrsv_blocks"));
+    RET(check_launch(ctx, "k_sptrsv_wide"));
   }
   if (ctx->profile) {
     CK(cudaEventRecord(e1, ctx->stream));

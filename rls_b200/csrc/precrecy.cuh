@@ -165,7 +165,7 @@ int lltp_tri(rls_ctx* ctx, int op, bool gather_p, int b, const cplx* B, int64_t 
     return RLS_ERR_SINGULAR;
   }
   const int64_t nblk = F.op[0].nblk;
-  const unsigned grid = (unsigned)std::min<int64_t>((nblk + SPT_WARPS - 1) / SPT_WARPS, 148 * 16);
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk, 148 * 4);
   for (int c0 = 0; c0 < b; c0 += 8) {
     const int kk = std::min(8, b - c0);
     F.epoch += 1;
@@ -182,10 +182,10 @@ int lltp_tri(rls_ctx* ctx, int op, bool gather_p, int b, const cplx* B, int64_t 
 #define RLS_TRI_CASE(K)                                                                                         \
   case K:                                                                                                       \
     if (op == 0)                                                                                                \
-      k_sptrsv_blocks<K, false><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(F.op[0], Bc, ldb, gat, Oc, ldo, tk, fl, \
+      k_sptrsv_wide<K, false><<<grid, 32 * SPW_WARPS, 0, ctx->stream>>>(F.op[0], Bc, ldb, gat, Oc, ldo, tk, fl, \
                                                                           F.epoch, ctx->derr);                  \
     else                                                                                                        \
-      k_sptrsv_blocks<K, true><<<grid, 32 * SPT_WARPS, 0, ctx->stream>>>(F.op[1], Bc, ldb, nullptr, Oc, ldo, tk,  \
+      k_sptrsv_wide<K, true><<<grid, 32 * SPW_WARPS, 0, ctx->stream>>>(F.op[1], Bc, ldb, nullptr, Oc, ldo, tk,  \
                                                                          fl, F.epoch, ctx->derr);               \
     break;
     switch (kk) {
@@ -193,7 +193,7 @@ int lltp_tri(rls_ctx* ctx, int op, bool gather_p, int b, const cplx* B, int64_t 
       RLS_TRI_CASE(5) RLS_TRI_CASE(6) RLS_TRI_CASE(7) RLS_TRI_CASE(8)
     }
 #undef RLS_TRI_CASE
-    RET(check_launch(ctx, "k_sptrsv_blocks"));
+    RET(check_launch(ctx, "k_sptrsv_wide"));
   }
   return RLS_OK;
 }

@@ -168,3 +168,126 @@ __global__ void __launch_bounds__(256) k_gather_rows(int64_t n, const int64_t* _
 #pragma unroll
   for (int c = 0; c < K; ++c) X[(int64_t)c * ldx + i] = W[(int64_t)c * ldw + s];
 }
+
+// The same solve with a CTA of SPW_WARPS warps per block row: every warp takes a strided share
+// (offset w, stride SPW_WARPS) of each row's terms from each dependency, waiting for that
+// dependency's flag first, so a block row's terms from block rows finished long ago stream
+// while the block row finished last is still being solved; after its flag only about
+// (terms from it) / SPW_WARPS loads per lane remain on the critical path.  The warps' partial
+// sums meet in shared memory in a fixed order (deterministic), and warp 0 does the in-block
+// sweep and publishes the block row.  Same plan, flags and ticket order as k_sptrsv_blocks.
+constexpr int SPW_WARPS = 8;
+
+template <int K, bool BACK>
+__global__ void __launch_bounds__(32 * SPW_WARPS) k_sptrsv_wide(TriBlocks A, const cplx* __restrict__ rhs, int64_t ldr,
+                                                                const int64_t* __restrict__ gather, cplx* out,
+                                                                int64_t ldo, int* ticket, int* flags, int epoch,
+                                                                int* err) {
+  __shared__ cplx sm_m[SPT_ROWS * SPT_ROWS];
+  __shared__ cplx sm_acc[SPW_WARPS - 1][K][SPT_ROWS];   // warps 1.. (warp 0 keeps its own)
+  __shared__ int s_t;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int t = s_t;
+    if (t >= A.nblk) break;                               // uniform over the CTA
+    const int64_t b = BACK ? (A.nblk - 1 - t) : t;
+    const int64_t i = b * SPT_ROWS + lane;
+    const bool live = i < A.n;
+    const cplx* mb = A.blk + b * (SPT_ROWS * SPT_ROWS);
+    for (int q = threadIdx.x; q < SPT_ROWS * SPT_ROWS; q += blockDim.x) sm_m[q] = mb[q];
+    cplx acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = czero();
+    int64_t e = live ? A.rowptr[i] : 0;
+    const int64_t k1 = A.depptr[b + 1];
+    for (int64_t k = A.depptr[b]; k < k1; ++k) {
+      if (lane == 0) {
+        const int* f = &flags[(int64_t)A.deps[k] * SPT_FLAG_STRIDE];
+        int spins = 0;
+        unsigned ns = 32;
+        while (spt_ld_acquire(f) != epoch) {
+          if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
+          if (spins > 16) {
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+          }
+        }
+      }
+      __syncwarp();
+      const int64_t eend = live ? A.segend[k * SPT_ROWS + lane] : 0;
+      int64_t q = e + w;
+      for (; q + 3 * SPW_WARPS < eend; q += 4 * SPW_WARPS) {
+        int64_t j[4];
+        cplx v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          j[u] = A.col[q + u * SPW_WARPS];
+          v[u] = A.val[q + u * SPW_WARPS];
+        }
+        cplx xv[4][K];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < K; ++c) xv[u][c] = __ldcg(&out[(int64_t)c * ldo + j[u]]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < K; ++c) acc[c] = cfma(v[u], xv[u][c], acc[c]);
+      }
+      for (; q < eend; q += SPW_WARPS) {
+        const int64_t jj = A.col[q];
+        const cplx vv = A.val[q];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] = cfma(vv, __ldcg(&out[(int64_t)c * ldo + jj]), acc[c]);
+      }
+      e = eend;
+    }
+    if (w > 0) {
+#pragma unroll
+      for (int c = 0; c < K; ++c) sm_acc[w - 1][c][lane] = acc[c];
+    }
+    __syncthreads();
+    if (w == 0) {
+      cplx r[K], x[K];
+      cplx d = czero();
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        cplx s = acc[c];
+        for (int q = 0; q < SPW_WARPS - 1; ++q) s = cadd(s, sm_acc[q][c][lane]);
+        acc[c] = s;
+        r[c] = czero();
+        x[c] = czero();
+      }
+      if (live) {
+        d = A.dinv[i];
+        const int64_t src = gather ? gather[i] : i;
+#pragma unroll
+        for (int c = 0; c < K; ++c) r[c] = rhs[(int64_t)c * ldr + src];
+      }
+#pragma unroll 4
+      for (int qq = 0; qq < SPT_ROWS; ++qq) {
+        const int s = BACK ? (SPT_ROWS - 1 - qq) : qq;
+        const cplx ms = sm_m[s * SPT_ROWS + lane];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const cplx mine = cmul(csub(r[c], acc[c]), d);
+          cplx xs;
+          xs.x = __shfl_sync(0xffffffffu, mine.x, s);
+          xs.y = __shfl_sync(0xffffffffu, mine.y, s);
+          if (lane == s) x[c] = xs;
+          acc[c] = cfma(ms, xs, acc[c]);
+        }
+      }
+      if (live) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) out[(int64_t)c * ldo + i] = x[c];
+      }
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) spt_st_release(&flags[b * SPT_FLAG_STRIDE], epoch);
+    }
+    __syncthreads();
+  }
+}
