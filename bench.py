@@ -184,11 +184,13 @@ class ClockSampler:
 def column_offset(rank, world, nZ, col):
     """First traversal index of this rank's share: the traversal's columns (col = k points
     each, one grid column of a serpentine strip) are split into `world` near-equal contiguous
-    runs, and rank i starts its own traversal, with its own recycled space, at run i."""
-    ncols = -(-nZ // col)
-    if world > ncols:
-        raise SystemExit(f"{world} ranks for {ncols} columns of the traversal")
-    return min(nZ, (rank * ncols // world) * col)
+    runs, and rank i starts its own traversal, with its own recycled space, at run i
+    (rls_b200.distributed.column_shares, the library's rank split)."""
+    from rls_b200.distributed import column_shares
+    try:
+        return int(column_shares(nZ, col, world)[rank])
+    except ValueError as exc:
+        raise SystemExit(str(exc))
 
 
 def lane_plan(nZ, world, lanes, chunk, nsteps, col):

@@ -20,6 +20,7 @@ from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine
                       PsPrecRecyStats, PrecRecyRun, psPrecRecy)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
+from .distributed import psTriRecy_ranks, column_shares
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
@@ -27,5 +28,5 @@ __all__ = [
     "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
     "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
     "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException", "PsPrecRecyControl",
-    "PsPrecRecyStats", "PrecRecyRun", "psPrecRecy",
+    "PsPrecRecyStats", "PrecRecyRun", "psPrecRecy", "psTriRecy_ranks", "column_shares",
 ]

@@ -80,3 +80,51 @@ def test_column_shares_fit_ten_lanes_per_rank(world):
 def test_column_offset_rejects_more_ranks_than_columns():
     with pytest.raises(SystemExit):
         bench.column_offset(0, 2001, 200 * 200, 20)
+
+
+def _fake_solve(C_, sub, control, X0):
+    """Stands in for the per-rank GPU solve: σ = |z| + 1 and per-point counters from z."""
+    from rls_b200.solvers import PsTriRecyStats
+    st = PsTriRecyStats.alloc(len(sub.Z))
+    st.refine_it[:] = (np.round(sub.Z.real * 1000).astype(np.int64) % 7)
+    st.p_count[:] = np.arange(len(sub.Z))               # local index: shows each share restarts
+    st.n_it, st.n_pts = int(st.refine_it.sum()), len(sub.Z)
+    return np.abs(sub.Z) + 1.0, st
+
+
+def _ranks_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from datetime import timedelta
+    from rls_b200.grid import recursion_grid
+    from rls_b200.distributed import psTriRecy_ranks
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        rec = recursion_grid(0.45, 0.55, 0.0, 0.1, 30, 12, 4)
+        sig, st = psTriRecy_ranks(None, rec, solve=_fake_solve)
+        np.savez(os.path.join(out_dir, f"ranks{rank}.npz"), sig=sig, refine_it=st.refine_it, p_count=st.p_count,
+                 n_it=st.n_it, n_pts=st.n_pts)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_library_gather_of_rank_shares(tmp_path):
+    """rls_b200.distributed.psTriRecy_ranks on two gloo ranks: every rank ends with the whole
+    grid's σ and per-point statistics in rec.Z order, each share solved from its own start."""
+    import torch.multiprocessing as mp
+    from rls_b200.grid import recursion_grid
+    from rls_b200.distributed import column_shares
+    world = 2
+    mp.start_processes(_ranks_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    rec = recursion_grid(0.45, 0.55, 0.0, 0.1, 30, 12, 4)
+    offs = column_shares(len(rec.Z), rec.k, world)
+    ref_sig = np.abs(rec.Z) + 1.0
+    for r in range(world):
+        d = np.load(tmp_path / f"ranks{r}.npz")
+        assert np.array_equal(d["sig"], ref_sig)
+        assert np.array_equal(d["refine_it"], np.round(rec.Z.real * 1000).astype(np.int64) % 7)
+        local = np.concatenate([np.arange(offs[q + 1] - offs[q]) for q in range(world)])
+        assert np.array_equal(d["p_count"], local)
+        assert int(d["n_pts"]) == len(rec.Z)
+    assert offs[1] % rec.k == 0 and 0 < offs[1] < len(rec.Z)
