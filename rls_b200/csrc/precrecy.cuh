@@ -19,6 +19,7 @@
 //   K_ad⁻¹ = K⁻¹ + E·GramE⁻¹·Eᴴ   SparseLLTP_AD ldiv! (RLSPreconditioner.jl:229-262)
 #pragma once
 #include <functional>
+#include <map>
 
 struct PrecState {
   int64_t n = 0;
@@ -39,6 +40,15 @@ struct PrecState {
   cplx *hA = nullptr, *hv[2] = {nullptr, nullptr}, *hy = nullptr, *hpart = nullptr, *htau = nullptr;
   double *hd = nullptr, *he = nullptr, *he2 = nullptr, *hlu = nullptr;
   cplx* hG = nullptr;        // pr_max × r eigenvectors
+  cplx* hz = nullptr;        // the shift, read by the captured sequence
+  // the eigensolve's launch sequence for each order pr, captured once and replayed (its
+  // 2·(pr − 1) + 4 launches are fixed by pr; z is read from hz)
+  std::map<int, cudaGraphExec_t> heev_graphs;
+  void drop_graphs() {
+    for (auto& g : heev_graphs) cudaGraphExecDestroy(g.second);
+    heev_graphs.clear();
+  }
+  ~PrecState() { drop_graphs(); }
   // two-level preconditioner: GramE (r × r), its Cholesky inverse, coefficients
   cplx *gram = nullptr, *grinv = nullptr, *coef = nullptr, *coef2 = nullptr, *chol_ws = nullptr;
   // LOBPCG scratch (lob_scratch): shifted Cholesky-QR work for up to qcap columns, operator
@@ -412,16 +422,17 @@ int lobpcg_gen(rls_ctx* ctx, const DevOp& C, const std::function<int(cplx*, int)
 // ---- prediction recycled space ------------------------------------------------------------
 
 // Ritz pairs 1..nvec of Hz = H1 − zH2 − z̄H2ᴴ + |z|²H3 (pr × pr): λ into lam, G (pr × nvec, ld
-// pr_max) into ps.hG.  Householder tridiagonalisation, two launches per column (pred.cuh).
-int pred_heev(rls_ctx* ctx, int pr, cplx z, int nvec, double* lam) {
+// pr_max) into ps.hG.  Householder tridiagonalisation, two launches per column (pred.cuh).  The
+// launch sequence depends on pr only (z is read from ps.hz), so it is captured into a CUDA graph
+// the first time an order pr occurs and replayed after that: one graph launch instead of
+// 2·(pr − 1) + 4 kernel launches.
+int pred_heev_launches(rls_ctx* ctx, int pr, int nvec, double* lam) {
   PrecState& ps = *ctx->prec;
   const int ld = ps.pr_max;
   cplx* A = ps.hA;
   k_hz_build<<<std::max(1, std::min(1024, (pr * pr + 255) / 256)), 256, 0, ctx->stream>>>(
-      pr, ps.H1, ps.H2, ps.H3, ld, z, 0.0, A, pr);
+      pr, ps.H1, ps.H2, ps.H3, ld, ps.hz, 0.0, A, pr);
   RET(check_launch(ctx, "k_hz_build"));
-  cudaEvent_t e0 = nullptr;
-  prof_begin(ctx, KP_HEEV, &e0);
   if (pr > 1) {
     k_trd_first<<<1, 32, 0, ctx->stream>>>(pr, A, pr, ps.hv[0], ps.htau, ps.hd, ps.he);
     RET(check_launch(ctx, "k_trd_first"));
@@ -432,7 +443,6 @@ int pred_heev(rls_ctx* ctx, int pr, cplx z, int nvec, double* lam) {
       k_trd_symv<<<gs, 256, 0, ctx->stream>>>(k, pr, A, pr, ps.hv[k & 1], ps.htau, ps.hy, ps.hpart);
       k_trd_update<<<gu, 256, 0, ctx->stream>>>(k, pr, A, pr, ps.hv[k & 1], ps.htau, ps.hy, ps.hpart, gs,
                                                ps.hv[(k + 1) & 1], ps.hd, ps.he);
-      ctx->launches += 2;
     }
     RET(check_launch(ctx, "k_trd_update"));
   } else {
@@ -445,6 +455,33 @@ int pred_heev(rls_ctx* ctx, int pr, cplx z, int nvec, double* lam) {
     k_trd_backtransform<<<(nvec + 15) / 16, 256, 0, ctx->stream>>>(pr, A, pr, ps.htau, ps.hG, ld, nvec);
     RET(check_launch(ctx, "k_trd_backtransform"));
   }
+  return RLS_OK;
+}
+
+int pred_heev(rls_ctx* ctx, int pr, cplx z, int nvec, double* lam) {
+  PrecState& ps = *ctx->prec;
+  CK(cudaMemcpyAsync(ps.hz, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  auto it = ps.heev_graphs.find(pr);
+  if (it == ps.heev_graphs.end()) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = pred_heev_launches(ctx, pr, nvec, lam);
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    if (st != RLS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    CK(ce);
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    it = ps.heev_graphs.emplace(pr, ex).first;
+  }
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_HEEV, &e0);
+  CK(cudaGraphLaunch(it->second, ctx->stream));
+  ctx->launches += (pr > 1) ? 2 * (pr - 1) + 4 : 3;
   prof_end(ctx, KP_HEEV, e0, 16.0 / 3.0 * (double)pr * pr * pr);
   return RLS_OK;
 }
@@ -662,10 +699,11 @@ int lob_scratch(rls_ctx* ctx, int k3) {
 int prec_alloc(rls_ctx* ctx, int r, int p_max) {
   PrecState& ps = *ctx->prec;
   if (ps.V && ps.r == r && ps.p_max == p_max && ps.n == ctx->n) return RLS_OK;
+  ps.drop_graphs();          // they hold the old arrays' addresses
   for (cplx** a : {&ps.V, &ps.J1, &ps.J2, &ps.J3, &ps.J4, &ps.J5, &ps.J6, &ps.L, &ps.H1, &ps.H2, &ps.H3, &ps.Hs,
                    &ps.hA, &ps.Ulist, &ps.rot_ws, &ps.S, &ps.CS, &ps.G, &ps.R, &ps.E, &ps.X0, &ps.bS, &ps.bCS, &ps.bG,
                    &ps.bR, &ps.bX0, &ps.hv[0], &ps.hv[1], &ps.hy, &ps.hpart, &ps.htau, &ps.hG, &ps.gram, &ps.grinv,
-                   &ps.chol_ws, &ps.coef, &ps.coef2}) {
+                   &ps.chol_ws, &ps.coef, &ps.coef2, &ps.hz}) {
     dfree(ctx, *a);
     *a = nullptr;
   }
@@ -708,6 +746,7 @@ int prec_alloc(rls_ctx* ctx, int r, int p_max) {
   RET(dalloc_t(ctx, &ps.he2, (size_t)prm));
   RET(dalloc_t(ctx, &ps.hlu, (size_t)16 * 6 * prm));
   RET(dalloc_t(ctx, &ps.hG, (size_t)prm * r));
+  RET(dalloc_t(ctx, &ps.hz, 1));
   RET(dalloc_t(ctx, &ps.gram, (size_t)r * r));
   RET(dalloc_t(ctx, &ps.grinv, (size_t)r * r));
   RET(dalloc_t(ctx, &ps.chol_ws, (size_t)r * r));

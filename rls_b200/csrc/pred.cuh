@@ -124,9 +124,12 @@ __global__ void k_colnorm2(int64_t nrows, const cplx* __restrict__ A, int64_t ld
 // ------------------------------------------------------------------------------------
 // Hz = H1 − z·H2 − z̄·H2ᴴ + (|z|² + shift)·H3 (affine_conbine!, fastRaylRitz.jl:6-28) from the
 // upper triangles, written to both triangles of A (n×n, ld lda).  H3 == nullptr stands for I.
+// z is read from device memory, so that a captured launch sequence serves every shift.
 // ------------------------------------------------------------------------------------
 __global__ void k_hz_build(int n, const cplx* __restrict__ H1, const cplx* __restrict__ H2,
-                           const cplx* __restrict__ H3, int ldh, cplx z, double shift, cplx* A, int lda) {
+                           const cplx* __restrict__ H3, int ldh, const cplx* __restrict__ zp, double shift, cplx* A,
+                           int lda) {
+  const cplx z = *zp;
   const double zz = z.x * z.x + z.y * z.y + shift;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < (int64_t)n * n;
        q += (int64_t)gridDim.x * blockDim.x) {
