@@ -822,7 +822,7 @@ def run_precrecy(args):
                     "pred_update_s": st.pred_update_time_ns / 1e9, "main_recycle_s": st.main_recycle_time_ns / 1e9,
                     "pred_recycle_s": st.pred_recycle_time_ns / 1e9, "main_update_s": st.main_update_time_ns / 1e9}
     names = {1: "pred-stage eigensolve (tridiagonalisation + Sturm + inverse iteration)", 4: "host waits",
-             5: "k_spmm_shifted (C − zI and its adjoint)", 6: "IC preconditioner solves (k_sptrsv_blocks)"}
+             5: "k_spmm_shifted (C − zI and its adjoint)", 6: "IC preconditioner solves (k_sptrsv_wide)"}
     out["kernel_time_ms"] = {names[k]: {"launches": c, "ms": m} for k, (c, m, w) in prof.items() if k != 4}
     out["host_waits"] = {"count": prof[4][0], "ms": prof[4][1]}
     cnt, tot, work = prof[6]
