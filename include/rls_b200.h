@@ -247,6 +247,37 @@ int rls_reorder_to_natural_grid(const rls_grid* g, const rls_c64* Z, int64_t nZ,
  * Host memory. */
 int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t ldt);
 
+/* The sparse branch of psTriRecy (pre_process(C::SparseMatrixCSC), src/core/psTriRecy.jl:47-61;
+ * the refine's factor get_R_factor!, :222-234, SPQR's qr(M − zS).R with M = C[:, p], S = I[:, p]).
+ * Installs the square sparse C (n × n, the reference's CSC layout, indices base 0 or 1) as the
+ * context's operator in the form B = PᵀCP for the column order perm (new → old, base as the CSC;
+ * NULL: rls_band_order's choice).  rls_pstrirecy_schur(_range) and the lane entry points then
+ * run the sparse branch: the recycled space's products on B's CSR, and at each refine point R of
+ * B − zI = Pᵀ(M − zS), the R of the reference's M − zS up to row phases, by a banded Householder
+ * QR on the device, solved with the dataflow triangular solve on its band tiles.  σ, the Ritz
+ * vectors, X0 and the space are in the reference's frame (right singular vectors of M − zS).
+ * The lower bandwidth of B must be at most 1008 (RLS_ERR_DIM otherwise); device memory is about
+ * n·(3l + 2u)·16 bytes for the band and twice that of R's band tiles.  rls_set_schur,
+ * rls_sparse_upload_csc or rls_psprecrecy on the context drop this operator. */
+int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                       const rls_c64* nzval, int base, const int64_t* perm);
+
+/* The symmetric order rls_set_sparse_tri takes when perm is NULL: the natural order or the
+ * reverse Cuthill–McKee order of |C| + |Cᵀ|, whichever gives the smaller banded-QR work
+ * l·(l + u); perm receives it (new → old, base as the CSC), *l and *u (may be NULL) the
+ * bandwidths of PᵀCP.  It stands in for the reference's AMD order of CᴴC (psTriRecy.jl:52),
+ * which serves SPQR's fill, where a banded QR's fill is its band.  Errors: rls_last_error(NULL). */
+int rls_band_order(int64_t n, const int64_t* colptr, const int64_t* rowval, int base, int64_t* perm,
+                   int64_t* l, int64_t* u);
+
+/* psTriRecy(C::SparseMatrixCSC, rec; control) (psTriRecy.jl:889-913): rls_set_sparse_tri then
+ * rls_pstrirecy_schur over the whole traversal.  stats->qr_time_ns gets the factorisation time
+ * when control->collect_timing is set (one extra stream synchronisation per refine point). */
+int rls_pstrirecy_sparse(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                         const rls_c64* nzval, int base, const int64_t* perm, const rls_c64* Z, int64_t nZ,
+                         const rls_grid* g, const rls_pstrirecy_control* control, const rls_c64* X0,
+                         double* sigma_min, rls_pstrirecy_stats* stats);
+
 /* Installs on dst the operator already uploaded to src (same device).  The two contexts
  * share src's device tiles of T, which no call writes after the upload; the tiles are freed
  * with the last context that uses them, and a later rls_set_schur on either context gives

@@ -60,6 +60,11 @@ int rls_test_space_get(rls_ctx* ctx, int* p, rls_c64* V, rls_c64* J1, rls_c64* J
 int rls_test_recycle(rls_ctx* ctx, rls_c64 z, double shift, double gap_tau, int* rr, double* sigma, rls_c64* X,
                      rls_c64* W, double* w0norm);
 
+/* The band QR of a context given rls_set_sparse_tri: R of B − zI (B = PᵀCP) read back from the
+ * band tiles the triangular solve uses, as a dense upper-triangular n × n matrix (column-major,
+ * leading dimension ldr; zero outside the band), with the bandwidths l and u of B. */
+int rls_test_band_r(rls_ctx* ctx, rls_c64 z, rls_c64* R, int64_t ldr, int64_t* l, int64_t* u);
+
 #ifdef __cplusplus
 }
 #endif

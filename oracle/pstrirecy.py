@@ -107,6 +107,46 @@ class InvAdjR:
         return sla.solve_triangular(self.R, Y, lower=False, trans="N", check_finite=False)
 
 
+class SparseOp:
+    """A sparse M (SciPy) as an operator: mul M·X, mul_adj Mᴴ·Y."""
+
+    def __init__(self, A):
+        self.A = A.tocsr()
+        self.AH = A.conj().T.tocsr()
+
+    def mul(self, X):
+        return np.asarray(self.A @ X)
+
+    def mul_adj(self, Y):
+        return np.asarray(self.AH @ Y)
+
+
+class ColPermOp:
+    """S = I[:, p] (psTriRecy.jl:59-60): (S·X)[p[k]] = X[k], Sᴴ·Y = Y[p]."""
+
+    def __init__(self, p):
+        self.p = np.asarray(p)
+
+    def mul(self, X):
+        Y = np.zeros_like(X)
+        Y[self.p] = X
+        return Y
+
+    def mul_adj(self, Y):
+        return Y[self.p].copy()
+
+
+def pre_process_sparse(C, p):
+    """psTriRecy.jl:47-61 (sparse branch) with the column order p given (the reference takes
+    p = amd(lower(CᴴC))): M = C[:, p], S = I[:, p]."""
+    import scipy.sparse as sp
+    C = sp.csc_matrix(C, dtype=np.complex128)
+    n = C.shape[0]
+    M = C[:, p]
+    S = sp.identity(n, dtype=np.complex128, format="csc")[:, p]
+    return M, S
+
+
 def pre_process_dense(C):
     """psTriRecy.jl:6-14 (square branch): complex Schur T of C."""
     T, _ = sla.schur(np.asarray(C, dtype=np.complex128), output="complex")
@@ -132,12 +172,17 @@ class PsTriRecyRun:
     RNG stream is not reproducible here, so the caller supplies it.
     """
 
-    def __init__(self, T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False):
-        n = T.shape[0]
+    def __init__(self, T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False,
+                 sparse=None):
+        n = T.shape[0] if sparse is None else sparse[0].shape[0]
         self.ritz_g1_always = ritz_g1_always
         r = ctl.r
         self.T, self.rec, self.ctl, self.log = T, rec, ctl, log
-        self.M, self.S = TriOp(T), IdentityOp()
+        if sparse is None:
+            self.M, self.S = TriOp(T), IdentityOp()
+        else:   # (M, S) of pre_process_sparse
+            self.Msp, self.Ssp = sparse
+            self.M, self.S = SparseOp(self.Msp), ColPermOp(self.Ssp.tocoo().row[np.argsort(self.Ssp.tocoo().col)])
         self.rs = RecycledSpace(n, n, ctl.p, r, p_min=ctl.p_min)
         self.keep = LobpcgSvdKeep(n, n, r)
         if X0 is None:
@@ -155,8 +200,18 @@ class PsTriRecyRun:
         self.sigma_min = np.full(nZ, np.nan)
         self.st = PsTriRecyStats.alloc(nZ)
         self.last_failed = None
-        self.Rz = T.copy()
-        self.diagT = np.diag(T).copy()
+        if sparse is None:
+            self.Rz = T.copy()
+            self.diagT = np.diag(T).copy()
+
+    def shift_factor(self, z):
+        """get_R_factor!: T − zI on the dense Schur factor (psTriRecy.jl:87-99), or the R of
+        qr(M − zS) (ordering = 0) on the sparse branch (psTriRecy.jl:222-234)."""
+        if self.T is not None:
+            np.fill_diagonal(self.Rz, self.diagT - z)
+            return self.Rz
+        A = (self.Msp - z * self.Ssp).toarray()
+        return np.linalg.qr(A, mode="r")
 
     def run(self, i_begin=0, i_end=None):
         rec, ctl, rs, keep, st = self.rec, self.ctl, self.rs, self.keep, self.st
@@ -184,8 +239,8 @@ class PsTriRecyRun:
                         self.log(i, z, "recycled", rs.p, r_svdrr, self.sigma_min[i], 0)
                     continue
             t0 = time.perf_counter_ns()
-            np.fill_diagonal(self.Rz, self.diagT - z)            # get_R_factor! (psTriRecy.jl:87-99)
-            _, it = lobpcg_svd(InvAdjR(self.Rz), X, None, keep, self.ctl_main)
+            Rz = self.shift_factor(z)
+            _, it = lobpcg_svd(InvAdjR(Rz), X, None, keep, self.ctl_main)
             self.sigma_min[i] = keep.sigma[0]
             st.refine_it[i] = it
             if it > 0:
@@ -215,6 +270,13 @@ def ps_tri_recy_schur(T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, 
     """_psTriRecy_impl (psTriRecy.jl:708-881) on a precomputed Schur factor T.
     Returns (σ_min, stats)."""
     return PsTriRecyRun(T, rec, ctl, X0=X0, seed=seed, log=log, ritz_g1_always=ritz_g1_always).run()
+
+
+def ps_tri_recy_sparse(C, p, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False):
+    """_psTriRecy_impl on the sparse branch (M = C[:, p], S = I[:, p]; dense QR for the shifted
+    factor, small n only).  Returns (σ_min, stats)."""
+    return PsTriRecyRun(None, rec, ctl, X0=X0, seed=seed, log=log, ritz_g1_always=ritz_g1_always,
+                        sparse=pre_process_sparse(C, p)).run()
 
 
 def dense_sigma_min(C, z):

@@ -16,7 +16,7 @@ from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_g
                    recursion_grid_spiral, recursion_natural_permutation, reorder_to_natural,
                    reorder_to_natural_grid)
 from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
-                      SparseLLTP_AD, SchurFactor, pre_process, psTriRecy, ic_factor, get_hsl_LLTP, PsPrecRecyControl,
+                      SparseLLTP_AD, SchurFactor, SparseTri, band_order, pre_process, psTriRecy, ic_factor, get_hsl_LLTP, PsPrecRecyControl,
                       PsPrecRecyStats, PrecRecyRun, psPrecRecy)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
@@ -25,7 +25,8 @@ from .distributed import psTriRecy_ranks, column_shares
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
     "recursion_natural_permutation", "reorder_to_natural", "reorder_to_natural_grid", "PsTriRecyControl",
-    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "pre_process",
+    "PsTriRecyStats", "LobpcgSvdControl", "Engine", "Lanes", "ShiftedMat", "SparseLLTP", "SchurFactor", "SparseTri", "band_order",
+    "pre_process",
     "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
     "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException", "PsPrecRecyControl",
     "PsPrecRecyStats", "PrecRecyRun", "psPrecRecy", "psTriRecy_ranks", "column_shares",

@@ -93,6 +93,10 @@ SIGNATURES = {
     "rls_reorder_to_natural_grid": (C.c_int, [C.POINTER(rls_grid), P, C.c_int64, P, P]),
     "rls_set_schur": (C.c_int, [P, C.c_int64, P, C.c_int64]),
     "rls_set_schur_copy": (C.c_int, [P, P]),
+    "rls_set_sparse_tri": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P]),
+    "rls_band_order": (C.c_int, [C.c_int64, P, P, C.c_int, P, P, P]),
+    "rls_pstrirecy_sparse": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P, P, C.c_int64, C.POINTER(rls_grid),
+                                       C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),
     "rls_set_trsm_ctas": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_host_wait": (C.c_int, [P, C.c_int]),
     "rls_pstrirecy_schur": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P, P,
@@ -139,6 +143,7 @@ SIGNATURES = {
     "rls_test_svd_rr": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P, P]),
     "rls_test_heev_rr": (C.c_int, [P, C.c_int, C.c_int, P, P, c64, C.c_double, C.c_double, P, P, P, P]),
     "rls_test_recip": (C.c_int, [P, C.c_int64, P, P, P]),
+    "rls_test_band_r": (C.c_int, [P, c64, P, C.c_int64, P, P]),
     "rls_test_space_update": (C.c_int, [P, c64, P, C.c_double, C.c_int, C.c_int]),
     "rls_test_space_get": (C.c_int, [P, P, P, P, P, P, P, P, P]),
     "rls_test_recycle": (C.c_int, [P, c64, C.c_double, C.c_double, P, P, P, P, P]),

@@ -1,0 +1,236 @@
+// Householder QR of a banded shifted matrix on the device: the R factor that sparse psTriRecy
+// solves with at a refine point (get_R_factor!, src/core/psTriRecy.jl:222-234, which calls
+// SPQR's qr(M − zS).R on the host).
+//
+// The matrix is A = B − zI with B = PᵀCP, where the symmetric permutation P keeps C's entries
+// within lower bandwidth l and upper bandwidth u.  R does not depend on the row order of the
+// matrix it factors (QR of ΠA is (ΠQ)R), so R of PᵀCP − zI = Pᵀ(CP − zP) is the R of the
+// reference's M − zS with M = C[:, p], S = I[:, p], up to unit-modulus row phases that no
+// singular value or right singular vector sees.
+//
+// Storage (LAPACK band layout with room for the fill): kd = l + u is R's upper bandwidth;
+// column j keeps rows j−kd..j+l at AB[j·ldab + (i − j + kd)], ldab = kd + l + 1.  After the
+// factorisation R occupies rows j−kd..j of column j (its diagonal real, LAPACK zlarfg's β) and
+// the reflector tails rows j+1..j+l.
+//
+// Blocked right-looking QR with panels of w ≤ 8 columns:
+//   * k_bqr_panel: one CTA of 8 warps, the panel (rows c0..c0+mp−1, mp ≤ w + l) in shared
+//     memory, warp q owning column q.  Step s: warp s forms reflector s with zlarfg's
+//     conventions (β = −sign(Re α)·‖x‖, τ = (β − α)/β, v = x/(α − β)), leaving v below the
+//     diagonal of its column and β on it; after one barrier warps q > s apply H_sᴴ =
+//     I − conj(τ)vvᴴ to their columns and warps q < s form v_qᴴv_s.  Column s is final after
+//     step s, so one barrier per step suffices.  Then lane q of warp 0 builds row q of the
+//     forward block-reflector factor T (zlarft: T[s][s] = τ_s, T[0:s, s] =
+//     −τ_s·T[0:s, 0:s]·(V[:, 0:s]ᴴv_s)), so that H_0 H_1 … H_{w−1} = I − V T Vᴴ.
+//   * k_bqr_update: the trailing columns c0+w .. min(n, c0+mp+u)−1 (every column with a
+//     nonzero in the panel's rows) get C ← (I − V T Vᴴ)ᴴ C = C − V·Tᴴ·(VᴴC): eight columns per
+//     CTA, a warp per column streaming its rows from L2 twice (VᴴC, then the update) with V
+//     staged in shared memory.
+//   Entries above a column's band (row < j − kd) are never filled: a reflector of the panel
+//   reaches row c0+s only if its column has a nonzero at or below c0+s+l, i.e. j − u ≤ c0+s+l.
+#pragma once
+#include "common.cuh"
+#include "sparse.cuh"
+#include "blas.cuh"
+
+#define BQR_W 8                       // panel width (one warp per column)
+#define BQR_MAXL 1008                 // largest lower bandwidth: mp ≤ 1016 rows
+#define BQR_MAXROWS 1024              // row stride of the panel's reflector array
+#define BQR_UCOLS 8                   // trailing columns per update CTA (a warp each)
+
+// A ← 0, then the entries of B (CSR, rows of PᵀCP) in band layout, then A[j][j] −= z.
+__global__ void k_band_scatter(int64_t n, int64_t kd, int64_t ldab, CsrDev B, cplx* __restrict__ AB) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int64_t e = B.rowptr[i]; e < B.rowptr[i + 1]; ++e) {
+    const int64_t j = B.col[e];
+    AB[j * ldab + (i - j + kd)] = cadd(AB[j * ldab + (i - j + kd)], B.val[e]);   // duplicates sum
+  }
+}
+
+__global__ void k_band_shift(int64_t n, int64_t kd, int64_t ldab, cplx z, cplx* __restrict__ AB) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) AB[j * ldab + kd] = csub(AB[j * ldab + kd], z);
+}
+
+// Dynamic shared memory: w·mp cplx (column q at P + q·mp).
+__global__ void __launch_bounds__(32 * BQR_W) k_bqr_panel(int64_t l, int64_t kd, int64_t ldab, cplx* __restrict__ AB,
+                                                          int64_t c0, int w, int mp, cplx* __restrict__ Vp,
+                                                          cplx* __restrict__ Tm, int* err) {
+  extern __shared__ cplx P[];
+  __shared__ cplx taus[BQR_W];
+  __shared__ cplx Y[BQR_W][BQR_W + 1];   // Y[q][s] = v_qᴴ v_s (q < s)
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
+  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
+    const int qq = e / mp, i = e % mp;
+    P[e] = valid(i, qq) ? AB[(c0 + qq) * ldab + (i - qq + kd)] : czero();
+  }
+  __syncthreads();
+  cplx* Pq = P + (size_t)q * mp;
+  for (int s = 0; s < w; ++s) {
+    cplx* Ps = P + (size_t)s * mp;
+    const int iend = (int)min((int64_t)mp, (int64_t)s + l + 1);   // reflector s covers rows s..iend−1
+    if (q == s) {
+      const cplx alpha = Pq[s];   // read by every lane before the shuffles below (lane 0 rewrites it)
+      double xn2 = 0.0;
+      for (int i = s + 1 + lane; i < iend; i += 32) xn2 += cabs2(Pq[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
+      cplx tau = czero(), scale = czero();
+      double beta = alpha.x;
+      if (xn2 > 0.0 || alpha.y != 0.0) {
+        const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+        beta = (alpha.x >= 0.0) ? -nrm : nrm;
+        tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+        scale = cinv(csub(alpha, cmk(beta, 0.0)));
+      }
+      for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cmul(Pq[i], scale);
+      if (lane == 0) {
+        Pq[s] = cmk(beta, 0.0);
+        taus[s] = tau;
+        if (!isfinite(beta)) atomicOr(err, DEVERR_NONFINITE);
+      }
+    }
+    __syncthreads();
+    if (q < w && q > s) {
+      // H_sᴴ on column q: a ← a − conj(τ)·v·(vᴴa), v = (1, Ps[s+1..iend−1])
+      cplx d = czero();
+      for (int i = s + 1 + lane; i < iend; i += 32) d = cfma(cconj(Ps[i]), Pq[i], d);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        d.x += __shfl_xor_sync(0xffffffffu, d.x, o);
+        d.y += __shfl_xor_sync(0xffffffffu, d.y, o);
+      }
+      d = cadd(d, Pq[s]);
+      const cplx f = cmul(cconj(taus[s]), d);
+      __syncwarp();
+      for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cfms(Ps[i], f, Pq[i]);
+      if (lane == 0) Pq[s] = csub(Pq[s], f);
+    } else if (q < s) {
+      // v_qᴴ v_s over rows ≥ s (> q), where column q holds v_q
+      cplx y = czero();
+      for (int i = s + 1 + lane; i < iend; i += 32) y = cfma(cconj(Pq[i]), Ps[i], y);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        y.x += __shfl_xor_sync(0xffffffffu, y.x, o);
+        y.y += __shfl_xor_sync(0xffffffffu, y.y, o);
+      }
+      if (lane == 0) Y[q][s] = cadd(y, cconj(Pq[s]));
+    }
+  }
+  __syncthreads();
+  // write back: R rows ≤ q and reflector tails in place; V (unit diagonal, zero above) for
+  // the trailing update
+  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
+    const int qq = e / mp, i = e % mp;
+    const cplx v = P[e];
+    if (valid(i, qq)) AB[(c0 + qq) * ldab + (i - qq + kd)] = v;
+    Vp[(int64_t)qq * BQR_MAXROWS + i] = (i < qq) ? czero() : (i == qq ? cmk(1.0, 0.0) : v);
+  }
+  if (q == 0 && lane < BQR_W) {   // lane = row of T (Y is complete after the barrier above)
+    cplx trow[BQR_W];
+#pragma unroll
+    for (int s = 0; s < BQR_W; ++s) {
+      cplx tv = czero();
+      if (s < w) {
+        if (lane == s) {
+          tv = taus[s];
+        } else if (lane < s) {
+          cplx acc = czero();
+#pragma unroll
+          for (int k = 0; k < s; ++k)
+            if (k >= lane) acc = cfma(trow[k], Y[k][s], acc);
+          tv = cneg(cmul(taus[s], acc));
+        }
+      }
+      trow[s] = tv;
+      Tm[(int64_t)s * BQR_W + lane] = tv;
+    }
+  }
+}
+
+inline size_t bqr_panel_smem(int w, int mp) { return (size_t)w * mp * sizeof(cplx); }
+
+// C ← C − V·Tᴴ·(VᴴC) on the trailing columns jb .. je−1 (jb = c0 + w), rows c0 .. c0+mp−1.
+// Grid: ⌈(je − jb)/8⌉ CTAs of 8 warps, warp c on column jb + 8·blockIdx.x + c.
+// Dynamic shared memory: mp·w cplx of V (row i at Vs + i·w).
+__global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_t kd, int64_t ldab,
+                                                               cplx* __restrict__ AB, int64_t c0, int w, int mp,
+                                                               int64_t je, const cplx* __restrict__ Vp,
+                                                               const cplx* __restrict__ Tm) {
+  extern __shared__ cplx Vs[];
+  __shared__ cplx Ts[BQR_W * BQR_W];
+  for (int e = threadIdx.x; e < mp * w; e += blockDim.x) {
+    const int i = e / w, a = e % w;
+    Vs[e] = Vp[(int64_t)a * BQR_MAXROWS + i];
+  }
+  for (int e = threadIdx.x; e < BQR_W * BQR_W; e += blockDim.x) Ts[e] = Tm[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+  const int64_t jj = c0 + w + (int64_t)blockIdx.x * BQR_UCOLS + c;
+  if (jj >= je) return;
+  // rows of column jj inside its band: c0 + i ∈ [jj − kd, jj + l]
+  const int ilo = (int)max((int64_t)0, jj - kd - c0), ihi = (int)min((int64_t)mp, jj + l + 1 - c0);
+  cplx* col = AB + jj * ldab + (c0 - jj + kd);   // col[i] = A[c0 + i][jj]
+  cplx d[BQR_W];
+#pragma unroll
+  for (int a = 0; a < BQR_W; ++a) d[a] = czero();
+  for (int i = ilo + lane; i < ihi; i += 32) {
+    const cplx x = col[i];
+#pragma unroll
+    for (int a = 0; a < BQR_W; ++a) d[a] = cfma(cconj(Vs[i * w + min(a, w - 1)]), x, d[a]);
+  }
+#pragma unroll
+  for (int a = 0; a < BQR_W; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      d[a].x += __shfl_xor_sync(0xffffffffu, d[a].x, o);
+      d[a].y += __shfl_xor_sync(0xffffffffu, d[a].y, o);
+    }
+  }
+  // W = Tᴴ (VᴴC): W[a] = Σ_{k ≤ a} conj(T[k][a]) d[k]   (T column-major, ld BQR_W)
+  cplx W[BQR_W];
+#pragma unroll
+  for (int a = 0; a < BQR_W; ++a) {
+    cplx acc = czero();
+#pragma unroll
+    for (int k = 0; k <= a; ++k)
+      if (a < w) acc = cfma(cconj(Ts[a * BQR_W + k]), d[k], acc);
+    W[a] = acc;
+  }
+  for (int i = ilo + lane; i < ihi; i += 32) {
+    cplx x = col[i];
+#pragma unroll
+    for (int a = 0; a < BQR_W; ++a)
+      if (a < w) x = cfms(Vs[i * w + a], W[a], x);
+    col[i] = x;
+  }
+}
+
+inline size_t bqr_update_smem(int w, int mp) { return (size_t)mp * w * sizeof(cplx); }
+
+// Band tiles of R for the dataflow solve: tile (I, J), J − I ≤ bw, at slot tile_index_bw.
+// Grid: tile_slots(nb, bw) CTAs (unused slots return), 256 threads.
+__global__ void __launch_bounds__(256) k_band_tiles(int nb, int bw, int64_t n, int64_t kd, int64_t ldab,
+                                                    const cplx* __restrict__ AB, cplx* __restrict__ T) {
+  const int64_t idx = blockIdx.x;
+  int I, J;
+  if (bw >= nb - 1) {   // packed triangle: idx = J(J+1)/2 + I
+    J = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while ((int64_t)J * (J + 1) / 2 > idx) --J;
+    while ((int64_t)(J + 1) * (J + 2) / 2 <= idx) ++J;
+    I = (int)(idx - (int64_t)J * (J + 1) / 2);
+  } else {
+    J = (int)(idx / (bw + 1));
+    I = J - (int)(idx % (bw + 1));
+    if (I < 0) return;
+  }
+  cplx* tp = T + idx * (TILE * TILE);
+  for (int e = threadIdx.x; e < TILE * TILE; e += blockDim.x) {
+    const int rr = e % TILE, cc = e / TILE;
+    const int64_t gi = (int64_t)I * TILE + rr, gj = (int64_t)J * TILE + cc;
+    const bool in = gi < n && gj < n && gi <= gj && gj - gi <= kd;
+    tp[e] = in ? AB[gj * ldab + (gi - gj + kd)] : czero();
+  }
+}

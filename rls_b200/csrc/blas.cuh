@@ -16,6 +16,17 @@ __host__ __device__ __forceinline__ int64_t tile_index(int I, int J) {
   return (int64_t)J * (J + 1) / 2 + I;
 }
 
+// Tile slots of an upper-triangular factor whose tiles vanish beyond tile bandwidth bw
+// (J − I ≤ bw): the packed layout above when bw ≥ nb − 1, else tile (I, J) at slot
+// J·(bw + 1) + (J − I) (slots with J − I > J unused).  The banded R of a sparse shifted
+// factor uses the second form.
+__host__ __device__ __forceinline__ int64_t tile_index_bw(int I, int J, int nb, int bw) {
+  return (bw >= nb - 1) ? tile_index(I, J) : (int64_t)J * (bw + 1) + (J - I);
+}
+__host__ __device__ __forceinline__ int64_t tile_slots(int nb, int bw) {
+  return (bw >= nb - 1) ? (int64_t)nb * (nb + 1) / 2 : (int64_t)nb * (bw + 1);
+}
+
 // ------------------------------------------------------------------------------------
 // Gram: C (k1×k2) = alpha·AᴴB + beta·C in one launch.  Grid (row chunks, ceil(k1/8)):
 // warp w of CTA (c, g) owns column g·8+w of A and sums conj(A)·B over chunk c's rows,
@@ -287,13 +298,13 @@ __global__ void k_trmm_reduce(int nb, int k, const int* __restrict__ O_first, co
 // right-hand side, y_l is broadcast by shuffle and every lane updates its rows < l.
 // Pad rows (global row ≥ n) get 1 on the diagonal, so the pad stays inert.
 // Dynamic shared memory: TILE·TILE_LDS cplx.
-__global__ void __launch_bounds__(512) k_diag_inv(int nb, int64_t n, const cplx* __restrict__ T, cplx z,
+__global__ void __launch_bounds__(512) k_diag_inv(int nb, int bw, int64_t n, const cplx* __restrict__ T, cplx z,
                                                   cplx* __restrict__ Dinv, int* err) {
   extern __shared__ cplx sm[];
   cplx* sU = sm;                    // U[r][c] at sU[c*TILE_LDS + r], zero below the diagonal
   __shared__ cplx sdi[TILE];        // 1 / U[i][i]
   const int I = blockIdx.x;
-  const cplx* tp = T + tile_index(I, I) * (TILE * TILE);
+  const cplx* tp = T + tile_index_bw(I, I, nb, bw) * (TILE * TILE);
   for (int t = threadIdx.x; t < TILE * TILE; t += blockDim.x) {
     const int rr = t % TILE, cc = t / TILE;
     const int64_t g = (int64_t)I * TILE + rr;
@@ -336,24 +347,31 @@ __global__ void __launch_bounds__(512) k_diag_inv(int nb, int64_t n, const cplx*
 // R = D·(I + G) the solves need no D⁻¹ product on their dependency chain:
 //   R x = b   ⇔  x_b = D_b⁻¹ b_b − Σ_{J>b} G(b,J) x_J
 //   Rᴴ x = b  ⇔  u_b = b_b − Σ_{J<b} G(J,b)ᴴ u_J,  x_b = D_b⁻ᴴ u_b.
-// Grid: two CTAs per tile slot (nb(nb+1)/2 slots), CTA h computing output rows
+// Grid: two CTAs per tile slot (tile_slots(nb, bw) slots), CTA h computing output rows
 // [32h, 32h+32); 256 threads.  Warp w owns the four rows 4w..4w+3 (A values broadcast),
 // lane the columns lane and lane+32.  D_I⁻¹ is upper triangular, so warp w sums only
 // l ≥ 32h + 4w (a warp-uniform start).  The result is staged in shared memory and
 // written out coalesced.
 // Dynamic shared memory (scale_smem_bytes): 64×33 + 64×65 cplx, two CTAs per SM.
 #define SC_ALD 33
-__global__ void __launch_bounds__(256) k_trsm_scale(const cplx* __restrict__ T, const cplx* __restrict__ Dinv,
-                                                    cplx* __restrict__ G) {
+__global__ void __launch_bounds__(256) k_trsm_scale(int nb, int bw, const cplx* __restrict__ T,
+                                                    const cplx* __restrict__ Dinv, cplx* __restrict__ G) {
   extern __shared__ cplx sm[];
   cplx* sA = sm;                      // D⁻¹[32h + i][l] at sA[l*SC_ALD + i]
   cplx* sB = sm + TILE * SC_ALD;      // T[l][c] at sB[c*TILE_LDS + l]; output staging afterwards
   const int64_t idx = blockIdx.x >> 1;
   const int h = blockIdx.x & 1;
-  int J = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
-  while ((int64_t)J * (J + 1) / 2 > idx) --J;
-  while ((int64_t)(J + 1) * (J + 2) / 2 <= idx) ++J;
-  const int I = (int)(idx - (int64_t)J * (J + 1) / 2);
+  int I, J;
+  if (bw >= nb - 1) {
+    J = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while ((int64_t)J * (J + 1) / 2 > idx) --J;
+    while ((int64_t)(J + 1) * (J + 2) / 2 <= idx) ++J;
+    I = (int)(idx - (int64_t)J * (J + 1) / 2);
+  } else {
+    J = (int)(idx / (bw + 1));
+    I = J - (int)(idx % (bw + 1));
+    if (I < 0) return;
+  }
   if (I >= J) return;
   const cplx* dp = Dinv + (int64_t)I * TILE * TILE;
   const cplx* tp = T + idx * (TILE * TILE);
@@ -479,7 +497,8 @@ __device__ __forceinline__ void half_product(const cplx* sA, const cplx* sX, cpl
 }
 
 template <int K>
-__global__ void __launch_bounds__(256) k_trsm_half(int nb, const cplx* __restrict__ G, const cplx* __restrict__ Dinv,
+__global__ void __launch_bounds__(256) k_trsm_half(int nb, int bw, const cplx* __restrict__ G,
+                                                   const cplx* __restrict__ Dinv,
                                                    const cplx* __restrict__ B, cplx* __restrict__ X, cplx* U,
                                                    int64_t ldx, int adj, int* __restrict__ ticket, int* flags,
                                                    int epoch, int* err) {
@@ -499,11 +518,15 @@ __global__ void __launch_bounds__(256) k_trsm_half(int nb, const cplx* __restric
     const int b = adj ? pos : (nb - 1 - pos);
     const int64_t r0 = (int64_t)b * TILE + h * 32;   // first row of this half
     cplx* out = adj ? U : X;                          // where the chain's values live
-    const int ndep = adj ? b : (nb - 1 - b);
+    // dependencies in the order they complete: J = b+1..min(nb−1, b+bw) from the far end
+    // (forward), J = max(0, b−bw)..b−1 (adjoint)
+    const int dlo = adj ? max(0, b - bw) : b + 1;
+    const int dhi = adj ? b - 1 : min(nb - 1, b + bw);
+    const int ndep = dhi - dlo + 1;
     HalfTile pf;
-    auto dep_of = [&](int d) { return adj ? d : (nb - 1 - d); };
+    auto dep_of = [&](int d) { return adj ? dlo + d : dhi - d; };
     auto tile_of = [&](int dep) {
-      return adj ? G + tile_index(dep, b) * (TILE * TILE) : G + tile_index(b, dep) * (TILE * TILE);
+      return adj ? G + tile_index_bw(dep, b, nb, bw) * (TILE * TILE) : G + tile_index_bw(b, dep, nb, bw) * (TILE * TILE);
     };
     if (ndep > 0) pf.load(tile_of(dep_of(0)), h, adj);
     // start value: D_b⁻¹ b_b (forward) or b_b (adjoint) on this half's rows

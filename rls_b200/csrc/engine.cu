@@ -24,6 +24,7 @@
 #include "rotate.cuh"
 #include "small.cuh"
 #include "sparse.cuh"
+#include "bandqr.cuh"
 #include "sptrsv.cuh"
 #include "pred.cuh"
 #include "host_err.h"
@@ -61,6 +62,7 @@ struct rls_ctx {
   cplx* trsm_u = nullptr;   // n_pad × 8: the adjoint solve's chain values
   cplx* grad_ws = nullptr;  // 3 × n_pad: rls_sigma_grad's vectors
   cplx z_dinv = cmk(NAN, NAN);
+  int tile_bw = 0;          // tile bandwidth of T and G (nb − 1: the full packed triangle)
   int* flags = nullptr;     // 2·nb (one per half block row)
   int* ticket = nullptr;    // 1
   int trsm_ctas = 0;        // CTAs of a triangular solve (0: one per half block row)
@@ -181,6 +183,17 @@ struct rls_ctx {
   // products M·V and Mᴴ·[J5 V] use the uploaded CSR instead of the Schur tiles); the
   // prediction stage, the preconditioner and the run state live in `prec`.
   bool op_sparse = false;
+  // Sparse psTriRecy (rls_pstrirecy_sparse): T holds the band tiles of R, the factor of the
+  // Householder QR of the permuted shifted matrix B − zI (B = PᵀCP, lower/upper bandwidths
+  // l, u), recomputed on the device at every new shift (bandqr.cuh).
+  struct Band {
+    bool on = false;
+    int64_t l = 0, u = 0, kd = 0, ldab = 0;
+    cplx* AB = nullptr;          // n × ldab band work array
+    cplx* Vp = nullptr;          // BQR_MAXROWS × BQR_W reflectors of one panel
+    cplx* Tm = nullptr;          // BQR_W × BQR_W block-reflector factor of one panel
+    cplx* tmp = nullptr;         // n_pad: (B − zI)v for the refine-point gradient
+  } band;
   int scratch_cols = 0;            // minimum column count the shared scratch serves (setup_space)
   PrecState* prec = nullptr;
 
@@ -632,13 +645,22 @@ int orth_robust(rls_ctx* ctx, int64_t nrows, const cplx* V, int64_t ldv, int nV,
 // Triangular operator (tiled Schur factor)
 // ---------------------------------------------------------------------------------
 
+int band_factor(rls_ctx* ctx, cplx z);
+void band_release(rls_ctx* ctx);
+
 int ensure_dinv(rls_ctx* ctx, cplx z) {
   if (ctx->z_dinv.x == z.x && ctx->z_dinv.y == z.y) return RLS_OK;
-  k_diag_inv<<<ctx->nb, 512, TILE * TILE_LDS * sizeof(cplx), ctx->stream>>>(ctx->nb, ctx->n, ctx->T, z, ctx->Dinv,
-                                                                            ctx->derr);
+  cplx zd = z;
+  if (ctx->band.on) {   // T ← tiles of R(z); its diagonal blocks already carry the shift
+    RET(band_factor(ctx, z));
+    zd = czero();
+  }
+  k_diag_inv<<<ctx->nb, 512, TILE * TILE_LDS * sizeof(cplx), ctx->stream>>>(ctx->nb, ctx->tile_bw, ctx->n, ctx->T,
+                                                                            zd, ctx->Dinv, ctx->derr);
   RET(check_launch(ctx, "k_diag_inv"));
-  const unsigned nslots = (unsigned)((int64_t)ctx->nb * (ctx->nb + 1) / 2);
-  k_trsm_scale<<<2 * nslots, 256, scale_smem_bytes(), ctx->stream>>>(ctx->T, ctx->Dinv, ctx->G);
+  const unsigned nslots = (unsigned)tile_slots(ctx->nb, ctx->tile_bw);
+  k_trsm_scale<<<2 * nslots, 256, scale_smem_bytes(), ctx->stream>>>(ctx->nb, ctx->tile_bw, ctx->T, ctx->Dinv,
+                                                                     ctx->G);
   RET(check_launch(ctx, "k_trsm_scale"));
   ctx->z_dinv = z;
   return RLS_OK;
@@ -669,7 +691,8 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
   const unsigned ctas = ctx->trsm_ctas > 0 ? std::min<unsigned>((unsigned)ctx->trsm_ctas, grid) : grid;
 #define RLS_TRSM_CASE(K)                                                                                         \
   case K:                                                                                                        \
-    k_trsm_half<K><<<ctas, 256, smem, ctx->stream>>>(ctx->nb, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, ld, adj,     \
+    k_trsm_half<K><<<ctas, 256, smem, ctx->stream>>>(ctx->nb, ctx->tile_bw, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, \
+                                                     ld, adj,                                                    \
                                                      ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);           \
     break;
   switch (k) {
@@ -678,8 +701,10 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
     default: set_err(ctx, "trsm: %d columns", k); return RLS_ERR_ARG;
   }
 #undef RLS_TRSM_CASE
-  // algorithmic bytes: the upper triangle of the factor once (n²/2 complex) + B read + X written
-  prof_end(ctx, KP_TRSM, e0, 16.0 * ((double)ctx->n * (ctx->n + 1) / 2 + 2.0 * (double)ctx->n * k));
+  // algorithmic bytes: the upper triangle (or band) of the factor once + B read + X written
+  const double fac = ctx->band.on ? (double)ctx->n * (double)(ctx->band.kd + 1)
+                                  : (double)ctx->n * (ctx->n + 1) / 2;
+  prof_end(ctx, KP_TRSM, e0, 16.0 * (fac + 2.0 * (double)ctx->n * k));
   RET(check_launch(ctx, "k_trsm_half"));
   if (adj) {
 #define RLS_FIN_CASE(K) \
@@ -696,6 +721,10 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
 
 // Y = T X (adj=0) or Tᴴ X (adj=1); k <= 16.
 int trmm(rls_ctx* ctx, int adj, const cplx* X, cplx* Y, int64_t ld, int k) {
+  if (ctx->band.on) {
+    set_err(ctx, "trmm: the banded factor has no triangular product");
+    return RLS_ERR_STATE;
+  }
   const size_t smem = ((size_t)TILE * TILE_LDS + (size_t)TILE * k) * sizeof(cplx);
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_TRMM, &e0);
@@ -1340,6 +1369,8 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_trtri, optin));
   RET(allow_big_smem(ctx, k_blockrot_apply_g, optin));
   RET(allow_big_smem(ctx, k_blockrot_left_g, optin));
+  RET(allow_big_smem(ctx, k_bqr_update, optin));
+  RET(allow_big_smem(ctx, k_bqr_panel, optin));
   return RLS_OK;
 }
 
@@ -1441,10 +1472,11 @@ namespace {
 // Installs an operator of order n whose tiles (packed layout, n_pad = 64·ceil(n/64)) are
 // either copied from host memory (`tiles`) or, when `shared` is set, another context's
 // device tiles used in place, and allocates the per-operator workspaces.
-int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<cplx> shared) {
+// Drops the operator (Schur tiles or the sparse band), its per-shift arrays and the space.
+int operator_drop(rls_ctx* ctx) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
-  // drop an old operator (freed with its last user) and space
+  // an old operator is freed with its last user
   ctx->T_buf.reset();
   ctx->T = nullptr;
   for (void* q : {(void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->grad_ws,
@@ -1453,13 +1485,28 @@ int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<c
                   (void*)ctx->trmm_Ocount[0], (void*)ctx->trmm_uO[1], (void*)ctx->trmm_us[1],
                   (void*)ctx->trmm_Ofirst[1], (void*)ctx->trmm_Ocount[1]})
     dfree(ctx, q);
+  ctx->Dinv = ctx->G = ctx->trsm_u = ctx->trmm_part = nullptr;
+  ctx->flags = ctx->ticket = nullptr;
+  ctx->colpart = nullptr;
+  for (int a = 0; a < 2; ++a) {
+    ctx->trmm_uO[a] = ctx->trmm_us[a] = ctx->trmm_Ofirst[a] = ctx->trmm_Ocount[a] = nullptr;
+    ctx->trmm_units[a] = 0;
+  }
   ctx->grad_ws = nullptr;
   release_space(ctx);
+  band_release(ctx);
   ctx->op_sparse = false;
+  ctx->z_dinv = cmk(NAN, NAN);
+  return RLS_OK;
+}
+
+int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<cplx> shared) {
+  RET(operator_drop(ctx));
   ctx->n = n;
   ctx->nb = (int)((n + TILE - 1) / TILE);
   ctx->n_pad = (int64_t)ctx->nb * TILE;
   const int nb = ctx->nb;
+  ctx->tile_bw = nb - 1;
   const size_t elems = (size_t)nb * (nb + 1) / 2 * TILE * TILE;
   if (shared) {
     ctx->T_buf = std::move(shared);
@@ -1561,6 +1608,10 @@ extern "C" int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src) {
   }
   if (src->device != dst->device) {
     set_err(dst, "rls_set_schur_copy: contexts on devices %d and %d", src->device, dst->device);
+    return RLS_ERR_ARG;
+  }
+  if (src->band.on) {
+    set_err(dst, "rls_set_schur_copy: the source context holds a sparse operator (call rls_set_sparse_tri on each)");
     return RLS_ERR_ARG;
   }
   if (src == dst) return RLS_OK;
@@ -1729,7 +1780,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
   rls_pstrirecy_stats dummy{};
   if (!st) st = &dummy;
   if (i_begin == 0) {
-    ctx->op_sparse = false;     // the space's products use the Schur tiles
+    ctx->op_sparse = ctx->band.on;   // the space's products: Schur tiles, or the CSR of B
     RET(setup_space(ctx, r, (int)ctl->p));
     RET(upload_x0(ctx, X0, r));
     // recycle_fail_dist_thresh (recySpace.jl:22-38)
@@ -1785,10 +1836,26 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
   auto refine = [&](int64_t i, int r_svdrr) -> int {
     const cplx z = cmk(Z[i].re, Z[i].im);
     const uint64_t t1 = now_ns();
+    uint64_t qr_ns = 0;
+    if (ctx->band.on && ctl->collect_timing) {   // the sparse QR timed apart (psTriRecy.jl:515-530)
+      RET(ensure_dinv(ctx, z));
+      RET(sync_and_check(ctx));
+      qr_ns = now_ns() - t1;
+      st->qr_time_ns += qr_ns;
+    }
     LobpcgResult lres{};
     RET(lobpcg_invtri(ctx, z, r, 2000, lob_tol, true, &lres));
     double s0 = 0.0;
-    if (ctx->grad_on) {   // uᴴv = σ·(CX[:,1])ᴴX[:,1] (CX = R⁻ᴴX = u/σ at convergence)
+    if (ctx->grad_on && ctx->band.on) {
+      // R⁻ᴴX is Qᴴu/σ here: take w = ((B − zI)v)ᴴv = σ·uᴴv from one product instead
+      const int64_t np = ctx->n_pad;
+      RET(spmm_dev(ctx, cneg(z), 0, 1, ctx->S, np, ctx->band.tmp, np));
+      RET(gram(ctx, np, ctx->band.tmp, np, 1, ctx->S, np, 1, ctx->small[7], 1));
+      cplx w{0, 0};
+      RET(d2h2(ctx, &s0, ctx->sig, 1, &w, ctx->small[7], 1));   // keep.σ[1] = σ (side 'L')
+      if (st->dsdx) st->dsdx[i] = (s0 > 0.0) ? -w.x / s0 : 0.0;
+      if (st->dsdy) st->dsdy[i] = (s0 > 0.0) ? w.y / s0 : 0.0;
+    } else if (ctx->grad_on) {   // uᴴv = σ·(CX[:,1])ᴴX[:,1] (CX = R⁻ᴴX = u/σ at convergence)
       RET(gram(ctx, ctx->n_pad, ctx->CS, ctx->n_pad, 1, ctx->S, ctx->n_pad, 1, ctx->small[7], 1));
       cplx w{0, 0};
       RET(d2h2(ctx, &s0, ctx->sig, 1, &w, ctx->small[7], 1));
@@ -1802,7 +1869,7 @@ extern "C" int rls_pstrirecy_schur_range(rls_ctx* ctx, const rls_c64* Z, int64_t
     int64_t m_apps = 0, r_apps = 0;
     if (st->refine_it) st->refine_it[i] = it;
     if (it > 0) r_apps += 2 * r + it * r + (it - 1) * r;
-    st->refine_time_ns += now_ns() - t1;
+    st->refine_time_ns += now_ns() - t1 - qr_ns;
     st->n_it += it;
     if (st->pts) st->pts[st->n_pts] = Z[i];
     st->n_pts += 1;
@@ -1959,6 +2026,7 @@ extern "C" int rls_sparse_upload_csc(rls_ctx* ctx, int64_t m, int64_t n, const i
     }
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->band.on) RET(operator_drop(ctx));   // its band factor belongs to the old matrix
   for (auto& a : ctx->sp) {
     dfree(ctx, a.rowptr);
     dfree(ctx, a.col);
@@ -2770,6 +2838,7 @@ extern "C" int rls_tsqr_r_noalloc(const rls_c64* A, int64_t lda, int64_t m, int 
   return RLS_OK;
 }
 
+#include "sparsetri.cuh"
 #include "precrecy.cuh"
 #include "../../include/rls_b200_testing.h"
 #include "testing.cuh"

@@ -213,13 +213,14 @@ int invF_mul(rls_ctx* ctx, int b, const cplx* X, cplx* Y) {
   PrecState& ps = *ctx->prec;
   const int64_t np = ctx->n_pad;
   RET(lltp_tri(ctx, 1, false, b, X, np, ps.opt2, np));
-  const unsigned gg = (unsigned)((ps.n + 255) / 256);
+  const int64_t nf = ctx->lltp.n;   // the factor's order (ps.n is set only by a psPrecRecy run)
+  const unsigned gg = (unsigned)((nf + 255) / 256);
   for (int c0 = 0; c0 < b; c0 += 8) {
     const int kk = std::min(8, b - c0);
     const cplx* W = ps.opt2 + (int64_t)c0 * np;
     cplx* Yc = Y + (int64_t)c0 * np;
 #define RLS_G_CASE(K) \
-  case K: k_gather_rows<K><<<gg, 256, 0, ctx->stream>>>(ps.n, ctx->lltp.invp, W, np, Yc, np); break;
+  case K: k_gather_rows<K><<<gg, 256, 0, ctx->stream>>>(nf, ctx->lltp.invp, W, np, Yc, np); break;
     switch (kk) {
       RLS_G_CASE(1) RLS_G_CASE(2) RLS_G_CASE(3) RLS_G_CASE(4)
       RLS_G_CASE(5) RLS_G_CASE(6) RLS_G_CASE(7) RLS_G_CASE(8)
@@ -318,7 +319,9 @@ int svd_rr_gen(rls_ctx* ctx, LobKeep& k, cplx* CSv, int nS, const LobCtl& c, boo
     RET(tsqr_r(ctx, np, CSv, np, nS, k.R));
     *cs_is_q = false;
   }
-  const bool glob = nS > 80;
+  // A and V in shared memory while they fit beside the r-wide work arrays (to 80 columns at
+  // small r), else in the global scratch
+  const bool glob = nS > 80 || svd_rr_smem_bytes(nS, r, false) > kSvdSmemShared;
   k_svd_rr<<<1, 256, svd_rr_smem_bytes(nS, r, glob), ctx->stream>>>(nS, r, c.sideL ? 1 : 0, 1, k.R, nS, k.sig, k.lam,
                                                                    k.G, 3 * r, glob ? ctx->svdA : nullptr,
                                                                    glob ? ctx->svdV : nullptr);
@@ -863,7 +866,7 @@ extern "C" int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colp
       set_err(ctx, "rls_psprecrecy: C must be a square CSC of order >= 2 with base 0 or 1");
       return RLS_ERR_ARG;
     }
-    if (ctx->T && ctx->n != n) {
+    if (ctx->T && ctx->n != n && !ctx->band.on) {
       set_err(ctx, "rls_psprecrecy: the context holds a Schur operator of order %lld", (long long)ctx->n);
       return RLS_ERR_STATE;
     }

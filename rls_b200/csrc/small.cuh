@@ -391,6 +391,9 @@ __global__ void __launch_bounds__(256) k_svd_rr(int nS, int r, int sideL, int lq
   }
 }
 
+// Dynamic shared memory the shared-memory path of k_svd_rr may take (below the 227 KB opt-in).
+constexpr size_t kSvdSmemShared = 200 * 1024;
+
 inline size_t svd_rr_smem_bytes(int nS, int r, bool glob) {
   size_t s = ((size_t)2 * nS * r + r) * sizeof(cplx) + (size_t)nS * (2 * sizeof(double) + sizeof(int)) + 16;
   if (!glob) s += (size_t)2 * nS * nS * sizeof(cplx);

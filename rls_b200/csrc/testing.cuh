@@ -203,7 +203,7 @@ extern "C" int rls_test_svd_rr(rls_ctx* ctx, int nS, int r, int sideL, int lq, c
   double* dl = t.alloc<double>((size_t)nS);
   if (!dR || !dG || !ds || !dl) return RLS_ERR_NOMEM;
   CK(cudaMemcpyAsync(dR, R, sizeof(cplx) * nS * nS, cudaMemcpyHostToDevice, ctx->stream));
-  const bool glob = nS > 80;
+  const bool glob = nS > 80 || svd_rr_smem_bytes(nS, r, false) > kSvdSmemShared;
   cplx* gA = glob ? t.alloc<cplx>((size_t)nS * nS) : nullptr;
   cplx* gV = glob ? t.alloc<cplx>((size_t)nS * nS) : nullptr;
   k_svd_rr<<<1, 256, svd_rr_smem_bytes(nS, r, glob), ctx->stream>>>(nS, r, sideL, lq, dR, nS, ds, dl, dG, nS, gA, gV);
@@ -326,4 +326,36 @@ extern "C" int rls_test_recip(rls_ctx* ctx, int64_t n, const double* q, double* 
   CK(cudaMemcpyAsync(r_nr, d1, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(r_div, d2, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   return sync_and_check(ctx);
+}
+
+extern "C" int rls_test_band_r(rls_ctx* ctx, rls_c64 z, rls_c64* R, int64_t ldr, int64_t* l, int64_t* u) {
+  if (!ctx || !R) return RLS_ERR_ARG;
+  if (!ctx->band.on) {
+    set_err(ctx, "rls_test_band_r: no sparse operator (call rls_set_sparse_tri first)");
+    return RLS_ERR_STATE;
+  }
+  const int64_t n = ctx->n;
+  if (ldr < n) return RLS_ERR_DIM;
+  CK(cudaSetDevice(ctx->device));
+  ctx->z_dinv = cmk(NAN, NAN);
+  RET(ensure_dinv(ctx, cmk(z.re, z.im)));
+  const int nb = ctx->nb, bw = ctx->tile_bw;
+  const size_t slots = (size_t)tile_slots(nb, bw);
+  std::vector<cplx> h(slots * TILE * TILE);
+  CK(cudaMemcpyAsync(h.data(), ctx->T, sizeof(cplx) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  RET(sync_and_check(ctx));
+  for (int64_t j = 0; j < n; ++j)
+    for (int64_t i = 0; i < n; ++i) R[j * ldr + i] = rls_c64{0.0, 0.0};
+  for (int J = 0; J < nb; ++J)
+    for (int I = std::max(0, J - bw); I <= J; ++I) {
+      const cplx* tp = h.data() + tile_index_bw(I, J, nb, bw) * TILE * TILE;
+      for (int cc = 0; cc < TILE; ++cc)
+        for (int rr = 0; rr < TILE; ++rr) {
+          const int64_t gi = (int64_t)I * TILE + rr, gj = (int64_t)J * TILE + cc;
+          if (gi < n && gj < n) R[gj * ldr + gi] = rls_c64{tp[cc * TILE + rr].x, tp[cc * TILE + rr].y};
+        }
+    }
+  if (l) *l = ctx->band.l;
+  if (u) *u = ctx->band.u;
+  return RLS_OK;
 }

@@ -153,6 +153,47 @@ def pre_process(C_, return_q: bool = False):
     return (np.triu(T), Q) if return_q else np.triu(T)
 
 
+BAND_QR_MAX_L = 1008   # the device band QR's largest lower bandwidth (rls_set_sparse_tri)
+
+
+def _csc_arrays(C_):
+    import scipy.sparse as sp
+    A = sp.csc_matrix(C_, dtype=np.complex128)
+    A.sum_duplicates()
+    A.sort_indices()
+    if A.shape[0] != A.shape[1]:
+        raise DimensionMismatch(-2, f"pre_process only supports square matrices, got size {A.shape}")
+    return (A.shape[0], np.ascontiguousarray(A.indptr, dtype=np.int64),
+            np.ascontiguousarray(A.indices, dtype=np.int64), np.ascontiguousarray(A.data, dtype=np.complex128))
+
+
+def band_order(C_):
+    """The symmetric order sparse psTriRecy takes by default (rls_band_order): the natural or
+    the reverse Cuthill–McKee order of |C| + |Cᵀ|, whichever gives the smaller banded-QR work.
+    Returns (perm (new → old, 0-based), l, u), l and u the bandwidths of C[perm, perm]."""
+    n, colptr, rowval, _ = _csc_arrays(C_)
+    perm = np.zeros(n, dtype=np.int64)
+    l, u = C.c_int64(0), C.c_int64(0)
+    check(lib().rls_band_order(n, ptr(colptr), ptr(rowval), 0, ptr(perm), C.byref(l), C.byref(u)), None)
+    return perm, int(l.value), int(u.value)
+
+
+class SparseTri:
+    """A sparse C for psTriRecy's sparse branch (pre_process(C::SparseMatrixCSC),
+    psTriRecy.jl:47-61): the CSC arrays and the symmetric order P (perm, new → old; None:
+    band_order's).  Each Engine it is installed on holds B = PᵀCP and refactors R of B − zI on
+    the device at every refine point."""
+
+    def __init__(self, C_, perm=None):
+        self.n, self.colptr, self.rowval, self.nzval = _csc_arrays(C_)
+        if perm is None:
+            perm, self.l, self.u = band_order(C_)
+        else:
+            perm = np.ascontiguousarray(perm, dtype=np.int64)
+            self.l = self.u = None
+        self.perm = perm
+
+
 class SchurFactor:
     """A precomputed Schur factor T (skip pre_process on repeated runs)."""
 
@@ -193,6 +234,22 @@ class Engine:
         self._T_id = id(T)
         self._Q_id = None
         self.n = n
+
+    def set_sparse_tri(self, S: "SparseTri"):
+        """Installs a sparse C for psTriRecy's sparse branch (rls_set_sparse_tri)."""
+        check(lib().rls_set_sparse_tri(self._h, S.n, ptr(S.colptr), ptr(S.rowval), ptr(S.nzval), 0, ptr(S.perm)),
+              self._h)
+        self._T_id = None
+        self._Q_id = None
+        self.n = S.n
+
+    def band_r(self, z: complex):
+        """R of B − zI from the device band QR, dense (test hook rls_test_band_r), with (l, u)."""
+        n = self.n
+        R = np.zeros((n, n), dtype=np.complex128, order="F")
+        l, u = C.c_int64(0), C.c_int64(0)
+        check(lib().rls_test_band_r(self._h, c64(z), ptr(R), n, C.byref(l), C.byref(u)), self._h)
+        return R, int(l.value), int(u.value)
 
     def set_log(self, fn, verbose=1):
         if fn is None:
@@ -570,6 +627,11 @@ class Lanes:
             check(lib().rls_set_schur_copy(e._h, self.engines[0]._h), e._h)
             e.n = self.engines[0].n
 
+    def set_sparse_tri(self, S: "SparseTri"):
+        """Every lane holds its own B = PᵀCP and band factor (R changes with each lane's shift)."""
+        for e in self.engines:
+            e.set_sparse_tri(S)
+
     def set_batch(self, max_points: int):
         for e in self.engines:
             e.set_batch(max_points)
@@ -662,6 +724,11 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
               device: int = 0, lanes: int = 1, grad: bool = False):
     """psTriRecy (psTriRecy.jl:889-913) → (σ_min in rec.Z order, PsTriRecyStats).
 
+    A SciPy sparse C takes the sparse branch (SparseTri: B = PᵀCP, R of B − zI by the device
+    band QR at every refine point) when its ordered lower bandwidth is at most 1008, and the
+    dense Schur path otherwise (σ is invariant under the unitary similarity).  A dense C,
+    SchurFactor or SparseTri is used as given.
+
     ``X0`` (n × r) stands in for the reference's ``rand!(X)``; None draws a
     deterministic uniform [0,1) complex block on the device.  ``lanes`` > 1 splits the
     traversal on column boundaries into concurrent lanes on the same GPU (class Lanes);
@@ -669,27 +736,44 @@ def psTriRecy(C_, rec: Recursion, control: PsTriRecyControl = None, verbose: int
     ∂σ/∂Re z and ∂σ/∂Im z at every point from its own singular pair (no reference
     counterpart).
     """
+    import scipy.sparse as sp
     control = control or PsTriRecyControl()
     io = io if io is not None else sys.stdout
     if verbose >= 1:
         _print_startup(io, rec, control)
     t0 = time.perf_counter_ns()
-    if isinstance(C_, SchurFactor):
-        T = C_.T
-        pre_ns = C_.preprocess_time_ns
-    else:
-        T = pre_process(C_)
+    op = None
+    if isinstance(C_, (SchurFactor, SparseTri)):
+        op = C_
+        pre_ns = getattr(C_, "preprocess_time_ns", 0)
+    elif sp.issparse(C_):
+        S = SparseTri(C_)
+        if S.l <= BAND_QR_MAX_L:           # the sparse branch on the device band QR
+            op = S
+        else:                              # too wide a band: the unitarily equivalent Schur form
+            op = SchurFactor(pre_process(C_))
         pre_ns = time.perf_counter_ns() - t0
+    else:
+        op = SchurFactor(pre_process(C_))
+        pre_ns = time.perf_counter_ns() - t0
+
+    def install(target):
+        if isinstance(op, SparseTri):
+            target.set_sparse_tri(op)
+        else:
+            target.set_schur(op.T)
+
     if lanes > 1:
-        ls = Lanes(lanes, device, T)
+        ls = Lanes(lanes, device)
         try:
+            install(ls)
             sigma, st = ls.pstrirecy(rec, control, X0=X0, grad=grad)
         finally:
             ls.close()
         st.preprocess_time_ns = pre_ns
         return sigma, st
     eng = _engine(device)
-    eng.set_schur(T)
+    install(eng)
     if verbose >= 1:
         eng.set_log(lambda line: (io.write(line + "\n"), io.write("-" * 100 + "\n")), verbose)
     else:
