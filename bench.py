@@ -87,7 +87,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sprand4000", choices=["sprand4000", "laser5000", "af23560"],
+    ap.add_argument("--workload", default="sprand4000", choices=["sprand4000", "laser5000", "af23560", "skewlap3d"],
                     help="sprand4000 (default, the headline), laser5000 (dense laser operator), af23560 "
                          "(psPrecRecy on the af23560-shaped synthetic matrix)")
     ap.add_argument("--chunk", type=int, default=200,
@@ -96,7 +96,7 @@ def parse():
     ap.add_argument("--trsm-ctas", type=int, default=0,
                     help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
-    ap.add_argument("--pp-chunk", type=int, default=10, help="grid points per step of the af23560 (psPrecRecy) leg")
+    ap.add_argument("--pp-chunk", type=int, default=100, help="grid points per step of the af23560 (psPrecRecy) leg")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=None, help="matrix order (default: the workload's)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -654,6 +654,9 @@ def main():
     if args.workload == "af23560":
         run_precrecy(args)
         return
+    if args.workload == "skewlap3d":
+        run_sparse_tri(args)
+        return
     select_workload(args.workload)
     if args.n is None:
         args.n = N_MAT
@@ -866,6 +869,225 @@ def run_precrecy(args):
                                          f"restatement (SciPy sparse solves, LAPACK; IC by the C++ host build), "
                                          f"{el:.1f} s"}
     print(json.dumps(out), flush=True)
+
+
+
+# ---- psTriRecy's sparse branch on the 3-D skew Laplacian ---------------------------------------
+
+SKEW_GRID = (-550.0, 100.0, -200.0, 200.0, 200, 200, 20)
+
+
+def run_sparse_tri(args):
+    """psTriRecy on the sparse skewlap3d matrix (example/skewlap3d/skewlap3d.jl: N = 25,
+    n = 24³ = 13,824, normC = 7471.59; skewlap3d_psTriRecy.jl's control), 200 × 200 grid, k = 20,
+    with ∂σ/∂z at every point: the sparse branch (B = PᵀCP, band QR of B − zI per refine point)
+    on concurrent lanes, steps of --chunk lane-local points as in the dense workloads."""
+    import torch
+    import torch.distributed as dist
+    import rls_b200 as R
+    from rls_b200.examples import skewlap3d, SKEWLAP_NORMC
+    from rls_b200.solvers import PsTriRecyControl, PsTriRecyStats
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    C = skewlap3d(25)
+    n = C.shape[0]
+    normC = SKEWLAP_NORMC
+    rec = R.recursion_grid(*SKEW_GRID)
+    col = SKEW_GRID[6]
+    desc = ("psTriRecy sparse branch, skewlap3d N=25 (n=13824, 7-point skew Laplacian, normC=7471.59), 200x200 grid "
+            "[-550,100]x[-200,200], k=20, tol=1e-4, p=60, r=6, recy_tau=1.6, dsigma/dz at every point")
+    out = {"metric": "σ_min grid pts/s (psTriRecy sparse, skewlap3d n=13824, 200×200 grid, k=20, tol 1e-4)",
+           "unit": "pts/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+           "data": "synthetic (skewlap3d.jl's matrix: N²·tridiag(1.5, −2, 0.5) in each of three Kronecker directions)",
+           "config": {"workload": desc, "n": n, "nnz": int(C.nnz), "grid": list(SKEW_GRID)}}
+    ctl = PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=60, recy_tau=1.6, implict_recycle=True)
+    rng = np.random.default_rng(1 + rank)
+    X0 = rng.random((n, 6)) + 1j * rng.random((n, 6))
+    nst = args.warmup + args.steps
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import recugrid as G
+        import oracle.pstrirecy as OP
+        t0 = time.perf_counter()
+        p, l, u = R.band_order(C)
+        run = OP.PsTriRecyRun(None, G.recursion_grid(*SKEW_GRID),
+                              OP.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=60, recy_tau=1.6), X0=X0,
+                              sparse=OP.pre_process_sparse(C, p), factor="lu")
+        pre_s = time.perf_counter() - t0
+        rs = args.ref_chunk
+        for w in range(args.warmup):
+            run.run(w * rs, (w + 1) * rs)
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            a = (args.warmup + k) * rs
+            run.run(a, a + rs)
+        el = time.perf_counter() - t0
+        v = args.steps * rs / el
+        out.update({"impl": "reference", "value": v, "ms_per_step": el * 1e3 / args.steps, "preprocess_s": pre_s,
+                    "cpu_baseline": {"value": v, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+                                     "sample": f"{rs} points per step after {args.warmup} warm-up steps; CPU "
+                                               "restatement of the sparse branch with a SuperLU operator in place "
+                                               "of SPQR's R (same σ and right singular vectors), all host threads"},
+                    "e2e": {"value": v, "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        out["config"]["points_per_step"] = rs
+        print(json.dumps(out), flush=True)
+        return
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    t0 = time.perf_counter()
+    S = R.SparseTri(C)
+    pre_s = time.perf_counter() - t0
+    off = column_offset(rank, world, len(rec.Z), col)
+    end = column_offset(rank + 1, world, len(rec.Z), col) if rank + 1 < world else len(rec.Z)
+    sub = R.Recursion(*SKEW_GRID)
+    sub.Z = np.ascontiguousarray(rec.Z[off:end])
+    lanes, s = lane_plan(len(rec.Z), world, args.lanes, args.chunk, nst, col)
+    need = nst * s
+
+    def timed(nl, profile):
+        ls = R.Lanes(nl, local)
+        ls.set_sparse_tri(S)
+        offs = ls.offsets(sub)
+        if need > int(np.min(np.diff(offs))):
+            raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds a lane of {int(np.min(np.diff(offs)))} points")
+        sig = np.full(len(sub.Z), np.nan)
+        st = PsTriRecyStats.alloc(len(sub.Z), grad=True)
+        cst = ls.engines[0].stats_struct(st)
+        for w in range(args.warmup):
+            ls.pstrirecy_range(sub, ctl, w * s, (w + 1) * s, sig, st, cst, X0=X0)
+        if profile:
+            ls.set_profile(True)
+        streams = [torch.cuda.ExternalStream(q) for q in ls.streams()]
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = None
+        if profile:
+            clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
+                               os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
+            clk.start()
+            time.sleep(0.3)
+        l0 = ls.launches()
+        for e, q in zip(ev0, streams):
+            e.record(q)
+        ls.pstrirecy_range(sub, ctl, args.warmup * s, need, sig, st, cst)
+        for e, q in zip(ev1, streams):
+            e.record(q)
+        for e in ev1:
+            e.synchronize()
+        torch.cuda.synchronize()
+        l1 = ls.launches()
+        if clk is not None:
+            clk.stop()
+        if world > 1:
+            dist.barrier()
+        ms = max(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+        tim = np.concatenate([np.arange(o + args.warmup * s, o + need) for o in offs[:-1]])
+        res = {"ms": max_over_ranks(ms, world, "cuda"), "launches": int(l1 - l0), "sig": sig, "st": st, "timed": tim,
+               "clk": clk, "offs": offs}
+        if profile:
+            res["prof"] = {k: ls.profile(k) for k in (0, 1, 2, 5, 7)}
+            res["waits"] = ls.profile(4)
+        ls.close()
+        return res
+
+    single = timed(1, False) if lanes > 1 else None
+    main_ = timed(lanes, True)
+    ms = main_["ms"]
+    sig, st, tim, prof = main_["sig"], main_["st"], main_["timed"], main_["prof"]
+    value = world * lanes * args.steps * s / (ms / 1e3)
+    out["n_gpus"] = world
+    out.update({"value": value, "ms_per_step": ms / args.steps, "gpu_launches": main_["launches"],
+                "clocks": main_["clk"].summary(), "preprocess_s": pre_s})
+    out["config"].update({"points_per_step": lanes * s, "lanes": lanes, "chunk": s,
+                          "band": {"l": S.l, "u": S.u, "order": "reverse Cuthill-McKee of |C|+|Cᵀ| (band_order)"},
+                          "parallelism": f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU",
+                          "refine_fraction_timed": float(np.mean(st.refine_it[tim] > 0)),
+                          "l2": "the band array (n·(3l+2u+1)·16 B ≈ 0.3 GB) and R's band tiles exceed L2 (126 MB); "
+                                "every refine point rebuilds and streams them"})
+    if single is not None:
+        out["single_lane"] = {"value": world * args.steps * s / (single["ms"] / 1e3), "unit": "pts/s",
+                              "mode": "one traversal per GPU (the reference's single recycled space)"}
+    names = {0: "k_trsm_half on R's band tiles", 1: "k_heev_rr (projected eigensolve)",
+             2: "recycle step span", 5: "k_spmm_shifted (B and Bᴴ products of the space)",
+             7: "band QR of B − zI (k_bqr_panel + k_bqr_update, per refine point)"}
+    out["kernel_time_ms"] = {names[k]: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}
+    out["host_waits"] = {"count": main_["waits"][0], "ms": main_["waits"][1]}
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    cnt, tot, work = prof[0]
+    if cnt:
+        ach = (work / cnt) / (tot / cnt / 1e3) / 1e9
+        out["roofline"] = {"bound": "hbm", "kernel": names[0], "achieved": ach, "peak": hbm, "unit": "GB/s",
+                           "frac": ach / hbm, "traffic": None, "launches": cnt, "avg_us": tot / cnt * 1e3,
+                           "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    c7, t7, f7 = prof[7]
+    if c7:
+        out["band_qr_fp64"] = {"gflops": f7 / (t7 / 1e3) / 1e9, "launches": c7, "avg_ms": t7 / c7,
+                               "flops_per_factorisation": f7 / c7}
+    # gradient and σ at sampled timed points against the FP64 sparse-LU truth (after timing)
+    if args.accuracy_points > 0:
+        pick = tim[np.linspace(0, len(tim) - 1, min(args.accuracy_points, 24)).astype(np.int64)]
+        t0 = time.perf_counter()
+        truth, bound = sparse_truth(C, sub.Z[pick])
+        err = np.abs(sig[pick] - truth)
+        out["accuracy"] = {"points": int(pick.size), "max_abs_err": float(err.max()),
+                           "max_abs_err_over_normC": float(err.max() / normC),
+                           "max_rel_err": float(np.max(err / truth)), "within_bar": bool(err.max() <= 1e-4 * normC),
+                           "truth_max_err_bound": float(bound.max()),
+                           "truth": "block inverse iteration on (C−zI)ᴴ(C−zI), SciPy sparse LU (host)",
+                           "seconds": time.perf_counter() - t0}
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S2 = R.SparseTri(C)
+        ls2 = R.Lanes(lanes, local)
+        ls2.set_sparse_tri(S2)
+        sig2 = np.full(len(sub.Z), np.nan)
+        st2 = PsTriRecyStats.alloc(len(sub.Z), grad=True)
+        cst2 = ls2.engines[0].stats_struct(st2)
+        for k in range(nst):
+            ls2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sig2, st2, cst2, X0=X0)
+        el = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        ls2.close()
+        out["e2e"] = {"value": world * lanes * nst * s / el, "unit": "pts/s",
+                      "h2d_bytes_per_step": int((lanes * C.nnz * (16 + 8) + lanes * nst * s * 16) / nst),
+                      "d2h_bytes_per_step": int(lanes * s * 24),
+                      "span": f"band order + upload of C to each of {lanes} lanes + steps 0..{nst - 1} (σ and ∂σ/∂z "
+                              "out), wall clock",
+                      "matches_device_run": bool(np.allclose(sig2[tim], sig[tim], rtol=0, atol=1e-12))}
+    if rank == 0 and world == 1 and args.cpu_sample_s > 0:
+        from oracle import recugrid as G
+        import oracle.pstrirecy as OP
+        run = OP.PsTriRecyRun(None, G.recursion_grid(*SKEW_GRID),
+                              OP.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=60, recy_tau=1.6), X0=X0,
+                              sparse=OP.pre_process_sparse(C, S.perm), factor="lu")
+        t0 = time.perf_counter()
+        i = 0
+        while i < 4000 and (i < 2 or time.perf_counter() - t0 < args.cpu_sample_s):
+            run.run(i, i + 1)
+            i += 1
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": i / el, "unit": "pts/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"first {i} points of the traversal, CPU restatement of the sparse branch "
+                                         f"with a SuperLU operator in place of SPQR's R, {el:.1f} s"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -213,7 +213,8 @@ int rls_ctx_set_ritz_basis(rls_ctx* ctx, int g1_always);
  * milliseconds and algorithmic work (bytes; flops for kernel 1).  kernel 4
  * returns the host's blocking waits on the stream instead: their number and
  * total wall milliseconds (work = 0); kernel 5 is the sparse shifted product
- * (rls_spmm_shifted*); kernel 6 the preconditioner solve (rls_lltp_ldiv*).  No
+ * (rls_spmm_shifted*); kernel 6 the preconditioner solve (rls_lltp_ldiv*); kernel 7 the
+ * sparse branch's band QR of B − zI (work: 16·(l+1)·(l+u) flops per column).  No
  * reference counterpart (the reference times phases
  * with time_ns, psTriRecy.jl:306-309). */
 int rls_ctx_set_profile(rls_ctx* ctx, int on);

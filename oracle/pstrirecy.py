@@ -136,6 +136,23 @@ class ColPermOp:
         return Y[self.p].copy()
 
 
+class InvAdjLU:
+    """(M − zS)⁻ᴴ through SuperLU (scipy splu), for sparse sizes where a dense QR is out of
+    reach.  With M − zS = QR, R⁻ᴴ = Qᴴ·(M − zS)⁻ᴴ: the two operators differ by a unitary factor
+    on the left, so LOBPCG side 'L' finds the same σ and right singular vectors with either
+    (its Gram matrices and residuals see only CᴴC).  mul: (M − zS)⁻ᴴX, mul_adj: (M − zS)⁻¹Y."""
+
+    def __init__(self, A):
+        import scipy.sparse.linalg as spla
+        self.lu = spla.splu(A.tocsc())
+
+    def mul(self, X):
+        return self.lu.solve(np.ascontiguousarray(X), trans="H")
+
+    def mul_adj(self, Y):
+        return self.lu.solve(np.ascontiguousarray(Y))
+
+
 def pre_process_sparse(C, p):
     """psTriRecy.jl:47-61 (sparse branch) with the column order p given (the reference takes
     p = amd(lower(CᴴC))): M = C[:, p], S = I[:, p]."""
@@ -173,7 +190,7 @@ class PsTriRecyRun:
     """
 
     def __init__(self, T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False,
-                 sparse=None):
+                 sparse=None, factor="qr"):
         n = T.shape[0] if sparse is None else sparse[0].shape[0]
         self.ritz_g1_always = ritz_g1_always
         r = ctl.r
@@ -200,9 +217,17 @@ class PsTriRecyRun:
         self.sigma_min = np.full(nZ, np.nan)
         self.st = PsTriRecyStats.alloc(nZ)
         self.last_failed = None
+        self.factor = factor
         if sparse is None:
             self.Rz = T.copy()
             self.diagT = np.diag(T).copy()
+
+    def refine_operator(self, z):
+        """InvMat(adjoint(Rz)) (psTriRecy.jl:796-797); on the sparse branch with factor="lu"
+        the equivalent (M − zS)⁻ᴴ by sparse LU."""
+        if self.T is None and self.factor == "lu":
+            return InvAdjLU(self.Msp - z * self.Ssp)
+        return InvAdjR(self.shift_factor(z))
 
     def shift_factor(self, z):
         """get_R_factor!: T − zI on the dense Schur factor (psTriRecy.jl:87-99), or the R of
@@ -239,8 +264,7 @@ class PsTriRecyRun:
                         self.log(i, z, "recycled", rs.p, r_svdrr, self.sigma_min[i], 0)
                     continue
             t0 = time.perf_counter_ns()
-            Rz = self.shift_factor(z)
-            _, it = lobpcg_svd(InvAdjR(Rz), X, None, keep, self.ctl_main)
+            _, it = lobpcg_svd(self.refine_operator(z), X, None, keep, self.ctl_main)
             self.sigma_min[i] = keep.sigma[0]
             st.refine_it[i] = it
             if it > 0:
@@ -272,11 +296,13 @@ def ps_tri_recy_schur(T, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, 
     return PsTriRecyRun(T, rec, ctl, X0=X0, seed=seed, log=log, ritz_g1_always=ritz_g1_always).run()
 
 
-def ps_tri_recy_sparse(C, p, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False):
-    """_psTriRecy_impl on the sparse branch (M = C[:, p], S = I[:, p]; dense QR for the shifted
-    factor, small n only).  Returns (σ_min, stats)."""
+def ps_tri_recy_sparse(C, p, rec, ctl: PsTriRecyControl, X0=None, seed=0, log=None, ritz_g1_always=False,
+                       factor="qr"):
+    """_psTriRecy_impl on the sparse branch (M = C[:, p], S = I[:, p]).  The shifted factor is
+    the dense QR's R (factor="qr", small n) or the equivalent sparse LU operator (factor="lu").
+    Returns (σ_min, stats)."""
     return PsTriRecyRun(None, rec, ctl, X0=X0, seed=seed, log=log, ritz_g1_always=ritz_g1_always,
-                        sparse=pre_process_sparse(C, p)).run()
+                        sparse=pre_process_sparse(C, p), factor=factor).run()
 
 
 def dense_sigma_min(C, z):

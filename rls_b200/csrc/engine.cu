@@ -97,6 +97,7 @@ struct rls_ctx {
 
   // recycled space
   int r = 0, p_max = 0, pr_max = 0, p = 0;
+  int64_t space_np = 0;            // n_pad the space's tall arrays were sized for
   std::vector<rls_c64> pts;
   cplx *V = nullptr, *J1 = nullptr, *J2 = nullptr, *J5 = nullptr, *shift_tmp = nullptr;
   cplx *L = nullptr, *H1 = nullptr, *H2 = nullptr, *Hs = nullptr;  // pr_max²
@@ -158,7 +159,8 @@ struct rls_ctx {
     double ms = 0.0;
     double bytes = 0.0;
     std::vector<double> pending_bytes;
-  } kprof[7];                      // 0..3 kernels below, 4 unused (host waits), 5 sparse products
+  } kprof[8];                      // 0..3 kernels below, 4 unused (host waits), 5 sparse products,
+                                   // 6 preconditioner solves, 7 band QR
 
   rls_pstrirecy_stats lane_stats{};   // this context's run as one lane of rls_pstrirecy_schur_lanes_range
   CsrDev sp[2];                        // uploaded sparse C: [0] CSR of C, [1] CSR of Cᴴ
@@ -263,7 +265,7 @@ int check_launch(rls_ctx* ctx, const char* what) {
   return RLS_OK;
 }
 
-enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3, KP_SPMM = 5, KP_SPTRSV = 6 };
+enum { KP_TRSM = 0, KP_HEEV = 1, KP_RECYCLE_GEMM = 2, KP_TRMM = 3, KP_SPMM = 5, KP_SPTRSV = 6, KP_BANDQR = 7 };
 
 void prof_begin(rls_ctx* ctx, int id, cudaEvent_t* e0) {
   if (!ctx->profile) return;
@@ -769,7 +771,8 @@ void release_space(rls_ctx* ctx) {
 }
 
 int setup_space(rls_ctx* ctx, int r, int p_max) {
-  if (ctx->r == r && ctx->p_max == p_max && ctx->V && ctx->small_dim >= std::max(ctx->scratch_cols, 1)) {
+  if (ctx->r == r && ctx->p_max == p_max && ctx->V && ctx->space_np == ctx->n_pad &&
+      ctx->small_dim >= std::max(ctx->scratch_cols, 1)) {
     ctx->p = 0;
     ctx->pts.assign(p_max, rls_c64{0, 0});
     return RLS_OK;
@@ -778,6 +781,7 @@ int setup_space(rls_ctx* ctx, int r, int p_max) {
   ctx->r = r;
   ctx->p_max = p_max;
   ctx->pr_max = r * p_max;
+  ctx->space_np = ctx->n_pad;
   ctx->p = 0;
   ctx->pts.assign(p_max, rls_c64{0, 0});
   const int64_t np = ctx->n_pad;
@@ -2685,7 +2689,7 @@ extern "C" int rls_ctx_set_profile(rls_ctx* ctx, int on) {
 }
 
 extern "C" int rls_ctx_profile_get(rls_ctx* ctx, int kernel, int64_t* count, double* total_ms, double* work) {
-  if (!ctx || kernel < 0 || kernel > 6) return RLS_ERR_ARG;
+  if (!ctx || kernel < 0 || kernel > 7) return RLS_ERR_ARG;
   RET(sync_and_check(ctx));
   prof_resolve(ctx);
   if (kernel == 4) {

@@ -29,6 +29,8 @@ void band_release(rls_ctx* ctx) {
 int band_factor(rls_ctx* ctx, cplx z) {
   auto& B = ctx->band;
   const int64_t n = ctx->n;
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_BANDQR, &e0);
   CK(cudaMemsetAsync(B.AB, 0, sizeof(cplx) * (size_t)n * (size_t)B.ldab, ctx->stream));
   const unsigned gr = (unsigned)((n + 255) / 256);
   k_band_scatter<<<gr, 256, 0, ctx->stream>>>(n, B.kd, B.ldab, ctx->sp[0], B.AB);
@@ -46,6 +48,8 @@ int band_factor(rls_ctx* ctx, cplx z) {
                      ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm);
   }
   RET(check_launch(ctx, "k_bqr_panel/k_bqr_update"));
+  // algorithmic flops: per column, a reflector of l + 1 rows onto l + u columns (dot + update)
+  prof_end(ctx, KP_BANDQR, e0, 16.0 * (double)(B.l + 1) * (double)(B.l + B.u) * (double)n);
   k_band_tiles<<<(unsigned)tile_slots(ctx->nb, ctx->tile_bw), 256, 0, ctx->stream>>>(ctx->nb, ctx->tile_bw, n, B.kd,
                                                                                      B.ldab, B.AB, ctx->T);
   return check_launch(ctx, "k_band_tiles");

@@ -248,7 +248,8 @@ class Engine:
         n = self.n
         R = np.zeros((n, n), dtype=np.complex128, order="F")
         l, u = C.c_int64(0), C.c_int64(0)
-        check(lib().rls_test_band_r(self._h, c64(z), ptr(R), n, C.byref(l), C.byref(u)), self._h)
+        z = complex(z)
+        check(lib().rls_test_band_r(self._h, c64(z.real, z.imag), ptr(R), n, C.byref(l), C.byref(u)), self._h)
         return R, int(l.value), int(u.value)
 
     def set_log(self, fn, verbose=1):

@@ -83,3 +83,19 @@ def test_sparse_branch_restatement_matches_dense_svd_and_the_device_frame():
     assert np.array_equal(st_ms.r_recy, st_b.r_recy)
     assert np.array_equal(st_ms.p_count, st_b.p_count)
     assert 0 < int(np.sum(st_ms.refine_it > 0)) < len(rec.Z)
+
+
+def test_sparse_lu_operator_gives_the_qr_operators_results():
+    """The CPU baseline's sparse-LU operator (M − zS)⁻ᴴ and the reference's InvMat(Rᴴ) give the
+    same σ and the same decisions on the restatement."""
+    C, normC, grid = _skew_case(N=6, nx=6, k=3)
+    n = C.shape[0]
+    p, l, u = R.band_order(C)
+    rec = G.recursion_grid(*grid)
+    ctl = OP.PsTriRecyControl(normC=normC, tol=1e-4, p=10, p_min=1, recy_tau=1.6)
+    rng = np.random.default_rng(4)
+    X0 = rng.random((n, ctl.r)) + 1j * rng.random((n, ctl.r))
+    s_qr, st_qr = OP.ps_tri_recy_sparse(C, p, rec, ctl, X0=X0)
+    s_lu, st_lu = OP.ps_tri_recy_sparse(C, p, rec, ctl, X0=X0, factor="lu")
+    assert np.max(np.abs(s_qr - s_lu) / s_qr) <= 1e-8
+    assert np.array_equal(st_qr.refine_it > 0, st_lu.refine_it > 0)
