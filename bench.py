@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--pp-chunk", type=int, default=100, help="grid points per step of the af23560 (psPrecRecy) leg")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=None, help="matrix order (default: the workload's)")
+    ap.add_argument("--factor-only", type=int, default=0,
+                    help="skewlap3d: time this many band QR factorisations alone (one context) and exit")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmm", action="store_true", help="skip the sparse shifted product measurement")
     ap.add_argument("--no-ic", action="store_true", help="skip the IC preconditioner apply measurement")
@@ -936,6 +938,24 @@ def run_sparse_tri(args):
         print(json.dumps(out), flush=True)
         return
     torch.cuda.set_device(local)
+    if args.factor_only > 0:   # the refine's factorisation alone: R(z) of B − zI at successive grid points
+        if rank != 0:
+            return
+        S = R.SparseTri(C)
+        eng = R.Engine(local)
+        eng.set_sparse_tri(S)
+        eng.set_profile(True)
+        wall = []
+        for i in range(args.factor_only):
+            t0 = time.perf_counter()
+            eng.band_factor(rec.Z[i])
+            wall.append(time.perf_counter() - t0)
+        cnt, ms_, fl = eng.profile(7)
+        eng.close()
+        print(json.dumps({"workload": desc, "band": {"l": S.l, "u": S.u}, "factorisations": cnt,
+                          "device_ms_each": ms_ / max(cnt, 1), "gflops": fl / (ms_ / 1e3) / 1e9 if ms_ else None,
+                          "wall_ms": [w * 1e3 for w in wall]}), flush=True)
+        return
     if world > 1:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         from datetime import timedelta

@@ -64,6 +64,8 @@ int rls_test_recycle(rls_ctx* ctx, rls_c64 z, double shift, double gap_tau, int*
  * band tiles the triangular solve uses, as a dense upper-triangular n × n matrix (column-major,
  * leading dimension ldr; zero outside the band), with the bandwidths l and u of B. */
 int rls_test_band_r(rls_ctx* ctx, rls_c64 z, rls_c64* R, int64_t ldr, int64_t* l, int64_t* u);
+/* The same factorisation (and the solve's scaled band tiles) without the read-back. */
+int rls_test_band_factor(rls_ctx* ctx, rls_c64 z);
 
 #ifdef __cplusplus
 }

@@ -144,6 +144,7 @@ SIGNATURES = {
     "rls_test_heev_rr": (C.c_int, [P, C.c_int, C.c_int, P, P, c64, C.c_double, C.c_double, P, P, P, P]),
     "rls_test_recip": (C.c_int, [P, C.c_int64, P, P, P]),
     "rls_test_band_r": (C.c_int, [P, c64, P, C.c_int64, P, P]),
+    "rls_test_band_factor": (C.c_int, [P, c64]),
     "rls_test_space_update": (C.c_int, [P, c64, P, C.c_double, C.c_int, C.c_int]),
     "rls_test_space_get": (C.c_int, [P, P, P, P, P, P, P, P, P]),
     "rls_test_recycle": (C.c_int, [P, c64, C.c_double, C.c_double, P, P, P, P, P]),

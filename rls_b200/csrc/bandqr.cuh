@@ -13,8 +13,9 @@
 // factorisation R occupies rows j−kd..j of column j (its diagonal real, LAPACK zlarfg's β) and
 // the reflector tails rows j+1..j+l.
 //
-// Blocked right-looking QR with panels of w ≤ 8 columns:
-//   * k_bqr_panel: one CTA of 8 warps, the panel (rows c0..c0+mp−1, mp ≤ w + l) in shared
+// Blocked right-looking QR with panels of w ≤ W columns (W = 16 where a 16-column panel fits
+// in shared memory, else 8):
+//   * k_bqr_panel<W>: one CTA of W warps, the panel (rows c0..c0+mp−1, mp ≤ w + l) in shared
 //     memory, warp q owning column q.  Step s: warp s forms reflector s with zlarfg's
 //     conventions (β = −sign(Re α)·‖x‖, τ = (β − α)/β, v = x/(α − β)), leaving v below the
 //     diagonal of its column and β on it; after one barrier warps q > s apply H_sᴴ =
@@ -33,8 +34,8 @@
 #include "sparse.cuh"
 #include "blas.cuh"
 
-#define BQR_W 8                       // panel width (one warp per column)
-#define BQR_MAXL 1008                 // largest lower bandwidth: mp ≤ 1016 rows
+#define BQR_WMAX 16                   // widest panel (one warp per column)
+#define BQR_MAXL 1008                 // largest lower bandwidth: mp ≤ 1016 rows at W = 8
 #define BQR_MAXROWS 1024              // row stride of the panel's reflector array
 #define BQR_UCOLS 8                   // trailing columns per update CTA (a warp each)
 
@@ -48,18 +49,21 @@ __global__ void k_band_scatter(int64_t n, int64_t kd, int64_t ldab, CsrDev B, cp
   }
 }
 
-__global__ void k_band_shift(int64_t n, int64_t kd, int64_t ldab, cplx z, cplx* __restrict__ AB) {
+// The shift comes from device memory, so a captured factorisation serves every z.
+__global__ void k_band_shift(int64_t n, int64_t kd, int64_t ldab, const cplx* __restrict__ zp, cplx* __restrict__ AB) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const cplx z = *zp;
   if (j < n) AB[j * ldab + kd] = csub(AB[j * ldab + kd], z);
 }
 
-// Dynamic shared memory: w·mp cplx (column q at P + q·mp).
-__global__ void __launch_bounds__(32 * BQR_W) k_bqr_panel(int64_t l, int64_t kd, int64_t ldab, cplx* __restrict__ AB,
-                                                          int64_t c0, int w, int mp, cplx* __restrict__ Vp,
-                                                          cplx* __restrict__ Tm, int* err) {
+// Dynamic shared memory: w·mp cplx (column q at P + q·mp).  Tm: W × W, column-major, ld W.
+template <int W>
+__global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int64_t ldab, cplx* __restrict__ AB,
+                                                      int64_t c0, int w, int mp, cplx* __restrict__ Vp,
+                                                      cplx* __restrict__ Tm, int* err) {
   extern __shared__ cplx P[];
-  __shared__ cplx taus[BQR_W];
-  __shared__ cplx Y[BQR_W][BQR_W + 1];   // Y[q][s] = v_qᴴ v_s (q < s)
+  __shared__ cplx taus[W];
+  __shared__ cplx Y[W][W + 1];   // Y[q][s] = v_qᴴ v_s (q < s)
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
   auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
   for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
@@ -128,10 +132,10 @@ __global__ void __launch_bounds__(32 * BQR_W) k_bqr_panel(int64_t l, int64_t kd,
     if (valid(i, qq)) AB[(c0 + qq) * ldab + (i - qq + kd)] = v;
     Vp[(int64_t)qq * BQR_MAXROWS + i] = (i < qq) ? czero() : (i == qq ? cmk(1.0, 0.0) : v);
   }
-  if (q == 0 && lane < BQR_W) {   // lane = row of T (Y is complete after the barrier above)
-    cplx trow[BQR_W];
+  if (q == 0 && lane < W) {   // lane = row of T (Y is complete after the barrier above)
+    cplx trow[W];
 #pragma unroll
-    for (int s = 0; s < BQR_W; ++s) {
+    for (int s = 0; s < W; ++s) {
       cplx tv = czero();
       if (s < w) {
         if (lane == s) {
@@ -145,7 +149,7 @@ __global__ void __launch_bounds__(32 * BQR_W) k_bqr_panel(int64_t l, int64_t kd,
         }
       }
       trow[s] = tv;
-      Tm[(int64_t)s * BQR_W + lane] = tv;
+      Tm[(int64_t)s * W + lane] = tv;
     }
   }
 }
@@ -155,17 +159,18 @@ inline size_t bqr_panel_smem(int w, int mp) { return (size_t)w * mp * sizeof(cpl
 // C ← C − V·Tᴴ·(VᴴC) on the trailing columns jb .. je−1 (jb = c0 + w), rows c0 .. c0+mp−1.
 // Grid: ⌈(je − jb)/8⌉ CTAs of 8 warps, warp c on column jb + 8·blockIdx.x + c.
 // Dynamic shared memory: mp·w cplx of V (row i at Vs + i·w).
+template <int W>
 __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_t kd, int64_t ldab,
                                                                cplx* __restrict__ AB, int64_t c0, int w, int mp,
                                                                int64_t je, const cplx* __restrict__ Vp,
                                                                const cplx* __restrict__ Tm) {
   extern __shared__ cplx Vs[];
-  __shared__ cplx Ts[BQR_W * BQR_W];
+  __shared__ cplx Ts[W * W];
   for (int e = threadIdx.x; e < mp * w; e += blockDim.x) {
     const int i = e / w, a = e % w;
     Vs[e] = Vp[(int64_t)a * BQR_MAXROWS + i];
   }
-  for (int e = threadIdx.x; e < BQR_W * BQR_W; e += blockDim.x) Ts[e] = Tm[e];
+  for (int e = threadIdx.x; e < W * W; e += blockDim.x) Ts[e] = Tm[e];
   __syncthreads();
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   const int64_t jj = c0 + w + (int64_t)blockIdx.x * BQR_UCOLS + c;
@@ -173,37 +178,37 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
   // rows of column jj inside its band: c0 + i ∈ [jj − kd, jj + l]
   const int ilo = (int)max((int64_t)0, jj - kd - c0), ihi = (int)min((int64_t)mp, jj + l + 1 - c0);
   cplx* col = AB + jj * ldab + (c0 - jj + kd);   // col[i] = A[c0 + i][jj]
-  cplx d[BQR_W];
+  cplx d[W];
 #pragma unroll
-  for (int a = 0; a < BQR_W; ++a) d[a] = czero();
+  for (int a = 0; a < W; ++a) d[a] = czero();
   for (int i = ilo + lane; i < ihi; i += 32) {
     const cplx x = col[i];
 #pragma unroll
-    for (int a = 0; a < BQR_W; ++a) d[a] = cfma(cconj(Vs[i * w + min(a, w - 1)]), x, d[a]);
+    for (int a = 0; a < W; ++a) d[a] = cfma(cconj(Vs[i * w + min(a, w - 1)]), x, d[a]);
   }
 #pragma unroll
-  for (int a = 0; a < BQR_W; ++a) {
+  for (int a = 0; a < W; ++a) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       d[a].x += __shfl_xor_sync(0xffffffffu, d[a].x, o);
       d[a].y += __shfl_xor_sync(0xffffffffu, d[a].y, o);
     }
   }
-  // W = Tᴴ (VᴴC): W[a] = Σ_{k ≤ a} conj(T[k][a]) d[k]   (T column-major, ld BQR_W)
-  cplx W[BQR_W];
+  // Wc = Tᴴ (VᴴC): Wc[a] = Σ_{k ≤ a} conj(T[k][a]) d[k]   (T column-major, ld W)
+  cplx Wc[W];
 #pragma unroll
-  for (int a = 0; a < BQR_W; ++a) {
+  for (int a = 0; a < W; ++a) {
     cplx acc = czero();
 #pragma unroll
     for (int k = 0; k <= a; ++k)
-      if (a < w) acc = cfma(cconj(Ts[a * BQR_W + k]), d[k], acc);
-    W[a] = acc;
+      if (a < w) acc = cfma(cconj(Ts[a * W + k]), d[k], acc);
+    Wc[a] = acc;
   }
   for (int i = ilo + lane; i < ihi; i += 32) {
     cplx x = col[i];
 #pragma unroll
-    for (int a = 0; a < BQR_W; ++a)
-      if (a < w) x = cfms(Vs[i * w + a], W[a], x);
+    for (int a = 0; a < W; ++a)
+      if (a < w) x = cfms(Vs[i * w + a], Wc[a], x);
     col[i] = x;
   }
 }

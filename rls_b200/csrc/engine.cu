@@ -192,8 +192,12 @@ struct rls_ctx {
     bool on = false;
     int64_t l = 0, u = 0, kd = 0, ldab = 0;
     cplx* AB = nullptr;          // n × ldab band work array
-    cplx* Vp = nullptr;          // BQR_MAXROWS × BQR_W reflectors of one panel
-    cplx* Tm = nullptr;          // BQR_W × BQR_W block-reflector factor of one panel
+    int w = 8;                   // panel width (8 or 16)
+    cplx* Vp = nullptr;          // BQR_MAXROWS × BQR_WMAX reflectors of one panel
+    cplx* Tm = nullptr;          // w × w block-reflector factor of one panel
+    cplx* zdev = nullptr;        // the shift the captured factorisation reads
+    cudaGraphExec_t graph = nullptr;   // the factorisation's launch sequence, captured once
+    int64_t graph_launches = 0;
     cplx* tmp = nullptr;         // n_pad: (B − zI)v for the refine-point gradient
   } band;
   int scratch_cols = 0;            // minimum column count the shared scratch serves (setup_space)
@@ -1373,8 +1377,10 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_trtri, optin));
   RET(allow_big_smem(ctx, k_blockrot_apply_g, optin));
   RET(allow_big_smem(ctx, k_blockrot_left_g, optin));
-  RET(allow_big_smem(ctx, k_bqr_update, optin));
-  RET(allow_big_smem(ctx, k_bqr_panel, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<8>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<16>, optin));
+  RET(allow_big_smem(ctx, k_bqr_panel<8>, optin));
+  RET(allow_big_smem(ctx, k_bqr_panel<16>, optin));
   return RLS_OK;
 }
 

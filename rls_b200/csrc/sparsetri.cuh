@@ -21,38 +21,74 @@ namespace {
 
 void band_release(rls_ctx* ctx) {
   auto& B = ctx->band;
-  for (void* q : {(void*)B.AB, (void*)B.Vp, (void*)B.Tm, (void*)B.tmp}) dfree(ctx, q);
+  if (B.graph) cudaGraphExecDestroy(B.graph);   // before the arrays its nodes address
+  for (void* q : {(void*)B.AB, (void*)B.Vp, (void*)B.Tm, (void*)B.tmp, (void*)B.zdev}) dfree(ctx, q);
   B = rls_ctx::Band{};
 }
 
-// R(z) of B − zI into the band tiles T (kernels in bandqr.cuh).
-int band_factor(rls_ctx* ctx, cplx z) {
+// The factorisation's launches (captured once per operator, then replayed): B − zI into the
+// band array (z from B.zdev), the panels and their trailing updates, R into band tiles.
+template <int W>
+int band_factor_launches(rls_ctx* ctx, int64_t* count) {
   auto& B = ctx->band;
   const int64_t n = ctx->n;
-  cudaEvent_t e0 = nullptr;
-  prof_begin(ctx, KP_BANDQR, &e0);
   CK(cudaMemsetAsync(B.AB, 0, sizeof(cplx) * (size_t)n * (size_t)B.ldab, ctx->stream));
   const unsigned gr = (unsigned)((n + 255) / 256);
   k_band_scatter<<<gr, 256, 0, ctx->stream>>>(n, B.kd, B.ldab, ctx->sp[0], B.AB);
-  k_band_shift<<<gr, 256, 0, ctx->stream>>>(n, B.kd, B.ldab, z, B.AB);
+  k_band_shift<<<gr, 256, 0, ctx->stream>>>(n, B.kd, B.ldab, B.zdev, B.AB);
   RET(check_launch(ctx, "k_band_scatter"));
-  for (int64_t c0 = 0; c0 < n; c0 += BQR_W) {
-    const int w = (int)std::min<int64_t>(BQR_W, n - c0);
+  int64_t k = 2;
+  for (int64_t c0 = 0; c0 < n; c0 += W) {
+    const int w = (int)std::min<int64_t>(W, n - c0);
     const int mp = (int)std::min<int64_t>(n - c0, w + B.l);
-    k_bqr_panel<<<1, 32 * BQR_W, bqr_panel_smem(w, mp), ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, B.Vp,
-                                                                        B.Tm, ctx->derr);
+    k_bqr_panel<W><<<1, 32 * W, bqr_panel_smem(w, mp), ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, B.Vp,
+                                                                      B.Tm, ctx->derr);
+    ++k;
     const int64_t je = std::min<int64_t>(n, c0 + mp + B.u);
     const int64_t ncw = je - (c0 + w);
-    if (ncw > 0)
-      k_bqr_update<<<(unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS), 32 * BQR_UCOLS, bqr_update_smem(w, mp),
-                     ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm);
+    if (ncw > 0) {
+      k_bqr_update<W><<<(unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS), 32 * BQR_UCOLS, bqr_update_smem(w, mp),
+                        ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm);
+      ++k;
+    }
   }
   RET(check_launch(ctx, "k_bqr_panel/k_bqr_update"));
-  // algorithmic flops: per column, a reflector of l + 1 rows onto l + u columns (dot + update)
-  prof_end(ctx, KP_BANDQR, e0, 16.0 * (double)(B.l + 1) * (double)(B.l + B.u) * (double)n);
   k_band_tiles<<<(unsigned)tile_slots(ctx->nb, ctx->tile_bw), 256, 0, ctx->stream>>>(ctx->nb, ctx->tile_bw, n, B.kd,
                                                                                      B.ldab, B.AB, ctx->T);
+  *count = k + 1;
   return check_launch(ctx, "k_band_tiles");
+}
+
+// R(z) of B − zI into the band tiles T (kernels in bandqr.cuh): the shift goes to device
+// memory, then one graph launch replays the captured sequence.
+int band_factor(rls_ctx* ctx, cplx z) {
+  auto& B = ctx->band;
+  CK(cudaMemcpyAsync(B.zdev, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
+  if (!B.graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int64_t cnt = 0;
+    const int st = (B.w == 16) ? band_factor_launches<16>(ctx, &cnt) : band_factor_launches<8>(ctx, &cnt);
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    if (st != RLS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    CK(ce);
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    B.graph = ex;
+    B.graph_launches = cnt;
+  }
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, KP_BANDQR, &e0);
+  CK(cudaGraphLaunch(B.graph, ctx->stream));
+  ctx->launches += B.graph_launches;
+  // algorithmic flops: per column, a reflector of l + 1 rows onto l + u columns (dot + update)
+  prof_end(ctx, KP_BANDQR, e0, 16.0 * (double)(B.l + 1) * (double)(B.l + B.u) * (double)ctx->n);
+  return RLS_OK;
 }
 
 // Reverse Cuthill–McKee order (new → old) of the pattern of |C| + |Cᵀ|, each component from a
@@ -334,8 +370,11 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   RET(dalloc_t(ctx, &ctx->ticket, 1));
   RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
   RET(dalloc_t(ctx, &B.AB, (size_t)n * (size_t)B.ldab));
-  RET(dalloc_t(ctx, &B.Vp, (size_t)BQR_MAXROWS * BQR_W));
-  RET(dalloc_t(ctx, &B.Tm, (size_t)BQR_W * BQR_W));
+  // 16-column panels where the panel (and the update's copy of V) fit in 200 KB of shared memory
+  B.w = (bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && 16 + l <= BQR_MAXROWS) ? 16 : 8;
+  RET(dalloc_t(ctx, &B.Vp, (size_t)BQR_MAXROWS * BQR_WMAX));
+  RET(dalloc_t(ctx, &B.Tm, (size_t)BQR_WMAX * BQR_WMAX));
+  RET(dalloc_t(ctx, &B.zdev, 1));
   RET(dalloc_t(ctx, &B.tmp, (size_t)ctx->n_pad));
   B.on = true;
   ctx->op_sparse = true;

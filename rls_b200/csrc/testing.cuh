@@ -359,3 +359,15 @@ extern "C" int rls_test_band_r(rls_ctx* ctx, rls_c64 z, rls_c64* R, int64_t ldr,
   if (u) *u = ctx->band.u;
   return RLS_OK;
 }
+
+extern "C" int rls_test_band_factor(rls_ctx* ctx, rls_c64 z) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->band.on) {
+    set_err(ctx, "rls_test_band_factor: no sparse operator (call rls_set_sparse_tri first)");
+    return RLS_ERR_STATE;
+  }
+  CK(cudaSetDevice(ctx->device));
+  ctx->z_dinv = cmk(NAN, NAN);
+  RET(ensure_dinv(ctx, cmk(z.re, z.im)));
+  return sync_and_check(ctx);
+}

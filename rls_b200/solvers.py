@@ -252,6 +252,11 @@ class Engine:
         check(lib().rls_test_band_r(self._h, c64(z.real, z.imag), ptr(R), n, C.byref(l), C.byref(u)), self._h)
         return R, int(l.value), int(u.value)
 
+    def band_factor(self, z: complex):
+        """One device factorisation R(z) of B − zI (test hook rls_test_band_factor), synchronised."""
+        z = complex(z)
+        check(lib().rls_test_band_factor(self._h, c64(z.real, z.imag)), self._h)
+
     def set_log(self, fn, verbose=1):
         if fn is None:
             self._log_cb = None

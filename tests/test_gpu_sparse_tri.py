@@ -19,11 +19,16 @@ pytestmark = pytest.mark.gpu
 
 
 def _banded(n, l, u, seed):
+    """Random complex band matrix made well conditioned by its diagonal (a random band with
+    l ≫ u is numerically singular, and R's trailing phases are then noise)."""
     rng = np.random.default_rng(seed)
     diags, offs = [], []
     for d in range(-l, u + 1):
         m = n - abs(d)
-        diags.append(rng.standard_normal(m) + 1j * rng.standard_normal(m))
+        v = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+        if d == 0:
+            v = v + 4.0 * np.sqrt(l + u + 1)
+        diags.append(v)
         offs.append(d)
     return sp.diags(diags, offs, shape=(n, n), format="csc")
 
@@ -47,10 +52,11 @@ def test_band_qr_matches_lapack_r(cuda_device, name):
         B = sp.csc_matrix(C)[S.perm][:, S.perm].toarray()
         n = B.shape[0]
         scale = np.linalg.norm(B, 2) + 1.0
-        for z in (0.3 - 0.2j, -1.5 + 2.0j, complex(B[0, 0])):
+        for z in (0.3 - 0.2j, -1.5 + 2.0j, 0.5 * complex(B[0, 0]) + 0.1j):
             Rg, l, u = eng.band_r(z)
             A = B - z * np.eye(n)
             Rl = np.linalg.qr(A, mode="r")
+            assert np.min(np.abs(np.diag(Rl))) > 1e-6 * scale     # well conditioned: phases determined
             d = np.diag(Rl) / np.diag(Rg)
             assert np.allclose(np.abs(d), 1.0, atol=1e-9)
             err = np.max(np.abs(d[:, None] * Rg - Rl))
