@@ -158,7 +158,8 @@ inline size_t bqr_panel_smem(int w, int mp) { return (size_t)w * mp * sizeof(cpl
 
 // C ← C − V·Tᴴ·(VᴴC) on the trailing columns jb .. je−1 (jb = c0 + w), rows c0 .. c0+mp−1.
 // Grid: ⌈(je − jb)/8⌉ CTAs of 8 warps, warp c on column jb + 8·blockIdx.x + c.
-// Dynamic shared memory: mp·w cplx of V (row i at Vs + i·w).
+// Dynamic shared memory: mp·(W+1) cplx of V (row i at Vs + i·(W+1): the odd row stride keeps a
+// warp's lanes, which read one column at consecutive rows, on distinct banks).
 template <int W>
 __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_t kd, int64_t ldab,
                                                                cplx* __restrict__ AB, int64_t c0, int w, int mp,
@@ -166,9 +167,9 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
                                                                const cplx* __restrict__ Tm) {
   extern __shared__ cplx Vs[];
   __shared__ cplx Ts[W * W];
-  for (int e = threadIdx.x; e < mp * w; e += blockDim.x) {
-    const int i = e / w, a = e % w;
-    Vs[e] = Vp[(int64_t)a * BQR_MAXROWS + i];
+  for (int e = threadIdx.x; e < mp * W; e += blockDim.x) {   // coalesced along the rows of V
+    const int a = e / mp, i = e % mp;
+    Vs[i * (W + 1) + a] = (a < w) ? Vp[(int64_t)a * BQR_MAXROWS + i] : czero();
   }
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) Ts[e] = Tm[e];
   __syncthreads();
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
   for (int i = ilo + lane; i < ihi; i += 32) {
     const cplx x = col[i];
 #pragma unroll
-    for (int a = 0; a < W; ++a) d[a] = cfma(cconj(Vs[i * w + min(a, w - 1)]), x, d[a]);
+    for (int a = 0; a < W; ++a) d[a] = cfma(cconj(Vs[i * (W + 1) + a]), x, d[a]);
   }
 #pragma unroll
   for (int a = 0; a < W; ++a) {
@@ -208,12 +209,12 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
     cplx x = col[i];
 #pragma unroll
     for (int a = 0; a < W; ++a)
-      if (a < w) x = cfms(Vs[i * w + a], Wc[a], x);
+      if (a < w) x = cfms(Vs[i * (W + 1) + a], Wc[a], x);
     col[i] = x;
   }
 }
 
-inline size_t bqr_update_smem(int w, int mp) { return (size_t)mp * w * sizeof(cplx); }
+inline size_t bqr_update_smem(int W, int mp) { return (size_t)mp * (W + 1) * sizeof(cplx); }
 
 // Band tiles of R for the dataflow solve: tile (I, J), J − I ≤ bw, at slot tile_index_bw.
 // Grid: tile_slots(nb, bw) CTAs (unused slots return), 256 threads.

@@ -47,7 +47,7 @@ int band_factor_launches(rls_ctx* ctx, int64_t* count) {
     const int64_t je = std::min<int64_t>(n, c0 + mp + B.u);
     const int64_t ncw = je - (c0 + w);
     if (ncw > 0) {
-      k_bqr_update<W><<<(unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS), 32 * BQR_UCOLS, bqr_update_smem(w, mp),
+      k_bqr_update<W><<<(unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS), 32 * BQR_UCOLS, bqr_update_smem(W, mp),
                         ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm);
       ++k;
     }
@@ -371,7 +371,8 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
   RET(dalloc_t(ctx, &B.AB, (size_t)n * (size_t)B.ldab));
   // 16-column panels where the panel (and the update's copy of V) fit in 200 KB of shared memory
-  B.w = (bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && 16 + l <= BQR_MAXROWS) ? 16 : 8;
+  B.w = (bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && bqr_update_smem(16, (int)(16 + l)) <= 200 * 1024 &&
+         16 + l <= BQR_MAXROWS) ? 16 : 8;
   RET(dalloc_t(ctx, &B.Vp, (size_t)BQR_MAXROWS * BQR_WMAX));
   RET(dalloc_t(ctx, &B.Tm, (size_t)BQR_WMAX * BQR_WMAX));
   RET(dalloc_t(ctx, &B.zdev, 1));
