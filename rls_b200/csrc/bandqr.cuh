@@ -56,79 +56,118 @@ __global__ void k_band_shift(int64_t n, int64_t kd, int64_t ldab, const cplx* __
   if (j < n) AB[j * ldab + kd] = csub(AB[j * ldab + kd], z);
 }
 
+// Σ over the lane's rows of a·b (two accumulators, then the warp sum), rows lo + lane, step 32.
+template <bool CONJ_A>
+__device__ __forceinline__ cplx warp_dot(const cplx* __restrict__ a, const cplx* __restrict__ b, int lo, int hi,
+                                         int lane) {
+  cplx s0 = czero(), s1 = czero();
+  int i = lo + lane;
+  for (; i + 32 < hi; i += 64) {
+    s0 = cfma(CONJ_A ? cconj(a[i]) : a[i], b[i], s0);
+    s1 = cfma(CONJ_A ? cconj(a[i + 32]) : a[i + 32], b[i + 32], s1);
+  }
+  if (i < hi) s0 = cfma(CONJ_A ? cconj(a[i]) : a[i], b[i], s0);
+  cplx d = cadd(s0, s1);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d.x += __shfl_xor_sync(0xffffffffu, d.x, o);
+    d.y += __shfl_xor_sync(0xffffffffu, d.y, o);
+  }
+  return d;
+}
+
 // Dynamic shared memory: w·mp cplx (column q at P + q·mp).  Tm: W × W, column-major, ld W.
+// The reflector tails stay unscaled in P during the panel (v_s = (1, scl_s·x_s)); they are
+// scaled on the way out, which keeps the scaling off the per-reflector critical path.  The
+// next column's owner accumulates its tail norm while it applies the current reflector.
 template <int W>
 __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int64_t ldab, cplx* __restrict__ AB,
                                                       int64_t c0, int w, int mp, cplx* __restrict__ Vp,
                                                       cplx* __restrict__ Tm, int* err) {
   extern __shared__ cplx P[];
-  __shared__ cplx taus[W];
+  __shared__ cplx taus[W], scl[W];
   __shared__ cplx Y[W][W + 1];   // Y[q][s] = v_qᴴ v_s (q < s)
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
   auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
+  auto iend_of = [&](int s) { return (int)min((int64_t)mp, (int64_t)s + l + 1); };   // reflector s: rows s..iend−1
   for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
     const int qq = e / mp, i = e % mp;
     P[e] = valid(i, qq) ? AB[(c0 + qq) * ldab + (i - qq + kd)] : czero();
   }
   __syncthreads();
   cplx* Pq = P + (size_t)q * mp;
-  for (int s = 0; s < w; ++s) {
-    cplx* Ps = P + (size_t)s * mp;
-    const int iend = (int)min((int64_t)mp, (int64_t)s + l + 1);   // reflector s covers rows s..iend−1
-    if (q == s) {
-      const cplx alpha = Pq[s];   // read by every lane before the shuffles below (lane 0 rewrites it)
-      double xn2 = 0.0;
-      for (int i = s + 1 + lane; i < iend; i += 32) xn2 += cabs2(Pq[i]);
+  double xn2 = 0.0;   // owner of the next step: ‖tail‖² of its column
+  if (q == 0) {
+    const int e0 = iend_of(0);
+    double t0 = 0.0, t1 = 0.0;
+    int i = 1 + lane;
+    for (; i + 32 < e0; i += 64) { t0 += cabs2(Pq[i]); t1 += cabs2(Pq[i + 32]); }
+    if (i < e0) t0 += cabs2(Pq[i]);
+    xn2 = t0 + t1;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
-      cplx tau = czero(), scale = czero();
+    for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
+  }
+  for (int s = 0; s < w; ++s) {
+    const cplx* Ps = P + (size_t)s * mp;
+    const int iend = iend_of(s);
+    if (q == s) {   // zlarfg: β = −sign(Re α)·‖(α, x)‖, τ = (β − α)/β, tail scale 1/(α − β)
+      const cplx alpha = Pq[s];
+      cplx tau = czero(), sc = czero();
       double beta = alpha.x;
       if (xn2 > 0.0 || alpha.y != 0.0) {
         const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
         beta = (alpha.x >= 0.0) ? -nrm : nrm;
         tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-        scale = cinv(csub(alpha, cmk(beta, 0.0)));
+        sc = cinv(csub(alpha, cmk(beta, 0.0)));
       }
-      for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cmul(Pq[i], scale);
+      __syncwarp();   // every lane has read α
       if (lane == 0) {
         Pq[s] = cmk(beta, 0.0);
         taus[s] = tau;
+        scl[s] = sc;
         if (!isfinite(beta)) atomicOr(err, DEVERR_NONFINITE);
       }
     }
     __syncthreads();
     if (q < w && q > s) {
-      // H_sᴴ on column q: a ← a − conj(τ)·v·(vᴴa), v = (1, Ps[s+1..iend−1])
-      cplx d = czero();
-      for (int i = s + 1 + lane; i < iend; i += 32) d = cfma(cconj(Ps[i]), Pq[i], d);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        d.x += __shfl_xor_sync(0xffffffffu, d.x, o);
-        d.y += __shfl_xor_sync(0xffffffffu, d.y, o);
-      }
-      d = cadd(d, Pq[s]);
+      // H_sᴴ on column q: a ← a − conj(τ)·v·(vᴴa), v = (1, sc·x)
+      const cplx sc = scl[s];
+      const cplx d = cadd(Pq[s], cmul(cconj(sc), warp_dot<true>(Ps, Pq, s + 1, iend, lane)));
       const cplx f = cmul(cconj(taus[s]), d);
-      __syncwarp();
-      for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cfms(Ps[i], f, Pq[i]);
-      if (lane == 0) Pq[s] = csub(Pq[s], f);
-    } else if (q < s) {
-      // v_qᴴ v_s over rows ≥ s (> q), where column q holds v_q
-      cplx y = czero();
-      for (int i = s + 1 + lane; i < iend; i += 32) y = cfma(cconj(Pq[i]), Ps[i], y);
+      const cplx g = cmul(sc, f);
+      __syncwarp();   // every lane has read a_s
+      if (q == s + 1) {   // the next owner: update rows s+1.. and sum the new tail (rows > s+1)
+        const int e1 = iend_of(s + 1);
+        double t = 0.0;
+        for (int i = s + 1 + lane; i < e1; i += 32) {
+          cplx v = Pq[i];
+          if (i < iend) {
+            v = cfms(Ps[i], g, v);
+            Pq[i] = v;
+          }
+          if (i > s + 1) t += cabs2(v);
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        y.x += __shfl_xor_sync(0xffffffffu, y.x, o);
-        y.y += __shfl_xor_sync(0xffffffffu, y.y, o);
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        xn2 = t;
+      } else {
+        for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cfms(Ps[i], g, Pq[i]);
       }
-      if (lane == 0) Y[q][s] = cadd(y, cconj(Pq[s]));
+      if (lane == 0) Pq[s] = csub(Pq[s], f);
+      __syncwarp();   // the next owner's lanes see row s+1 (its α) as updated
+    } else if (q < s) {
+      // v_qᴴ v_s = conj(scl_q)·(conj(x_q,s) + scl_s·Σ_{i>s} conj(x_q,i)·x_s,i)
+      const cplx y = warp_dot<true>(Pq, Ps, s + 1, iend, lane);
+      if (lane == 0) Y[q][s] = cmul(cconj(scl[q]), cadd(cconj(Pq[s]), cmul(scl[s], y)));
     }
   }
   __syncthreads();
-  // write back: R rows ≤ q and reflector tails in place; V (unit diagonal, zero above) for
-  // the trailing update
+  // write back: R rows ≤ q and the scaled reflector tails in place; V (unit diagonal, zero
+  // above) for the trailing update
   for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
     const int qq = e / mp, i = e % mp;
-    const cplx v = P[e];
+    cplx v = P[e];
+    if (i > qq) v = cmul(v, scl[qq]);
     if (valid(i, qq)) AB[(c0 + qq) * ldab + (i - qq + kd)] = v;
     Vp[(int64_t)qq * BQR_MAXROWS + i] = (i < qq) ? czero() : (i == qq ? cmk(1.0, 0.0) : v);
   }
@@ -157,10 +196,11 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
 inline size_t bqr_panel_smem(int w, int mp) { return (size_t)w * mp * sizeof(cplx); }
 
 // C ← C − V·Tᴴ·(VᴴC) on the trailing columns jb .. je−1 (jb = c0 + w), rows c0 .. c0+mp−1.
-// Grid: ⌈(je − jb)/8⌉ CTAs of 8 warps, warp c on column jb + 8·blockIdx.x + c.
+// Grid: ⌈(je − jb)/8⌉ CTAs of 8 warps, warp c on column jb + 8·blockIdx.x + c; the column's rows
+// (at most 32·RPL) are loaded into registers at once, used for VᴴC and updated in place.
 // Dynamic shared memory: mp·(W+1) cplx of V (row i at Vs + i·(W+1): the odd row stride keeps a
 // warp's lanes, which read one column at consecutive rows, on distinct banks).
-template <int W>
+template <int W, int RPL>
 __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_t kd, int64_t ldab,
                                                                cplx* __restrict__ AB, int64_t c0, int w, int mp,
                                                                int64_t je, const cplx* __restrict__ Vp,
@@ -172,20 +212,30 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
     Vs[i * (W + 1) + a] = (a < w) ? Vp[(int64_t)a * BQR_MAXROWS + i] : czero();
   }
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) Ts[e] = Tm[e];
-  __syncthreads();
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   const int64_t jj = c0 + w + (int64_t)blockIdx.x * BQR_UCOLS + c;
-  if (jj >= je) return;
   // rows of column jj inside its band: c0 + i ∈ [jj − kd, jj + l]
-  const int ilo = (int)max((int64_t)0, jj - kd - c0), ihi = (int)min((int64_t)mp, jj + l + 1 - c0);
+  const int ilo = (jj < je) ? (int)max((int64_t)0, jj - kd - c0) : 0;
+  const int ihi = (jj < je) ? (int)min((int64_t)mp, jj + l + 1 - c0) : 0;
   cplx* col = AB + jj * ldab + (c0 - jj + kd);   // col[i] = A[c0 + i][jj]
+  cplx x[RPL];
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int i = ilo + lane + 32 * t;
+    x[t] = (i < ihi) ? col[i] : czero();
+  }
+  __syncthreads();
+  if (jj >= je) return;
   cplx d[W];
 #pragma unroll
   for (int a = 0; a < W; ++a) d[a] = czero();
-  for (int i = ilo + lane; i < ihi; i += 32) {
-    const cplx x = col[i];
 #pragma unroll
-    for (int a = 0; a < W; ++a) d[a] = cfma(cconj(Vs[i * (W + 1) + a]), x, d[a]);
+  for (int t = 0; t < RPL; ++t) {
+    const int i = ilo + lane + 32 * t;
+    if (i < ihi) {
+#pragma unroll
+      for (int a = 0; a < W; ++a) d[a] = cfma(cconj(Vs[i * (W + 1) + a]), x[t], d[a]);
+    }
   }
 #pragma unroll
   for (int a = 0; a < W; ++a) {
@@ -201,16 +251,18 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
   for (int a = 0; a < W; ++a) {
     cplx acc = czero();
 #pragma unroll
-    for (int k = 0; k <= a; ++k)
-      if (a < w) acc = cfma(cconj(Ts[a * W + k]), d[k], acc);
+    for (int k = 0; k <= a; ++k) acc = cfma(cconj(Ts[a * W + k]), d[k], acc);
     Wc[a] = acc;
   }
-  for (int i = ilo + lane; i < ihi; i += 32) {
-    cplx x = col[i];
 #pragma unroll
-    for (int a = 0; a < W; ++a)
-      if (a < w) x = cfms(Vs[i * (W + 1) + a], Wc[a], x);
-    col[i] = x;
+  for (int t = 0; t < RPL; ++t) {
+    const int i = ilo + lane + 32 * t;
+    if (i < ihi) {
+      cplx v = x[t];
+#pragma unroll
+      for (int a = 0; a < W; ++a) v = cfms(Vs[i * (W + 1) + a], Wc[a], v);
+      col[i] = v;
+    }
   }
 }
 

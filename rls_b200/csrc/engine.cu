@@ -193,6 +193,7 @@ struct rls_ctx {
     int64_t l = 0, u = 0, kd = 0, ldab = 0;
     cplx* AB = nullptr;          // n × ldab band work array
     int w = 8;                   // panel width (8 or 16)
+    int rpl = 8;                 // rows per lane of the trailing update (8, 16, 24 or 32)
     cplx* Vp = nullptr;          // BQR_MAXROWS × BQR_WMAX reflectors of one panel
     cplx* Tm = nullptr;          // w × w block-reflector factor of one panel
     cplx* zdev = nullptr;        // the shift the captured factorisation reads
@@ -1377,8 +1378,14 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_trtri, optin));
   RET(allow_big_smem(ctx, k_blockrot_apply_g, optin));
   RET(allow_big_smem(ctx, k_blockrot_left_g, optin));
-  RET(allow_big_smem(ctx, k_bqr_update<8>, optin));
-  RET(allow_big_smem(ctx, k_bqr_update<16>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<8, 8>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<8, 16>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<8, 24>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<8, 32>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<16, 8>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<16, 16>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<16, 24>, optin));
+  RET(allow_big_smem(ctx, k_bqr_update<16, 32>, optin));
   RET(allow_big_smem(ctx, k_bqr_panel<8>, optin));
   RET(allow_big_smem(ctx, k_bqr_panel<16>, optin));
   return RLS_OK;

@@ -47,8 +47,15 @@ int band_factor_launches(rls_ctx* ctx, int64_t* count) {
     const int64_t je = std::min<int64_t>(n, c0 + mp + B.u);
     const int64_t ncw = je - (c0 + w);
     if (ncw > 0) {
-      k_bqr_update<W><<<(unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS), 32 * BQR_UCOLS, bqr_update_smem(W, mp),
-                        ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm);
+      const unsigned g = (unsigned)((ncw + BQR_UCOLS - 1) / BQR_UCOLS);
+      const size_t sm = bqr_update_smem(W, mp);
+#define RLS_BQRU(R) \
+  case R: k_bqr_update<W, R><<<g, 32 * BQR_UCOLS, sm, ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm); break;
+      switch (B.rpl) {
+        RLS_BQRU(8) RLS_BQRU(16) RLS_BQRU(24) RLS_BQRU(32)
+        default: set_err(ctx, "band QR update: %d rows per lane", B.rpl); return RLS_ERR_STATE;
+      }
+#undef RLS_BQRU
       ++k;
     }
   }
@@ -373,6 +380,8 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   // 16-column panels where the panel (and the update's copy of V) fit in 200 KB of shared memory
   B.w = (bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && bqr_update_smem(16, (int)(16 + l)) <= 200 * 1024 &&
          16 + l <= BQR_MAXROWS) ? 16 : 8;
+  B.rpl = 8;   // the update's rows per lane: the panel's rows w + l over 32 lanes, in steps of 8
+  while (32 * B.rpl < B.w + l) B.rpl += 8;
   RET(dalloc_t(ctx, &B.Vp, (size_t)BQR_MAXROWS * BQR_WMAX));
   RET(dalloc_t(ctx, &B.Tm, (size_t)BQR_WMAX * BQR_WMAX));
   RET(dalloc_t(ctx, &B.zdev, 1));
