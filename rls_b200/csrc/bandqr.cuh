@@ -90,10 +90,12 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
   auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
   auto iend_of = [&](int s) { return (int)min((int64_t)mp, (int64_t)s + l + 1); };   // reflector s: rows s..iend−1
-  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
+  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {   // all copies in flight at once
     const int qq = e / mp, i = e % mp;
-    P[e] = valid(i, qq) ? AB[(c0 + qq) * ldab + (i - qq + kd)] : czero();
+    if (valid(i, qq)) cp_async16(&P[e], &AB[(c0 + qq) * ldab + (i - qq + kd)]);
+    else P[e] = czero();
   }
+  cp_async_wait_all();
   __syncthreads();
   cplx* Pq = P + (size_t)q * mp;
   double xn2 = 0.0;   // owner of the next step: ‖tail‖² of its column
@@ -207,11 +209,12 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
                                                                const cplx* __restrict__ Tm) {
   extern __shared__ cplx Vs[];
   __shared__ cplx Ts[W * W];
-  for (int e = threadIdx.x; e < mp * W; e += blockDim.x) {   // coalesced along the rows of V
+  for (int e = threadIdx.x; e < mp * W; e += blockDim.x) {   // coalesced along the rows of V, all in flight
     const int a = e / mp, i = e % mp;
-    Vs[i * (W + 1) + a] = (a < w) ? Vp[(int64_t)a * BQR_MAXROWS + i] : czero();
+    if (a < w) cp_async16(&Vs[i * (W + 1) + a], &Vp[(int64_t)a * BQR_MAXROWS + i]);
+    else Vs[i * (W + 1) + a] = czero();
   }
-  for (int e = threadIdx.x; e < W * W; e += blockDim.x) Ts[e] = Tm[e];
+  for (int e = threadIdx.x; e < W * W; e += blockDim.x) cp_async16(&Ts[e], &Tm[e]);
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
   const int64_t jj = c0 + w + (int64_t)blockIdx.x * BQR_UCOLS + c;
   // rows of column jj inside its band: c0 + i ∈ [jj − kd, jj + l]
@@ -224,6 +227,7 @@ __global__ void __launch_bounds__(32 * BQR_UCOLS) k_bqr_update(int64_t l, int64_
     const int i = ilo + lane + 32 * t;
     x[t] = (i < ihi) ? col[i] : czero();
   }
+  cp_async_wait_all();
   __syncthreads();
   if (jj >= je) return;
   cplx d[W];
