@@ -78,8 +78,12 @@ __device__ __forceinline__ cplx warp_dot(const cplx* __restrict__ a, const cplx*
 
 // Dynamic shared memory: w·mp cplx (column q at P + q·mp).  Tm: W × W, column-major, ld W.
 // The reflector tails stay unscaled in P during the panel (v_s = (1, scl_s·x_s)); they are
-// scaled on the way out, which keeps the scaling off the per-reflector critical path.  The
-// next column's owner accumulates its tail norm while it applies the current reflector.
+// scaled on the way out.  No block-wide barrier per reflector: warp q applies reflectors
+// 0..q−1 to its column as each is published (a flag in shared memory, set after a block fence),
+// accumulating its tail norm while it applies the last one, then forms and publishes its own
+// reflector.  The chain of owners is the critical path; the other warps catch up beside it.
+// Every wait is bounded (RLS_SPIN_LIMIT, then DEVERR_SPIN_TIMEOUT); a warp only waits on
+// reflectors of lower-numbered warps of the same block, which never wait on it.
 template <int W>
 __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int64_t ldab, cplx* __restrict__ AB,
                                                       int64_t c0, int w, int mp, cplx* __restrict__ Vp,
@@ -87,9 +91,11 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
   extern __shared__ cplx P[];
   __shared__ cplx taus[W], scl[W];
   __shared__ cplx Y[W][W + 1];   // Y[q][s] = v_qᴴ v_s (q < s)
+  __shared__ int ready[W];
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
   auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
   auto iend_of = [&](int s) { return (int)min((int64_t)mp, (int64_t)s + l + 1); };   // reflector s: rows s..iend−1
+  if (threadIdx.x < W) ready[threadIdx.x] = 0;
   for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {   // all copies in flight at once
     const int qq = e / mp, i = e % mp;
     if (valid(i, qq)) cp_async16(&P[e], &AB[(c0 + qq) * ldab + (i - qq + kd)]);
@@ -97,49 +103,39 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
   }
   cp_async_wait_all();
   __syncthreads();
-  cplx* Pq = P + (size_t)q * mp;
-  double xn2 = 0.0;   // owner of the next step: ‖tail‖² of its column
-  if (q == 0) {
-    const int e0 = iend_of(0);
-    double t0 = 0.0, t1 = 0.0;
-    int i = 1 + lane;
-    for (; i + 32 < e0; i += 64) { t0 += cabs2(Pq[i]); t1 += cabs2(Pq[i + 32]); }
-    if (i < e0) t0 += cabs2(Pq[i]);
-    xn2 = t0 + t1;
+  if (q < w) {
+    cplx* Pq = P + (size_t)q * mp;
+    double xn2 = 0.0;   // ‖tail‖² of this column when it is this warp's turn
+    if (q == 0) {
+      const int e0 = iend_of(0);
+      double t0 = 0.0, t1 = 0.0;
+      int i = 1 + lane;
+      for (; i + 32 < e0; i += 64) { t0 += cabs2(Pq[i]); t1 += cabs2(Pq[i + 32]); }
+      if (i < e0) t0 += cabs2(Pq[i]);
+      xn2 = t0 + t1;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
-  }
-  for (int s = 0; s < w; ++s) {
-    const cplx* Ps = P + (size_t)s * mp;
-    const int iend = iend_of(s);
-    if (q == s) {   // zlarfg: β = −sign(Re α)·‖(α, x)‖, τ = (β − α)/β, tail scale 1/(α − β)
-      const cplx alpha = Pq[s];
-      cplx tau = czero(), sc = czero();
-      double beta = alpha.x;
-      if (xn2 > 0.0 || alpha.y != 0.0) {
-        const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
-        beta = (alpha.x >= 0.0) ? -nrm : nrm;
-        tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-        sc = cinv(csub(alpha, cmk(beta, 0.0)));
-      }
-      __syncwarp();   // every lane has read α
-      if (lane == 0) {
-        Pq[s] = cmk(beta, 0.0);
-        taus[s] = tau;
-        scl[s] = sc;
-        if (!isfinite(beta)) atomicOr(err, DEVERR_NONFINITE);
-      }
+      for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
     }
-    __syncthreads();
-    if (q < w && q > s) {
+    for (int s = 0; s < q; ++s) {
+      // wait for reflector s (every lane observes the flag itself, then a block fence)
+      int spins = 0;
+      while (*(volatile int*)&ready[s] == 0) {
+        if (++spins > RLS_SPIN_LIMIT) {
+          if (lane == 0) atomicOr(err, DEVERR_SPIN_TIMEOUT);
+          break;
+        }
+      }
+      __threadfence_block();
+      const cplx* Ps = P + (size_t)s * mp;
+      const int iend = iend_of(s);
       // H_sᴴ on column q: a ← a − conj(τ)·v·(vᴴa), v = (1, sc·x)
       const cplx sc = scl[s];
       const cplx d = cadd(Pq[s], cmul(cconj(sc), warp_dot<true>(Ps, Pq, s + 1, iend, lane)));
       const cplx f = cmul(cconj(taus[s]), d);
       const cplx g = cmul(sc, f);
       __syncwarp();   // every lane has read a_s
-      if (q == s + 1) {   // the next owner: update rows s+1.. and sum the new tail (rows > s+1)
-        const int e1 = iend_of(s + 1);
+      if (s == q - 1) {   // the last one before this warp's turn: update and sum the new tail
+        const int e1 = iend_of(q);
         double t = 0.0;
         for (int i = s + 1 + lane; i < e1; i += 32) {
           cplx v = Pq[i];
@@ -147,7 +143,7 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
             v = cfms(Ps[i], g, v);
             Pq[i] = v;
           }
-          if (i > s + 1) t += cabs2(v);
+          if (i > q) t += cabs2(v);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
@@ -156,12 +152,39 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
         for (int i = s + 1 + lane; i < iend; i += 32) Pq[i] = cfms(Ps[i], g, Pq[i]);
       }
       if (lane == 0) Pq[s] = csub(Pq[s], f);
-      __syncwarp();   // the next owner's lanes see row s+1 (its α) as updated
-    } else if (q < s) {
-      // v_qᴴ v_s = conj(scl_q)·(conj(x_q,s) + scl_s·Σ_{i>s} conj(x_q,i)·x_s,i)
-      const cplx y = warp_dot<true>(Pq, Ps, s + 1, iend, lane);
-      if (lane == 0) Y[q][s] = cmul(cconj(scl[q]), cadd(cconj(Pq[s]), cmul(scl[s], y)));
+      __syncwarp();
     }
+    // this warp's reflector (zlarfg: β = −sign(Re α)·‖(α, x)‖, τ = (β − α)/β, tail scale 1/(α − β))
+    const cplx alpha = Pq[q];
+    cplx tau = czero(), sc = czero();
+    double beta = alpha.x;
+    if (xn2 > 0.0 || alpha.y != 0.0) {
+      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+      beta = (alpha.x >= 0.0) ? -nrm : nrm;
+      tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+      sc = cinv(csub(alpha, cmk(beta, 0.0)));
+    }
+    __syncwarp();   // every lane has read α
+    if (lane == 0) {
+      Pq[q] = cmk(beta, 0.0);
+      taus[q] = tau;
+      scl[q] = sc;
+      if (!isfinite(beta)) atomicOr(err, DEVERR_NONFINITE);
+      __threadfence_block();   // column q, τ and the scale before the flag
+      *(volatile int*)&ready[q] = 1;
+    }
+  }
+  __syncthreads();
+  // Y[k][s] = v_kᴴ v_s = conj(scl_k)·(conj(x_k,s) + scl_s·Σ_{i>s} conj(x_k,i)·x_s,i), pairs k < s
+  // spread over the warps
+  const int npairs = w * (w - 1) / 2;
+  for (int pidx = q; pidx < npairs; pidx += W) {
+    int s = 1, k = pidx;
+    while (k >= s) { k -= s; ++s; }   // pidx = s(s−1)/2 + k, 0 ≤ k < s
+    const cplx* Pk = P + (size_t)k * mp;
+    const cplx* Ps = P + (size_t)s * mp;
+    const cplx y = warp_dot<true>(Pk, Ps, s + 1, iend_of(s), lane);
+    if (lane == 0) Y[k][s] = cmul(cconj(scl[k]), cadd(cconj(Pk[s]), cmul(scl[s], y)));
   }
   __syncthreads();
   // write back: R rows ≤ q and the scaled reflector tails in place; V (unit diagonal, zero
@@ -173,7 +196,7 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
     if (valid(i, qq)) AB[(c0 + qq) * ldab + (i - qq + kd)] = v;
     Vp[(int64_t)qq * BQR_MAXROWS + i] = (i < qq) ? czero() : (i == qq ? cmk(1.0, 0.0) : v);
   }
-  if (q == 0 && lane < W) {   // lane = row of T (Y is complete after the barrier above)
+  if (q == 0 && lane < W) {   // lane = row of T
     cplx trow[W];
 #pragma unroll
     for (int s = 0; s < W; ++s) {
