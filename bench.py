@@ -533,11 +533,15 @@ def run_ours(args):
         ls2 = R.Lanes(lanes, local, T)
         if lanes > 1:
             ls2.set_trsm_ctas(args.trsm_ctas)
+        t_setup = time.perf_counter() - t0
         sigma2 = np.full(len(sub.Z), np.nan)
         st2 = PsTriRecyStats.alloc(len(sub.Z))
         cst2 = ls2.engines[0].stats_struct(st2)
+        t_steps = []
         for k in range(args.warmup + args.steps):
+            t1 = time.perf_counter()
             ls2.pstrirecy_range(sub, ctl, k * s, (k + 1) * s, sigma2, st2, cst2, X0=X0)
+            t_steps.append(time.perf_counter() - t1)
         el = max_over_ranks(time.perf_counter() - t0, world, "cuda")
         ls2.close()
         nsteps = args.warmup + args.steps
@@ -545,7 +549,8 @@ def run_ours(args):
         e2e = {"value": world * lanes * nsteps * s / el, "unit": "pts/s",
                "h2d_bytes_per_step": int((T_bytes + lanes * nsteps * s * 16) / nsteps),
                "d2h_bytes_per_step": int(lanes * s * 8),
-               "span": f"upload of T (host to lane 0, shared by the other {lanes - 1}) + steps 0..{nsteps - 1}"}
+               "span": f"upload of T (host to lane 0, shared by the other {lanes - 1}) + steps 0..{nsteps - 1}",
+               "setup_s": t_setup, "step_s": [round(t, 4) for t in t_steps]}
         e2e["matches_device_run"] = bool(np.allclose(sigma2[timed], sigma[timed], rtol=0, atol=1e-12))
 
     out = base_line(args, world)
@@ -954,8 +959,10 @@ def run_sparse_tri(args):
             eng.band_factor(rec.Z[i])
             wall.append(time.perf_counter() - t0)
         cnt, ms_, fl = eng.profile(7)
+        _, _, wsel, m8, m16 = eng.band_info()
         eng.close()
-        print(json.dumps({"workload": desc, "band": {"l": S.l, "u": S.u}, "factorisations": cnt,
+        print(json.dumps({"workload": desc, "band": {"l": S.l, "u": S.u},
+                          "panel": {"width": wsel, "timed_ms_w8": m8, "timed_ms_w16": m16}, "factorisations": cnt,
                           "device_ms_each": ms_ / max(cnt, 1), "gflops": fl / (ms_ / 1e3) / 1e9 if ms_ else None,
                           "wall_ms": [w * 1e3 for w in wall]}), flush=True)
         return
@@ -1019,6 +1026,7 @@ def run_sparse_tri(args):
         if profile:
             res["prof"] = {k: ls.profile(k) for k in (0, 1, 2, 5, 7)}
             res["waits"] = ls.profile(4)
+        res["band_info"] = ls.engines[0].band_info()
         ls.close()
         return res
 
@@ -1031,7 +1039,9 @@ def run_sparse_tri(args):
     out.update({"value": value, "ms_per_step": ms / args.steps, "gpu_launches": main_["launches"],
                 "clocks": main_["clk"].summary(), "preprocess_s": pre_s})
     out["config"].update({"points_per_step": lanes * s, "lanes": lanes, "chunk": s,
-                          "band": {"l": S.l, "u": S.u, "order": "reverse Cuthill-McKee of |C|+|Cᵀ| (band_order)"},
+                          "band": {"l": S.l, "u": S.u, "order": "reverse Cuthill-McKee of |C|+|Cᵀ| (band_order)",
+                                   "panel_width": main_["band_info"][2],
+                                   "panel_timed_ms": {"w8": main_["band_info"][3], "w16": main_["band_info"][4]}},
                           "parallelism": f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU",
                           "refine_fraction_timed": float(np.mean(st.refine_it[tim] > 0)),
                           "l2": "the band array (n·(3l+2u+1)·16 B ≈ 0.3 GB) and R's band tiles exceed L2 (126 MB); "

@@ -271,6 +271,17 @@ int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr, const int
 int rls_band_order(int64_t n, const int64_t* colptr, const int64_t* rowval, int base, int64_t* perm,
                    int64_t* l, int64_t* u);
 
+/* The band QR's panel width (no reference counterpart): 8 or 16 columns, or 0 (default) for the
+ * library's choice, made by timing one factorisation with each width (16 only where its panel
+ * fits in shared memory) at the first refine point of an operator shape on the device and kept
+ * for every later context of that shape, so lanes share one choice.  The setting outlives
+ * rls_set_sparse_tri. */
+int rls_band_set_panel(rls_ctx* ctx, int w);
+/* The installed sparse operator's bandwidths l, u, the panel width in use (0 before the first
+ * factorisation) and the two timed factorisations of the choice in ms (0 if not timed).
+ * RLS_ERR_STATE without a sparse operator.  Any output may be NULL. */
+int rls_band_info(const rls_ctx* ctx, int64_t* l, int64_t* u, int* w, double* ms_w8, double* ms_w16);
+
 /* psTriRecy(C::SparseMatrixCSC, rec; control) (psTriRecy.jl:889-913): rls_set_sparse_tri then
  * rls_pstrirecy_schur over the whole traversal.  stats->qr_time_ns gets the factorisation time
  * when control->collect_timing is set (one extra stream synchronisation per refine point). */

@@ -95,6 +95,8 @@ SIGNATURES = {
     "rls_set_schur_copy": (C.c_int, [P, P]),
     "rls_set_sparse_tri": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P]),
     "rls_band_order": (C.c_int, [C.c_int64, P, P, C.c_int, P, P, P]),
+    "rls_band_set_panel": (C.c_int, [P, C.c_int]),
+    "rls_band_info": (C.c_int, [P, P, P, P, P, P]),
     "rls_pstrirecy_sparse": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P, P, C.c_int64, C.POINTER(rls_grid),
                                        C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),
     "rls_set_trsm_ctas": (C.c_int, [P, C.c_int]),

@@ -12,7 +12,9 @@
 #include <cstdarg>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <thread>
 #include <vector>
@@ -192,8 +194,9 @@ struct rls_ctx {
     bool on = false;
     int64_t l = 0, u = 0, kd = 0, ldab = 0;
     cplx* AB = nullptr;          // n × ldab band work array
-    int w = 8;                   // panel width (8 or 16)
-    int rpl = 8;                 // rows per lane of the trailing update (8, 16, 24 or 32)
+    int w = 0;                   // panel width in use (8 or 16; 0 until the first factorisation)
+    bool w16_fits = false;       // 16-column panels fit in shared memory for this bandwidth
+    double tune_ms8 = 0.0, tune_ms16 = 0.0;   // the timed choice's two factorisations
     cplx* Vp = nullptr;          // BQR_MAXROWS × BQR_WMAX reflectors of one panel
     cplx* Tm = nullptr;          // w × w block-reflector factor of one panel
     cplx* zdev = nullptr;        // the shift the captured factorisation reads
@@ -201,6 +204,7 @@ struct rls_ctx {
     int64_t graph_launches = 0;
     cplx* tmp = nullptr;         // n_pad: (B − zI)v for the refine-point gradient
   } band;
+  int band_panel = 0;              // rls_band_set_panel: 8 or 16, 0 = timed choice
   int scratch_cols = 0;            // minimum column count the shared scratch serves (setup_space)
   PrecState* prec = nullptr;
 

@@ -32,6 +32,8 @@ template <int W>
 int band_factor_launches(rls_ctx* ctx, int64_t* count) {
   auto& B = ctx->band;
   const int64_t n = ctx->n;
+  int rpl = 8;   // the update's rows per lane: the panel's rows W + l over 32 lanes, in steps of 8
+  while (32 * rpl < W + B.l) rpl += 8;
   CK(cudaMemsetAsync(B.AB, 0, sizeof(cplx) * (size_t)n * (size_t)B.ldab, ctx->stream));
   const unsigned gr = (unsigned)((n + 255) / 256);
   k_band_scatter<<<gr, 256, 0, ctx->stream>>>(n, B.kd, B.ldab, ctx->sp[0], B.AB);
@@ -51,9 +53,9 @@ int band_factor_launches(rls_ctx* ctx, int64_t* count) {
       const size_t sm = bqr_update_smem(W, mp);
 #define RLS_BQRU(R) \
   case R: k_bqr_update<W, R><<<g, 32 * BQR_UCOLS, sm, ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, je, B.Vp, B.Tm); break;
-      switch (B.rpl) {
+      switch (rpl) {
         RLS_BQRU(8) RLS_BQRU(16) RLS_BQRU(24) RLS_BQRU(32)
-        default: set_err(ctx, "band QR update: %d rows per lane", B.rpl); return RLS_ERR_STATE;
+        default: set_err(ctx, "band QR update: %d rows per lane", rpl); return RLS_ERR_STATE;
       }
 #undef RLS_BQRU
       ++k;
@@ -66,28 +68,92 @@ int band_factor_launches(rls_ctx* ctx, int64_t* count) {
   return check_launch(ctx, "k_band_tiles");
 }
 
+int band_capture(rls_ctx* ctx, int W, cudaGraphExec_t* ex, int64_t* cnt) {
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const int st = (W == 16) ? band_factor_launches<16>(ctx, cnt) : band_factor_launches<8>(ctx, cnt);
+  const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+  if (st != RLS_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  CK(ce);
+  const cudaError_t ie = cudaGraphInstantiate(ex, g, 0);
+  cudaGraphDestroy(g);
+  CK(ie);
+  return RLS_OK;
+}
+
+// Panel width chosen by timing: one factorisation with 8- and one with 16-column panels (where
+// 16 fits) on the first refine of an operator shape, the faster kept for every later context
+// of the same shape on the device, so that lanes share one choice (and one rounding).
+struct BandTuneCache {
+  std::mutex m;
+  std::map<std::tuple<int, int64_t, int64_t, int64_t>, int> w;
+};
+BandTuneCache& band_tune_cache() {
+  static BandTuneCache c;
+  return c;
+}
+
+int band_time_graph(rls_ctx* ctx, cudaGraphExec_t ex, double* ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, ctx->stream));
+  CK(cudaGraphLaunch(ex, ctx->stream));
+  CK(cudaEventRecord(b, ctx->stream));
+  CK(cudaEventSynchronize(b));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = f;
+  return sync_and_check(ctx);
+}
+
 // R(z) of B − zI into the band tiles T (kernels in bandqr.cuh): the shift goes to device
 // memory, then one graph launch replays the captured sequence.
 int band_factor(rls_ctx* ctx, cplx z) {
   auto& B = ctx->band;
   CK(cudaMemcpyAsync(B.zdev, &z, sizeof(cplx), cudaMemcpyHostToDevice, ctx->stream));
   if (!B.graph) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    int64_t cnt = 0;
-    const int st = (B.w == 16) ? band_factor_launches<16>(ctx, &cnt) : band_factor_launches<8>(ctx, &cnt);
-    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-    if (st != RLS_OK) {
-      if (g) cudaGraphDestroy(g);
-      return st;
+    int w = ctx->band_panel;
+    if (w == 16 && !B.w16_fits) w = 8;
+    const auto key = std::make_tuple(ctx->device, ctx->n, B.l, B.u);
+    auto& cache = band_tune_cache();
+    std::unique_lock<std::mutex> lk(cache.m);
+    if (!w) {
+      auto it = cache.w.find(key);
+      if (it != cache.w.end()) w = it->second;
     }
-    CK(ce);
-    cudaGraphExec_t ex = nullptr;
-    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
-    cudaGraphDestroy(g);
-    CK(ie);
-    B.graph = ex;
-    B.graph_launches = cnt;
+    if (!w && !B.w16_fits) w = 8;
+    if (!w) {   // time both widths once
+      cudaGraphExec_t e8 = nullptr, e16 = nullptr;
+      int64_t c8 = 0, c16 = 0;
+      RET(band_capture(ctx, 8, &e8, &c8));
+      int st = band_capture(ctx, 16, &e16, &c16);
+      double m8 = 0.0, m16 = 0.0;
+      if (st == RLS_OK) st = band_time_graph(ctx, e8, &m8);
+      if (st == RLS_OK) st = band_time_graph(ctx, e16, &m16);
+      if (st != RLS_OK) {
+        if (e8) cudaGraphExecDestroy(e8);
+        if (e16) cudaGraphExecDestroy(e16);
+        return st;
+      }
+      ctx->launches += c8 + c16;
+      B.tune_ms8 = m8;
+      B.tune_ms16 = m16;
+      w = (m16 < m8) ? 16 : 8;
+      cache.w[key] = w;
+      B.graph = (w == 16) ? e16 : e8;
+      B.graph_launches = (w == 16) ? c16 : c8;
+      cudaGraphExecDestroy(w == 16 ? e8 : e16);
+    } else {
+      if (!ctx->band_panel) cache.w.emplace(key, w);
+      RET(band_capture(ctx, w, &B.graph, &B.graph_launches));
+    }
+    B.w = w;
   }
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_BANDQR, &e0);
@@ -377,11 +443,11 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   RET(dalloc_t(ctx, &ctx->ticket, 1));
   RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
   RET(dalloc_t(ctx, &B.AB, (size_t)n * (size_t)B.ldab));
-  // 16-column panels where the panel (and the update's copy of V) fit in 200 KB of shared memory
-  B.w = (bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && bqr_update_smem(16, (int)(16 + l)) <= 200 * 1024 &&
-         16 + l <= BQR_MAXROWS) ? 16 : 8;
-  B.rpl = 8;   // the update's rows per lane: the panel's rows w + l over 32 lanes, in steps of 8
-  while (32 * B.rpl < B.w + l) B.rpl += 8;
+  // 16-column panels are a candidate where the panel (and the update's copy of V) fit in
+  // 200 KB of shared memory; band_factor picks the width by timing
+  B.w16_fits = bqr_panel_smem(16, (int)(16 + l)) <= 200 * 1024 && bqr_update_smem(16, (int)(16 + l)) <= 200 * 1024 &&
+               16 + l <= BQR_MAXROWS;
+  B.w = 0;
   RET(dalloc_t(ctx, &B.Vp, (size_t)BQR_MAXROWS * BQR_WMAX));
   RET(dalloc_t(ctx, &B.Tm, (size_t)BQR_WMAX * BQR_WMAX));
   RET(dalloc_t(ctx, &B.zdev, 1));
@@ -401,4 +467,31 @@ extern "C" int rls_pstrirecy_sparse(rls_ctx* ctx, int64_t n, const int64_t* colp
   if (!ctx) return RLS_ERR_ARG;
   RET(rls_set_sparse_tri(ctx, n, colptr, rowval, nzval, base, perm));
   return rls_pstrirecy_schur_range(ctx, Z, nZ, g, ctl, X0, 0, nZ, sigma_min, st);
+}
+
+extern "C" int rls_band_set_panel(rls_ctx* ctx, int w) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (w != 0 && w != 8 && w != 16) {
+    set_err(ctx, "rls_band_set_panel: width %d (0, 8 or 16)", w);
+    return RLS_ERR_ARG;
+  }
+  ctx->band_panel = w;
+  if (ctx->band.on && ctx->band.graph) {   // recapture at the next factorisation
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaGraphExecDestroy(ctx->band.graph);
+    ctx->band.graph = nullptr;
+    ctx->z_dinv = cmk(NAN, NAN);
+  }
+  return RLS_OK;
+}
+
+extern "C" int rls_band_info(const rls_ctx* ctx, int64_t* l, int64_t* u, int* w, double* ms_w8, double* ms_w16) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (!ctx->band.on) return RLS_ERR_STATE;
+  if (l) *l = ctx->band.l;
+  if (u) *u = ctx->band.u;
+  if (w) *w = ctx->band.w;
+  if (ms_w8) *ms_w8 = ctx->band.tune_ms8;
+  if (ms_w16) *ms_w16 = ctx->band.tune_ms16;
+  return RLS_OK;
 }

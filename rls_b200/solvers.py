@@ -252,6 +252,17 @@ class Engine:
         check(lib().rls_test_band_r(self._h, c64(z.real, z.imag), ptr(R), n, C.byref(l), C.byref(u)), self._h)
         return R, int(l.value), int(u.value)
 
+    def band_set_panel(self, w: int):
+        """Band QR panel width: 8, 16 or 0 (timed choice)."""
+        check(lib().rls_band_set_panel(self._h, int(w)), self._h)
+
+    def band_info(self):
+        """(l, u, panel width in use, timed ms with 8 and with 16 columns) of the sparse operator."""
+        l, u, w = C.c_int64(0), C.c_int64(0), C.c_int(0)
+        m8, m16 = C.c_double(0), C.c_double(0)
+        check(lib().rls_band_info(self._h, C.byref(l), C.byref(u), C.byref(w), C.byref(m8), C.byref(m16)), self._h)
+        return int(l.value), int(u.value), int(w.value), float(m8.value), float(m16.value)
+
     def band_factor(self, z: complex):
         """One device factorisation R(z) of B − zI (test hook rls_test_band_factor), synchronised."""
         z = complex(z)

@@ -140,3 +140,32 @@ def test_sparse_operator_is_dropped_by_a_schur_upload(cuda_device):
             eng.band_r(0.1)                   # no sparse operator any more
     finally:
         eng.close()
+
+
+@pytest.mark.parametrize("name", ["skew7_rcm", "af_shaped_rcm"])
+def test_band_qr_panel_widths_agree(cuda_device, name):
+    """8- and 16-column panels (forced) give LAPACK's R up to row phases; the timed choice picks
+    one of them and reports both timings."""
+    C, perm = CASES[name]()
+    S = R.SparseTri(C, perm)
+    eng = R.Engine(0)
+    try:
+        eng.set_sparse_tri(S)
+        B = sp.csc_matrix(C)[S.perm][:, S.perm].toarray()
+        n = B.shape[0]
+        z = 0.3 - 0.2j
+        Rl = np.linalg.qr(B - z * np.eye(n), mode="r")
+        scale = np.linalg.norm(B, 2) + 1.0
+        for w in (8, 16, 0):
+            eng.band_set_panel(w)
+            Rg, l, u = eng.band_r(z)
+            d = np.diag(Rl) / np.diag(Rg)
+            assert np.allclose(np.abs(d), 1.0, atol=1e-9)
+            assert np.max(np.abs(d[:, None] * Rg - Rl)) <= 1e-12 * scale * np.sqrt(n)
+            _, _, wsel, m8, m16 = eng.band_info()
+            if w:
+                assert wsel == w
+            else:
+                assert wsel in (8, 16)
+    finally:
+        eng.close()
