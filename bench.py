@@ -97,6 +97,7 @@ def parse():
                     help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--pp-chunk", type=int, default=100, help="grid points per step of the af23560 (psPrecRecy) leg")
+    ap.add_argument("--pp-lanes", type=int, default=8, help="concurrent lanes of the af23560 (psPrecRecy) leg")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=None, help="matrix order (default: the workload's)")
     ap.add_argument("--factor-only", type=int, default=0,
@@ -796,6 +797,18 @@ def run_precrecy(args):
     X0p = rng.random((n, 40)) + 1j * rng.random((n, 40))
     xb = rng.random((n, 1)) + 1j * rng.random((n, 1))
     e = Engine(0)
+    if args.ncu_window:   # warm points, then the profiled window between profiler start/stop
+        warm, count = (int(x) for x in args.ncu_window.split(","))
+        run = PrecRecyRun(e, C, rec, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb)
+        run.run(0, warm)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        _, st = run.run(warm, warm + count)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(f"profiled points {warm}..{warm + count - 1}", flush=True)
+        e.close()
+        return
     t0 = time.perf_counter()
     run = PrecRecyRun(e, C, rec, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb)
     run.run(0, args.warmup * s)
@@ -852,6 +865,50 @@ def run_precrecy(args):
                            "frac": ach / hbm, "traffic": None,
                            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "launches": cnt,
                            "avg_us": tot / cnt * 1e3}
+    # concurrent lanes (PrecRecyLanes): every lane its own preconditioner and spaces, steps of s
+    # lane-local points; the timed steps are one lane-parallel call, device time = the latest lane
+    if args.pp_lanes > 1:
+        from rls_b200.solvers import PrecRecyLanes
+        L = args.pp_lanes
+        t0 = time.perf_counter()
+        ls = PrecRecyLanes(L, C, rec, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb)
+        offs = ls.offs
+        if nst * s > int(np.min(np.diff(offs))):
+            raise SystemExit(f"--pp-chunk × (warmup + steps) = {nst * s} exceeds a lane of {int(np.min(np.diff(offs)))}")
+        ls.run(0, args.warmup * s)
+        torch.cuda.synchronize()
+        t_warm_l = time.perf_counter() - t0
+        streams = [torch.cuda.ExternalStream(q) for q in ls.streams()]
+        e0s = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        e1s = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        l0 = ls.launches()
+        for a, q in zip(e0s, streams):
+            a.record(q)
+        t1 = time.perf_counter()
+        sigL, stL = ls.run(args.warmup * s, nst * s)
+        for b, q in zip(e1s, streams):
+            b.record(q)
+        for b in e1s:
+            b.synchronize()
+        wall_l = time.perf_counter() - t1
+        l1 = ls.launches()
+        ms_l = max(a.elapsed_time(b) for a, b in zip(e0s, e1s))
+        ls.close()
+        timedL = np.concatenate([np.arange(o + args.warmup * s, o + nst * s) for o in offs[:-1]])
+        out["single_lane"] = {"value": v, "unit": "pts/s", "mode": "one traversal (the reference's single run)"}
+        v = L * args.steps * s / (ms_l / 1e3)
+        out.update({"value": v, "ms_per_step": ms_l / args.steps, "gpu_launches": int(l1 - l0)})
+        out["e2e"] = {"value": L * nst * s / (t_warm_l + wall_l), "unit": "pts/s",
+                      "h2d_bytes_per_step": int((L * (C.nnz * 32 + n * 8) + L * nst * s * 16) / nst),
+                      "d2h_bytes_per_step": int(L * s * 8),
+                      "span": f"PrecRecyLanes through the public API from host buffers: C uploaded to {L} lanes, "
+                              f"each lane's preconditioner built at its first point, steps 0..{nst - 1}, wall clock"}
+        out["config"]["lanes"] = L
+        out["config"]["points_per_step"] = L * s
+        out["stats"]["lanes"] = {"main_refines_timed": int(np.sum(stL.main_refine_it[timedL] > 0)),
+                                 "pred_refines_timed": int(np.sum(stL.pred_refine_it[timedL] > 0)),
+                                 "precond_builds": stL.n_precond_rebuild_pts}
+        sig, timed = sigL, timedL
     # accuracy of the timed points against the FP64 sparse-LU truth (after the timed region)
     pick = timed[np.linspace(0, len(timed) - 1, min(args.accuracy_points, len(timed), 8)).astype(np.int64)]
     if args.accuracy_points > 0:
@@ -946,6 +1003,24 @@ def run_sparse_tri(args):
         print(json.dumps(out), flush=True)
         return
     torch.cuda.set_device(local)
+    if args.ncu_window:   # one context: warm points, then the profiled window between profiler start/stop
+        warm, count = (int(x) for x in args.ncu_window.split(","))
+        S = R.SparseTri(C)
+        eng = R.Engine(local)
+        eng.set_sparse_tri(S)
+        sig = np.full(len(rec.Z), np.nan)
+        st = PsTriRecyStats.alloc(len(rec.Z))
+        cst = eng.stats_struct(st)
+        eng.pstrirecy_range(rec, ctl, 0, warm, sig, st, cst, X0=X0)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        eng.pstrirecy_range(rec, ctl, warm, warm + count, sig, st, cst)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(f"profiled points {warm}..{warm + count - 1}: {int(np.sum(st.refine_it[warm:warm + count] > 0))} "
+              "refines", flush=True)
+        eng.close()
+        return
     if args.factor_only > 0:   # the refine's factorisation alone: R(z) of B − zI at successive grid points
         if rank != 0:
             return

@@ -17,7 +17,7 @@ from .grid import (Recursion, recursion_grid, recursion_grid_zigzag, recursion_g
                    reorder_to_natural_grid)
 from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine, Lanes, ShiftedMat, SparseLLTP,
                       SparseLLTP_AD, SchurFactor, SparseTri, band_order, pre_process, psTriRecy, ic_factor, get_hsl_LLTP, PsPrecRecyControl,
-                      PsPrecRecyStats, PrecRecyRun, psPrecRecy)
+                      PsPrecRecyStats, PrecRecyRun, PrecRecyLanes, psPrecRecy)
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
 from .distributed import psTriRecy_ranks, column_shares
@@ -29,5 +29,5 @@ __all__ = [
     "pre_process",
     "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
     "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException", "PsPrecRecyControl",
-    "PsPrecRecyStats", "PrecRecyRun", "psPrecRecy", "psTriRecy_ranks", "column_shares",
+    "PsPrecRecyStats", "PrecRecyRun", "PrecRecyLanes", "psPrecRecy", "psTriRecy_ranks", "column_shares",
 ]

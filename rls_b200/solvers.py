@@ -965,8 +965,89 @@ class PrecRecyRun:
         return self.sigma, self.st
 
 
+class PrecRecyLanes:
+    """psPrecRecy on concurrent lanes of one GPU (no reference counterpart): the traversal is split
+    on column boundaries as rls_lane_offsets splits it, and each lane runs the reference's loop on
+    its part from its own start (its own Engine, preconditioner built at its first point, both
+    recycled spaces), driven from its own host thread (the library calls release the GIL)."""
+
+    def __init__(self, lanes: int, C_, rec: Recursion, control: PsPrecRecyControl, p=None, X0_main=None,
+                 X0_pred=None, X0_bound=None, device: int = 0):
+        import scipy.sparse as sp
+        if lanes < 1:
+            raise ArgumentError(-1, f"lanes must be >= 1, got {lanes}")
+        A = sp.csc_matrix(C_, dtype=np.complex128)
+        nZ = len(rec.Z)
+        off = np.zeros(lanes + 1, dtype=np.int64)
+        g = rec.c_grid()
+        check(lib().rls_lane_offsets(C.byref(g), nZ, lanes, ptr(off)), None)
+        self.offs = off
+        self.nZ = nZ
+        self.engines, self.runs = [], []
+        for l in range(lanes):
+            sub = Recursion(rec.x_st, rec.x_ed, rec.y_st, rec.y_ed, rec.n_x, rec.n_y, rec.k)
+            sub.Z = np.ascontiguousarray(rec.Z[off[l]:off[l + 1]])
+            e = Engine(device)
+            self.engines.append(e)
+            self.runs.append(PrecRecyRun(e, A, sub, control, p=p, X0_main=X0_main, X0_pred=X0_pred,
+                                         X0_bound=X0_bound))
+
+    def run(self, j_begin=0, j_end=None):
+        """Lane-local points j_begin..j_end−1 of every lane (all lanes at once)."""
+        import threading
+        errs = [None] * len(self.runs)
+
+        def go(i):
+            r = self.runs[i]
+            n = len(r.Z)
+            b = min(j_begin, n)
+            e = n if j_end is None else min(j_end, n)
+            if b < e:
+                try:
+                    r.run(b, e)
+                except Exception as exc:  # noqa: BLE001  (re-raised below, first lane first)
+                    errs[i] = exc
+        th = [threading.Thread(target=go, args=(i,)) for i in range(len(self.runs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        for e in errs:
+            if e is not None:
+                raise e
+        return self.result()
+
+    def result(self):
+        """σ and stats over the whole traversal: per-point arrays in rec.Z order, the point lists
+        concatenated lane by lane, times and counts summed."""
+        sigma = np.concatenate([r.sigma for r in self.runs])
+        st = PsPrecRecyStats(self.nZ)
+        for f in PsPrecRecyStats._I:
+            setattr(st, f, np.concatenate([getattr(r.st, f) for r in self.runs]))
+        for f in PsPrecRecyStats._S:
+            setattr(st, f, sum(getattr(r.st, f) for r in self.runs))
+        lists = {"pts": "n_pts", "pred_pts": "n_pred_pts", "precond_rebuild_pts": "n_precond_rebuild_pts"}
+        for f, cnt in lists.items():
+            v = np.zeros(self.nZ, dtype=np.complex128)
+            parts = [getattr(r.st, f)[:getattr(r.st, cnt)] for r in self.runs]
+            cat = np.concatenate(parts) if parts else v[:0]
+            v[:cat.size] = cat
+            setattr(st, f, v)
+        return sigma, st
+
+    def streams(self):
+        return [e.stream_ptr() for e in self.engines]
+
+    def launches(self) -> int:
+        return sum(e.launches() for e in self.engines)
+
+    def close(self):
+        for e in self.engines:
+            e.close()
+
+
 def psPrecRecy(C_, rec: Recursion, control: PsPrecRecyControl = None, verbose: int = 1, io=None, p=None,
-               X0_main=None, X0_pred=None, X0_bound=None, device: int = 0):
+               X0_main=None, X0_pred=None, X0_bound=None, device: int = 0, lanes: int = 1):
     """psPrecRecy (psPrecRecy.jl:617-623; a dense C is made sparse, :1036-1042) →
     (σ_min in rec.Z order, PsPrecRecyStats).
 
@@ -974,6 +1055,8 @@ def psPrecRecy(C_, rec: Recursion, control: PsPrecRecyControl = None, verbose: i
     SuiteSparse; None here takes reverse Cuthill–McKee of C + Cᵀ as the stand-in fill-reducing
     order.  ``X0_main`` (n × r_main), ``X0_pred`` (n × r_pred) and ``X0_bound`` (n × 1) stand in
     for the reference's rand! draws; None draws fixed uniform [0,1) blocks on the device.
+    ``lanes`` > 1 runs column-aligned parts of the traversal concurrently (PrecRecyLanes); 1
+    keeps the reference's single traversal.
     """
     import scipy.sparse as sp
     control = control or PsPrecRecyControl()
@@ -989,6 +1072,14 @@ def psPrecRecy(C_, rec: Recursion, control: PsPrecRecyControl = None, verbose: i
         io.write("[psPrecRecy] control:\n")
         for f in control.__dataclass_fields__:
             io.write(f"  {f} = {getattr(control, f)!r}\n")
+    if lanes > 1:
+        ls = PrecRecyLanes(lanes, A, rec, control, p=p, X0_main=X0_main, X0_pred=X0_pred, X0_bound=X0_bound,
+                           device=device)
+        try:
+            sigma, st = ls.run()
+        finally:
+            ls.close()
+        return sigma, st
     eng = _engine(device)
     if verbose >= 1:
         eng.set_log(lambda line: io.write(line + "\n"), verbose)

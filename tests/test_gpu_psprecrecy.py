@@ -181,6 +181,38 @@ def test_psprecrecy_range_calls_equal_one_call(cuda_device):
     assert st1.n_pred_pts == st2.n_pred_pts
 
 
+def test_psprecrecy_lanes_equal_runs_on_their_subgrids(cuda_device):
+    """PrecRecyLanes: each lane is exactly a psPrecRecy run on its column-aligned part of the
+    traversal (same σ bit for bit, same per-point counters), and σ meets the dense SVD."""
+    from rls_b200.grid import Recursion
+    C, normC, p = small_case(240)
+    n = 240
+    rng = np.random.default_rng(23)
+    X0m, X0p, xb = crand(rng, n, 6), crand(rng, n, 4), crand(rng, n, 1)
+    ctl, _ = _pp_control(normC, 4, "shiftchol", 6)
+    rec = R.recursion_grid(-1.6, 0.8, -1.55, 1.55, 8, 6, 3)
+    sig, st = R.psPrecRecy(C, rec, ctl, verbose=0, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb, lanes=3)
+    ls = R.PrecRecyLanes(3, C, rec, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb)
+    offs = ls.offs
+    ls.close()
+    assert offs[0] == 0 and offs[-1] == len(rec.Z) and np.all(np.diff(offs) > 0)
+    e = R.Engine(0)
+    try:
+        for l in range(3):
+            sub = Recursion(rec.x_st, rec.x_ed, rec.y_st, rec.y_ed, rec.n_x, rec.n_y, rec.k)
+            sub.Z = np.ascontiguousarray(rec.Z[offs[l]:offs[l + 1]])
+            s1, st1 = R.PrecRecyRun(e, C, sub, ctl, p=p, X0_main=X0m, X0_pred=X0p, X0_bound=xb).run()
+            assert np.array_equal(sig[offs[l]:offs[l + 1]], s1)
+            assert np.array_equal(st.main_refine_it[offs[l]:offs[l + 1]], st1.main_refine_it)
+            assert np.array_equal(st.pred_refine_it[offs[l]:offs[l + 1]], st1.pred_refine_it)
+    finally:
+        e.close()
+    A = C.toarray()
+    truth = np.array([sla.svdvals(A - z * np.eye(n))[-1] for z in rec.Z])
+    assert np.max(np.abs(sig - truth)) <= 1e-4 * normC
+    assert st.n_precond_rebuild_pts >= 3     # one build per lane at least
+
+
 def test_psprecrecy_rejects_unsupported_settings(cuda_device):
     C, normC, p = small_case(120)
     rec = R.recursion_grid(-1.6, 0.8, -1.55, 1.55, 4, 4, 2)
