@@ -218,6 +218,184 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
   }
 }
 
+// Strided partial dot over rows lo + off, lo + off + step, ... < hi (two accumulators), then the
+// warp sum.
+template <bool CONJ_A>
+__device__ __forceinline__ cplx strided_dot(const cplx* __restrict__ a, const cplx* __restrict__ b, int lo, int hi,
+                                            int off, int step) {
+  cplx s0 = czero(), s1 = czero();
+  int i = lo + off;
+  for (; i + step < hi; i += 2 * step) {
+    s0 = cfma(CONJ_A ? cconj(a[i]) : a[i], b[i], s0);
+    s1 = cfma(CONJ_A ? cconj(a[i + step]) : a[i + step], b[i + step], s1);
+  }
+  if (i < hi) s0 = cfma(CONJ_A ? cconj(a[i]) : a[i], b[i], s0);
+  cplx d = cadd(s0, s1);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d.x += __shfl_xor_sync(0xffffffffu, d.x, o);
+    d.y += __shfl_xor_sync(0xffffffffu, d.y, o);
+  }
+  return d;
+}
+
+__device__ __forceinline__ void group_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// The same panel with G warps per column (W·G = 32 warps, 1024 threads): the G warps of column
+// q split its rows (warp g takes rows ≡ 32g + lane mod 32G), and their partial sums meet in
+// shared memory behind a named barrier of the column's G warps (id 1 + q), summed in a fixed
+// order.  Per reflector a column's chain is a quarter (G = 4) of the rows per lane; the flags
+// and everything else are those of k_bqr_panel.
+template <int W, int G>
+__global__ void __launch_bounds__(32 * W * G) k_bqr_panel_g(int64_t l, int64_t kd, int64_t ldab,
+                                                            cplx* __restrict__ AB, int64_t c0, int w, int mp,
+                                                            cplx* __restrict__ Vp, cplx* __restrict__ Tm, int* err) {
+  static_assert(W * G == 32 && W <= 15, "32 warps, at most 15 named column barriers");
+  extern __shared__ cplx P[];
+  __shared__ cplx taus[W], scl[W], alph[W];
+  __shared__ cplx part[W][G];
+  __shared__ double npart[W][G];
+  __shared__ cplx Y[W][W + 1];
+  __shared__ int ready[W];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int q = wid / G, g = wid % G;          // column, and this warp's share of its rows
+  const int off = 32 * g + lane, step = 32 * G;
+  auto valid = [&](int i, int qq) { return (int64_t)(i - qq) <= l && (int64_t)(qq - i) <= kd; };
+  auto iend_of = [&](int s) { return (int)min((int64_t)mp, (int64_t)s + l + 1); };
+  if (threadIdx.x < W) ready[threadIdx.x] = 0;
+  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
+    const int qq = e / mp, i = e % mp;
+    if (valid(i, qq)) cp_async16(&P[e], &AB[(c0 + qq) * ldab + (i - qq + kd)]);
+    else P[e] = czero();
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (q < w) {
+    cplx* Pq = P + (size_t)q * mp;
+    double xn2 = 0.0;
+    if (q == 0) {   // tail norm and α of column 0
+      const int e0 = iend_of(0);
+      double t = 0.0;
+      for (int i = 1 + off; i < e0; i += step) t += cabs2(Pq[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) npart[0][g] = t;
+      if (g == 0 && lane == 0) alph[0] = Pq[0];
+      group_bar(1 + q, 32 * G);
+#pragma unroll
+      for (int h = 0; h < G; ++h) xn2 += npart[0][h];
+    }
+    for (int s = 0; s < q; ++s) {
+      int spins = 0;
+      while (*(volatile int*)&ready[s] == 0) {
+        if (++spins > RLS_SPIN_LIMIT) {
+          if (lane == 0) atomicOr(err, DEVERR_SPIN_TIMEOUT);
+          break;
+        }
+      }
+      __threadfence_block();
+      const cplx* Ps = P + (size_t)s * mp;
+      const int iend = iend_of(s);
+      const cplx dp = strided_dot<true>(Ps, Pq, s + 1, iend, off, step);
+      if (lane == 0) part[q][g] = dp;
+      const cplx as = Pq[s];   // read by every warp of the group before the barrier
+      group_bar(1 + q, 32 * G);
+      cplx dsum = czero();
+#pragma unroll
+      for (int h = 0; h < G; ++h) dsum = cadd(dsum, part[q][h]);
+      const cplx sc = scl[s];
+      const cplx f = cmul(cconj(taus[s]), cadd(as, cmul(cconj(sc), dsum)));
+      const cplx gg = cmul(sc, f);
+      if (s == q - 1) {   // the last one before this column's turn: update, sum the new tail, α
+        const int e1 = iend_of(q);
+        double t = 0.0;
+        for (int i = s + 1 + off; i < e1; i += step) {
+          cplx v = Pq[i];
+          if (i < iend) {
+            v = cfms(Ps[i], gg, v);
+            Pq[i] = v;
+          }
+          if (i > q) t += cabs2(v);
+          if (i == q) alph[q] = v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) npart[q][g] = t;
+        if (g == 0 && lane == 0) Pq[s] = csub(as, f);
+        group_bar(1 + q, 32 * G);
+        xn2 = 0.0;
+#pragma unroll
+        for (int h = 0; h < G; ++h) xn2 += npart[q][h];
+      } else {
+        for (int i = s + 1 + off; i < iend; i += step) Pq[i] = cfms(Ps[i], gg, Pq[i]);
+        if (g == 0 && lane == 0) Pq[s] = csub(as, f);
+        // the next reflector's partial sums go to part[q][·] again: every warp of the group has
+        // read this one's before any rewrites it
+        group_bar(1 + q, 32 * G);
+      }
+    }
+    // this column's reflector, formed redundantly by the G warps from the same sums
+    const cplx alpha = alph[q];
+    cplx tau = czero(), sc = czero();
+    double beta = alpha.x;
+    if (xn2 > 0.0 || alpha.y != 0.0) {
+      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+      beta = (alpha.x >= 0.0) ? -nrm : nrm;
+      tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+      sc = cinv(csub(alpha, cmk(beta, 0.0)));
+    }
+    if (g == 0 && lane == 0) {
+      Pq[q] = cmk(beta, 0.0);
+      taus[q] = tau;
+      scl[q] = sc;
+      if (!isfinite(beta)) atomicOr(err, DEVERR_NONFINITE);
+      __threadfence_block();
+      *(volatile int*)&ready[q] = 1;
+    }
+  }
+  __syncthreads();
+  // Y[k][s] = v_kᴴ v_s, pairs k < s spread over the warps
+  const int npairs = w * (w - 1) / 2;
+  for (int pidx = wid; pidx < npairs; pidx += 32) {
+    int s = 1, k = pidx;
+    while (k >= s) { k -= s; ++s; }
+    const cplx* Pk = P + (size_t)k * mp;
+    const cplx* Ps = P + (size_t)s * mp;
+    const cplx y = warp_dot<true>(Pk, Ps, s + 1, iend_of(s), lane);
+    if (lane == 0) Y[k][s] = cmul(cconj(scl[k]), cadd(cconj(Pk[s]), cmul(scl[s], y)));
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < w * mp; e += blockDim.x) {
+    const int qq = e / mp, i = e % mp;
+    cplx v = P[e];
+    if (i > qq) v = cmul(v, scl[qq]);
+    if (valid(i, qq)) AB[(c0 + qq) * ldab + (i - qq + kd)] = v;
+    Vp[(int64_t)qq * BQR_MAXROWS + i] = (i < qq) ? czero() : (i == qq ? cmk(1.0, 0.0) : v);
+  }
+  if (wid == 0 && lane < W) {
+    cplx trow[W];
+#pragma unroll
+    for (int s = 0; s < W; ++s) {
+      cplx tv = czero();
+      if (s < w) {
+        if (lane == s) {
+          tv = taus[s];
+        } else if (lane < s) {
+          cplx acc = czero();
+#pragma unroll
+          for (int k = 0; k < s; ++k)
+            if (k >= lane) acc = cfma(trow[k], Y[k][s], acc);
+          tv = cneg(cmul(taus[s], acc));
+        }
+      }
+      trow[s] = tv;
+      Tm[(int64_t)s * W + lane] = tv;
+    }
+  }
+}
+
 inline size_t bqr_panel_smem(int w, int mp) { return (size_t)w * mp * sizeof(cplx); }
 
 // C ← C − V·Tᴴ·(VᴴC) on the trailing columns jb .. je−1 (jb = c0 + w), rows c0 .. c0+mp−1.

@@ -1390,7 +1390,7 @@ int set_kernel_attrs(rls_ctx* ctx) {
   RET(allow_big_smem(ctx, k_bqr_update<16, 16>, optin));
   RET(allow_big_smem(ctx, k_bqr_update<16, 24>, optin));
   RET(allow_big_smem(ctx, k_bqr_update<16, 32>, optin));
-  RET(allow_big_smem(ctx, k_bqr_panel<8>, optin));
+  RET(allow_big_smem(ctx, k_bqr_panel_g<8, 4>, optin));
   RET(allow_big_smem(ctx, k_bqr_panel<16>, optin));
   return RLS_OK;
 }

@@ -43,8 +43,12 @@ int band_factor_launches(rls_ctx* ctx, int64_t* count) {
   for (int64_t c0 = 0; c0 < n; c0 += W) {
     const int w = (int)std::min<int64_t>(W, n - c0);
     const int mp = (int)std::min<int64_t>(n - c0, w + B.l);
-    k_bqr_panel<W><<<1, 32 * W, bqr_panel_smem(w, mp), ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, B.Vp,
-                                                                      B.Tm, ctx->derr);
+    if (W == 8)   // 8 columns, 4 warps per column
+      k_bqr_panel_g<8, 4><<<1, 1024, bqr_panel_smem(w, mp), ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp,
+                                                                           B.Vp, B.Tm, ctx->derr);
+    else
+      k_bqr_panel<W><<<1, 32 * W, bqr_panel_smem(w, mp), ctx->stream>>>(B.l, B.kd, B.ldab, B.AB, c0, w, mp, B.Vp,
+                                                                        B.Tm, ctx->derr);
     ++k;
     const int64_t je = std::min<int64_t>(n, c0 + mp + B.u);
     const int64_t ncw = je - (c0 + w);
