@@ -161,8 +161,11 @@ __global__ void __launch_bounds__(32 * W) k_bqr_panel(int64_t l, int64_t kd, int
     if (xn2 > 0.0 || alpha.y != 0.0) {
       const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
       beta = (alpha.x >= 0.0) ? -nrm : nrm;
-      tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-      sc = cinv(csub(alpha, cmk(beta, 0.0)));
+      const double ib = recip_nr(beta);                      // reciprocals refined by Newton–Raphson
+      tau = cmk((beta - alpha.x) * ib, -alpha.y * ib);
+      const double ar = alpha.x - beta, ai = alpha.y;        // sc = 1 / (α − β)
+      const double id = recip_nr(ar * ar + ai * ai);
+      sc = cmk(ar * id, -ai * id);
     }
     __syncwarp();   // every lane has read α
     if (lane == 0) {
@@ -343,8 +346,11 @@ __global__ void __launch_bounds__(32 * W * G) k_bqr_panel_g(int64_t l, int64_t k
     if (xn2 > 0.0 || alpha.y != 0.0) {
       const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
       beta = (alpha.x >= 0.0) ? -nrm : nrm;
-      tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-      sc = cinv(csub(alpha, cmk(beta, 0.0)));
+      const double ib = recip_nr(beta);                      // reciprocals refined by Newton–Raphson
+      tau = cmk((beta - alpha.x) * ib, -alpha.y * ib);
+      const double ar = alpha.x - beta, ai = alpha.y;        // sc = 1 / (α − β)
+      const double id = recip_nr(ar * ar + ai * ai);
+      sc = cmk(ar * id, -ai * id);
     }
     if (g == 0 && lane == 0) {
       Pq[q] = cmk(beta, 0.0);
