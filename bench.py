@@ -93,6 +93,7 @@ def parse():
     ap.add_argument("--chunk", type=int, default=200,
                     help="grid points per lane per step (at most; lowered to fit the lane's share of the grid)")
     ap.add_argument("--lanes", type=int, default=20, help="concurrent grid lanes per GPU")
+    ap.add_argument("--trsm-backoff", type=int, default=32, help="longest ns between TRSM flag polls")
     ap.add_argument("--trsm-ctas", type=int, default=0,
                     help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
@@ -452,6 +453,7 @@ def run_ours(args):
         ls = R.Lanes(nl, local, T)
         if nl > 1:
             ls.set_trsm_ctas(args.trsm_ctas)
+        ls.set_trsm_backoff(args.trsm_backoff)
         offs = ls.offsets(sub)
         if need > int(np.min(np.diff(offs))):
             raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds a lane of {int(np.min(np.diff(offs)))} points")
@@ -561,6 +563,7 @@ def run_ours(args):
     out["config"]["lanes"] = lanes
     out["config"]["chunk"] = s
     out["config"]["trsm_ctas"] = args.trsm_ctas or "one per half block row"
+    out["config"]["trsm_backoff_ns"] = args.trsm_backoff
     out["config"]["parallelism"] = (f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
                                     "(independent traversals from column starts)")
     out["config"]["refine_fraction_timed"] = refines / (lanes * args.steps * s)

@@ -304,6 +304,11 @@ int rls_set_schur_copy(rls_ctx* dst, rls_ctx* src);
  * makes each CTA solve several half block rows in dependency order and leaves SMs to
  * concurrent lanes.  Values above 2·ceil(n/64) act as 0.  No reference counterpart. */
 int rls_set_trsm_ctas(rls_ctx* ctx, int ctas);
+/* Longest back-off, in ns, between the triangular solve's polls of a dependency's flag (32 to
+ * 2^20; default 32): polls start back-to-back and, after 64, sleep 32 ns doubling up to this
+ * cap.  A longer cap lowers the L2 traffic of waiting CTAs at the cost of hand-off latency.  No
+ * reference counterpart. */
+int rls_set_trsm_backoff(rls_ctx* ctx, int max_ns);
 
 /* ---- solvers ------------------------------------------------------------------ */
 

@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(256) k_trsm_half(int nb, int bw, const cplx* _
                                                    const cplx* __restrict__ Dinv,
                                                    const cplx* __restrict__ B, cplx* __restrict__ X, cplx* U,
                                                    int64_t ldx, int adj, int* __restrict__ ticket, int* flags,
-                                                   int epoch, int* err) {
+                                                   int epoch, int* err, int sleep_cap) {
   extern __shared__ cplx sm[];
   cplx* sA = sm;                       // TILE·HT_LDS
   cplx* sX = sA + TILE * HT_LDS;       // TILE·K
@@ -554,9 +554,13 @@ __global__ void __launch_bounds__(256) k_trsm_half(int nb, int bw, const cplx* _
       if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {             // threads 0 and 32: one half each
         const int* f = &flags[2 * dep + (threadIdx.x >> 5)];
         int spins = 0;
+        unsigned ns = 32;   // back-off between polls after 64 spins: 32 ns doubling up to sleep_cap
         while (ld_acquire(f) != epoch) {
           if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
-          if (spins > 64) __nanosleep(32);
+          if (spins > 64) {
+            __nanosleep(ns);
+            if (ns < (unsigned)sleep_cap) ns <<= 1;
+          }
         }
       }
       __syncthreads();

@@ -68,6 +68,7 @@ struct rls_ctx {
   int* flags = nullptr;     // 2·nb (one per half block row)
   int* ticket = nullptr;    // 1
   int trsm_ctas = 0;        // CTAs of a triangular solve (0: one per half block row)
+  int trsm_sleep_cap = 32;  // longest back-off between flag polls of the triangular solve, ns
   int epoch = 0;
   int* trmm_uO[2] = {nullptr, nullptr};
   int* trmm_us[2] = {nullptr, nullptr};
@@ -704,7 +705,8 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
   case K:                                                                                                        \
     k_trsm_half<K><<<ctas, 256, smem, ctx->stream>>>(ctx->nb, ctx->tile_bw, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, \
                                                      ld, adj,                                                    \
-                                                     ctx->ticket, ctx->flags, ctx->epoch, ctx->derr);           \
+                                                     ctx->ticket, ctx->flags, ctx->epoch, ctx->derr,            \
+                                                     ctx->trsm_sleep_cap);                                       \
     break;
   switch (k) {
     RLS_TRSM_CASE(1) RLS_TRSM_CASE(2) RLS_TRSM_CASE(3) RLS_TRSM_CASE(4)
@@ -1609,6 +1611,16 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
       }
     }
   return operator_setup(ctx, n, h.data(), nullptr);
+}
+
+extern "C" int rls_set_trsm_backoff(rls_ctx* ctx, int max_ns) {
+  if (!ctx) return RLS_ERR_ARG;
+  if (max_ns < 32 || max_ns > 1 << 20) {
+    set_err(ctx, "rls_set_trsm_backoff: %d ns (32 .. 1048576)", max_ns);
+    return RLS_ERR_ARG;
+  }
+  ctx->trsm_sleep_cap = max_ns;
+  return RLS_OK;
 }
 
 extern "C" int rls_set_trsm_ctas(rls_ctx* ctx, int ctas) {

@@ -352,6 +352,10 @@ class Engine:
         """Host waits: spin (spin_us < 0, default) or poll spin_us µs and then sleep."""
         check(lib().rls_ctx_set_host_wait(self._h, int(spin_us)), self._h)
 
+    def set_trsm_backoff(self, max_ns: int):
+        """Longest back-off (ns) between the triangular solve's flag polls."""
+        check(lib().rls_set_trsm_backoff(self._h, int(max_ns)), self._h)
+
     def stream_ptr(self) -> int:
         return int(lib().rls_ctx_stream(self._h) or 0)
 
@@ -660,6 +664,10 @@ class Lanes:
     def set_host_wait(self, spin_us: int):
         for e in self.engines:
             e.set_host_wait(spin_us)
+
+    def set_trsm_backoff(self, max_ns: int):
+        for e in self.engines:
+            e.set_trsm_backoff(max_ns)
 
     def set_profile(self, on: bool):
         for e in self.engines:
