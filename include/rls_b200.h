@@ -309,6 +309,12 @@ int rls_set_trsm_ctas(rls_ctx* ctx, int ctas);
  * cap.  A longer cap lowers the L2 traffic of waiting CTAs at the cost of hand-off latency.  No
  * reference counterpart. */
 int rls_set_trsm_backoff(rls_ctx* ctx, int max_ns);
+/* CUDA-graph replay of the refine's steady LOBPCG iteration (on: 1, the default; off: 0).  From
+ * the second iteration on, the previous iteration's orthogonalisation and solve and this one's
+ * Rayleigh–Ritz and residual (≈30 launches) are one graph launch, captured once per space;
+ * results are the same bit for bit.  Per-kernel profiling (rls_ctx_set_profile) runs the
+ * launches directly.  No reference counterpart. */
+int rls_ctx_set_graphs(rls_ctx* ctx, int on);
 
 /* ---- solvers ------------------------------------------------------------------ */
 

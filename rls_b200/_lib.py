@@ -101,6 +101,7 @@ SIGNATURES = {
                                        C.POINTER(rls_pstrirecy_control), P, P, C.POINTER(rls_pstrirecy_stats)]),
     "rls_set_trsm_ctas": (C.c_int, [P, C.c_int]),
     "rls_set_trsm_backoff": (C.c_int, [P, C.c_int]),
+    "rls_ctx_set_graphs": (C.c_int, [P, C.c_int]),
     "rls_ctx_set_host_wait": (C.c_int, [P, C.c_int]),
     "rls_pstrirecy_schur": (C.c_int, [P, P, C.c_int64, C.POINTER(rls_grid), C.POINTER(rls_pstrirecy_control), P, P,
                                       C.POINTER(rls_pstrirecy_stats)]),

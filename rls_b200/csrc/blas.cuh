@@ -501,19 +501,35 @@ __global__ void __launch_bounds__(256) k_trsm_half(int nb, int bw, const cplx* _
                                                    const cplx* __restrict__ Dinv,
                                                    const cplx* __restrict__ B, cplx* __restrict__ X, cplx* U,
                                                    int64_t ldx, int adj, int* __restrict__ ticket, int* flags,
-                                                   int epoch, int* err, int sleep_cap) {
+                                                   int* err, int sleep_cap) {
   extern __shared__ cplx sm[];
   cplx* sA = sm;                       // TILE·HT_LDS
   cplx* sX = sA + TILE * HT_LDS;       // TILE·K
   cplx* sAcc = sX + TILE * K;          // 32·K
   cplx* sPart = sAcc + 32 * K;         // 8·K·32
   __shared__ int sblk;
+  // ticket[0]: the work counter; ticket[1]: the epoch of the previous solve.  This solve's flags
+  // carry epoch = ticket[1] + 1; the CTA that takes the last exit ticket (every other CTA has
+  // taken its own by then, after reading ticket[1]) stores the epoch and rearms the counter, so
+  // a solve needs no host-side reset and replays unchanged from a captured graph.
+  const int epoch = __ldcg(&ticket[1]) + 1;
   for (;;) {
     // every thread has read the previous ticket: the unit below passes at least one barrier
     if (threadIdx.x == 0) sblk = atomicAdd(ticket, 1);
     __syncthreads();
     const int unit = sblk;
-    if (unit >= 2 * nb) break;                        // uniform over the block
+    if (unit >= 2 * nb) {                              // uniform over the block
+      if (threadIdx.x == 0 && unit == 2 * nb + (int)gridDim.x - 1) {
+        if (epoch >= (1 << 30)) {   // wrap: flags back to 0, the next solve uses epoch 1
+          for (int q = 0; q < 2 * nb; ++q) flags[q] = 0;
+          ticket[1] = 0;
+        } else {
+          ticket[1] = epoch;
+        }
+        ticket[0] = 0;
+      }
+      break;
+    }
     const int pos = unit >> 1, h = unit & 1;
     const int b = adj ? pos : (nb - 1 - pos);
     const int64_t r0 = (int64_t)b * TILE + h * 32;   // first row of this half

@@ -69,7 +69,6 @@ struct rls_ctx {
   int* ticket = nullptr;    // 1
   int trsm_ctas = 0;        // CTAs of a triangular solve (0: one per half block row)
   int trsm_sleep_cap = 32;  // longest back-off between flag polls of the triangular solve, ns
-  int epoch = 0;
   int* trmm_uO[2] = {nullptr, nullptr};
   int* trmm_us[2] = {nullptr, nullptr};
   int* trmm_Ofirst[2] = {nullptr, nullptr};
@@ -118,6 +117,15 @@ struct rls_ctx {
   double* sig_rec = nullptr;  // pr_max
   // LOBPCG keep
   cplx *S = nullptr, *CS = nullptr;   // n_pad × 3r
+  // lobpcg_invtri's steady iteration (the previous iteration's orthogonalisation and solve,
+  // then this one's Rayleigh–Ritz and residual) captured once per space as a CUDA graph
+  struct {
+    cudaGraphExec_t ex = nullptr;
+    const void* key = nullptr;   // the S array it was captured on (reallocated with the space)
+    int r = 0;
+    int64_t launches = 0;
+  } lob_graph;
+  bool lob_graphs = true;          // rls_ctx_set_graphs
   cplx *Gk = nullptr, *Rk = nullptr;  // 3r × 3r
   double *sig = nullptr, *lam = nullptr;
 
@@ -690,12 +698,6 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
     set_err(ctx, "trsm: output must not alias the right-hand side, and ld must be n_pad");
     return RLS_ERR_ARG;
   }
-  ctx->epoch += 1;
-  if (ctx->epoch > (1 << 30)) {
-    ctx->epoch = 1;
-    CK(cudaMemsetAsync(ctx->flags, 0, sizeof(int) * 2 * ctx->nb, ctx->stream));
-  }
-  CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(int), ctx->stream));
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, KP_TRSM, &e0);
   const size_t smem = trsm_half_smem_bytes(k);
@@ -705,7 +707,7 @@ int trsm(rls_ctx* ctx, cplx z, int adj, const cplx* B, cplx* X, int64_t ld, int 
   case K:                                                                                                        \
     k_trsm_half<K><<<ctas, 256, smem, ctx->stream>>>(ctx->nb, ctx->tile_bw, ctx->G, ctx->Dinv, B, X, ctx->trsm_u, \
                                                      ld, adj,                                                    \
-                                                     ctx->ticket, ctx->flags, ctx->epoch, ctx->derr,            \
+                                                     ctx->ticket, ctx->flags, ctx->derr,                        \
                                                      ctx->trsm_sleep_cap);                                       \
     break;
   switch (k) {
@@ -760,7 +762,16 @@ int trmm(rls_ctx* ctx, int adj, const cplx* X, cplx* Y, int64_t ld, int k) {
 // Workspace set-up
 // ---------------------------------------------------------------------------------
 
+// The captured LOBPCG iteration addresses the space, the operator's arrays and the solve's
+// settings: every change of those drops it.
+void drop_lob_graph(rls_ctx* ctx) {
+  if (ctx->lob_graph.ex) cudaGraphExecDestroy(ctx->lob_graph.ex);
+  ctx->lob_graph.ex = nullptr;
+  ctx->lob_graph.key = nullptr;
+}
+
 void release_space(rls_ctx* ctx) {
+  drop_lob_graph(ctx);
   cplx** bufs[] = {&ctx->V, &ctx->J1, &ctx->J2, &ctx->J5, &ctx->shift_tmp, &ctx->L, &ctx->H1, &ctx->H2, &ctx->Hs,
                    &ctx->Ulist, &ctx->heev.A, &ctx->Gheev, &ctx->CzX, &ctx->Gtot, &ctx->S, &ctx->CS, &ctx->Gk,
                    &ctx->Rk, &ctx->tall_tmp, &ctx->gram_part, &ctx->tsqr_stack[0], &ctx->tsqr_stack[1],
@@ -889,6 +900,7 @@ int lobpcg_invtri(rls_ctx* ctx, cplx z, int r, int64_t maxit, double tol, bool s
                                                                     ctx->lam, ctx->Gk, 3 * r, nullptr, nullptr);
     return check_launch(ctx, "k_svd_rr");
   };
+  double dummy_w0 = 0.0;
   auto residual = [&](cplx* Wd, double* w0) -> int {
     RET(trsm(ctx, z, adjCt, CX, Wd, np, r));
     const int threads = 256;
@@ -910,18 +922,57 @@ int lobpcg_invtri(rls_ctx* ctx, cplx z, int r, int64_t maxit, double tol, bool s
   RET(residual(P, nullptr));
   RET(orth_twice(ctx, np, X, np, r, P, np, r));
   RET(trsm(ctx, z, adjC, P, CP, np, r));
+  // the previous iteration's tail (orthogonalise W against [X P], CW = C·W) and this
+  // iteration's head (Rayleigh–Ritz on [X P W], basis update, residual)
+  auto tail = [&]() -> int {
+    RET(orth_twice(ctx, np, S, np, 2 * r, W, np, r));
+    return trsm(ctx, z, adjC, W, CW, np, r);
+  };
+  auto head = [&](int nS) -> int {
+    RET(svd_rr(CS, nS));
+    RET(gemm_rows(ctx, np, one_src(S), np, nS, ctx->Gk, 3 * r, 2 * r, S, np));
+    RET(gemm_rows(ctx, np, one_src(CS), np, nS, ctx->Gk, 3 * r, 2 * r, CS, np));
+    return residual(W, &dummy_w0);
+  };
+  // From the second iteration on, tail + head is one fixed launch sequence on fixed buffers
+  // (the shift enters through the scaled factor, rebuilt in place by the first solve of a
+  // refine), replayed from a graph captured once per space.  Per-kernel profiling keeps the
+  // direct launches.
+  const bool use_graph = ctx->lob_graphs && !ctx->profile;
+  if (use_graph && (ctx->lob_graph.key != (const void*)S || ctx->lob_graph.r != r)) {
+    if (ctx->lob_graph.ex) cudaGraphExecDestroy(ctx->lob_graph.ex);
+    ctx->lob_graph.ex = nullptr;
+  }
   for (int64_t i = 1; i <= maxit; ++i) {
     if (i == 1) {
-      RET(svd_rr(CS, 2 * r));
-      RET(gemm_rows(ctx, np, one_src(S), np, 2 * r, ctx->Gk, 3 * r, 2 * r, S, np));
-      RET(gemm_rows(ctx, np, one_src(CS), np, 2 * r, ctx->Gk, 3 * r, 2 * r, CS, np));
+      RET(head(2 * r));
+    } else if (use_graph) {
+      if (!ctx->lob_graph.ex) {
+        cudaGraph_t g = nullptr;
+        const int64_t l0 = ctx->launches;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int st = tail();
+        if (st == RLS_OK) st = head(3 * r);
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+        if (st != RLS_OK) {
+          if (g) cudaGraphDestroy(g);
+          return st;
+        }
+        CK(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&ctx->lob_graph.ex, g, 0);
+        cudaGraphDestroy(g);
+        CK(ie);
+        ctx->lob_graph.key = S;
+        ctx->lob_graph.r = r;
+        ctx->lob_graph.launches = ctx->launches - l0;
+        ctx->launches = l0;
+      }
+      CK(cudaGraphLaunch(ctx->lob_graph.ex, ctx->stream));
+      ctx->launches += ctx->lob_graph.launches;
     } else {
-      RET(svd_rr(CS, 3 * r));
-      RET(gemm_rows(ctx, np, one_src(S), np, 3 * r, ctx->Gk, 3 * r, 2 * r, S, np));
-      RET(gemm_rows(ctx, np, one_src(CS), np, 3 * r, ctx->Gk, 3 * r, 2 * r, CS, np));
+      RET(tail());
+      RET(head(3 * r));
     }
-    double w0 = 0.0;
-    RET(residual(W, &w0));
     double hs[2];
     double s0;
     RET(d2h2(ctx, hs, ctx->dscal, 1, &s0, ctx->sig, 1));
@@ -932,8 +983,6 @@ int lobpcg_invtri(rls_ctx* ctx, cplx z, int r, int64_t maxit, double tol, bool s
       res->it = i;
       return RLS_OK;
     }
-    RET(orth_twice(ctx, np, S, np, 2 * r, W, np, r));
-    RET(trsm(ctx, z, adjC, W, CW, np, r));
   }
   double s0;
   RET(d2h(ctx, &s0, ctx->sig, 1));
@@ -1466,6 +1515,9 @@ extern "C" void rls_ctx_destroy(rls_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_lob_graph(ctx);
+  if (ctx->band.graph) cudaGraphExecDestroy(ctx->band.graph);
+  ctx->band.graph = nullptr;
   for (auto& b : ctx->owned) cudaFree(b.p);
   ctx->owned.clear();
   prec_state_delete(ctx->prec);
@@ -1500,6 +1552,7 @@ int operator_drop(rls_ctx* ctx) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   // an old operator is freed with its last user
+  drop_lob_graph(ctx);
   ctx->T_buf.reset();
   ctx->T = nullptr;
   for (void* q : {(void*)ctx->Dinv, (void*)ctx->G, (void*)ctx->trsm_u, (void*)ctx->grad_ws,
@@ -1555,9 +1608,8 @@ int operator_setup(rls_ctx* ctx, int64_t n, const cplx* tiles, std::shared_ptr<c
   RET(dalloc_t(ctx, &ctx->G, elems));
   RET(dalloc_t(ctx, &ctx->trsm_u, (size_t)ctx->n_pad * 8));
   RET(dalloc_t(ctx, &ctx->flags, (size_t)2 * nb));
-  RET(dalloc_t(ctx, &ctx->ticket, 1));
+  RET(dalloc_t(ctx, &ctx->ticket, 2));   // work counter, epoch of the last solve (k_trsm_half)
   ctx->z_dinv = cmk(NAN, NAN);
-  ctx->epoch = 0;
   // TRMM work units
   size_t maxunits = 0;
   for (int adj = 0; adj < 2; ++adj) {
@@ -1613,12 +1665,22 @@ extern "C" int rls_set_schur(rls_ctx* ctx, int64_t n, const rls_c64* T, int64_t 
   return operator_setup(ctx, n, h.data(), nullptr);
 }
 
+extern "C" int rls_ctx_set_graphs(rls_ctx* ctx, int on) {
+  if (!ctx) return RLS_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  drop_lob_graph(ctx);
+  ctx->lob_graphs = on != 0;
+  return RLS_OK;
+}
+
 extern "C" int rls_set_trsm_backoff(rls_ctx* ctx, int max_ns) {
   if (!ctx) return RLS_ERR_ARG;
   if (max_ns < 32 || max_ns > 1 << 20) {
     set_err(ctx, "rls_set_trsm_backoff: %d ns (32 .. 1048576)", max_ns);
     return RLS_ERR_ARG;
   }
+  CK(cudaStreamSynchronize(ctx->stream));
+  drop_lob_graph(ctx);   // the cap is a kernel argument of the captured solves
   ctx->trsm_sleep_cap = max_ns;
   return RLS_OK;
 }
@@ -1629,6 +1691,8 @@ extern "C" int rls_set_trsm_ctas(rls_ctx* ctx, int ctas) {
     set_err(ctx, "rls_set_trsm_ctas: %d CTAs", ctas);
     return RLS_ERR_ARG;
   }
+  CK(cudaStreamSynchronize(ctx->stream));
+  drop_lob_graph(ctx);   // the grid size is baked into the captured solves
   ctx->trsm_ctas = ctas;
   return RLS_OK;
 }

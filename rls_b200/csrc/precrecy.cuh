@@ -903,6 +903,7 @@ extern "C" int rls_psprecrecy_range(rls_ctx* ctx, int64_t n, const int64_t* colp
     if (!ctx->T) {
       ctx->n = n;
       ctx->n_pad = (n + 63) / 64 * 64;
+      drop_lob_graph(ctx);
       dfree(ctx, ctx->colpart);     // per-CTA partial sums of the recycle step, sized by n_pad
       ctx->colpart = nullptr;
       RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
@@ -1288,6 +1289,7 @@ extern "C" int rls_lobpcg_svd(rls_ctx* ctx, int op, rls_c64 z, int prec, const r
   if (sparse_op && !ctx->T && ctx->n != n) {
     ctx->n = n;
     ctx->n_pad = (n + 63) / 64 * 64;
+    drop_lob_graph(ctx);
     dfree(ctx, ctx->colpart);
     ctx->colpart = nullptr;
     RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));

@@ -444,7 +444,7 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   RET(dalloc_t(ctx, &ctx->Dinv, (size_t)nb * TILE * TILE));
   RET(dalloc_t(ctx, &ctx->trsm_u, (size_t)ctx->n_pad * 8));
   RET(dalloc_t(ctx, &ctx->flags, (size_t)2 * nb));
-  RET(dalloc_t(ctx, &ctx->ticket, 1));
+  RET(dalloc_t(ctx, &ctx->ticket, 2));   // work counter, epoch of the last solve (k_trsm_half)
   RET(dalloc_t(ctx, &ctx->colpart, (size_t)(ctx->n_pad / 32 + 64)));
   RET(dalloc_t(ctx, &B.AB, (size_t)n * (size_t)B.ldab));
   // 16-column panels are a candidate where the panel (and the update's copy of V) fit in
@@ -459,7 +459,6 @@ extern "C" int rls_set_sparse_tri(rls_ctx* ctx, int64_t n, const int64_t* colptr
   B.on = true;
   ctx->op_sparse = true;
   ctx->z_dinv = cmk(NAN, NAN);
-  ctx->epoch = 0;
   CK(cudaStreamSynchronize(ctx->stream));
   return RLS_OK;
 }

@@ -356,6 +356,10 @@ class Engine:
         """Longest back-off (ns) between the triangular solve's flag polls."""
         check(lib().rls_set_trsm_backoff(self._h, int(max_ns)), self._h)
 
+    def set_graphs(self, on: bool):
+        """CUDA-graph replay of the refine's steady LOBPCG iteration (default on)."""
+        check(lib().rls_ctx_set_graphs(self._h, int(bool(on))), self._h)
+
     def stream_ptr(self) -> int:
         return int(lib().rls_ctx_stream(self._h) or 0)
 
@@ -668,6 +672,10 @@ class Lanes:
     def set_trsm_backoff(self, max_ns: int):
         for e in self.engines:
             e.set_trsm_backoff(max_ns)
+
+    def set_graphs(self, on: bool):
+        for e in self.engines:
+            e.set_graphs(on)
 
     def set_profile(self, on: bool):
         for e in self.engines:

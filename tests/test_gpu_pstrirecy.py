@@ -201,3 +201,28 @@ def test_lanes_cover_grid_and_match_truth(sprand_case):
     assert stL.n_pts == int(np.sum(stL.refine_it > 0))
     for b in off[:-1]:
         assert stL.refine_it[b] > 0 and stL.p_count[b] == 0   # each lane starts from an empty space
+
+
+def test_graph_replay_equals_direct_launches(sprand_case):
+    """The refine's steady LOBPCG iteration replayed from its captured graph gives the direct
+    launches' results bit for bit (σ, iteration counts, space sizes), and a TRSM setting change
+    recaptures it."""
+    C, T, normC, grid = sprand_case
+    n = T.shape[0]
+    X0 = _x0(n, 6)
+    rec = R.recursion_grid(*grid)
+    ctl = R.PsTriRecyControl(normC=normC, tol=1e-4, p_min=1, p=20, recy_tau=1.6)
+    out = []
+    for graphs, ctas in ((False, 0), (True, 0), (True, 5)):
+        e = R.Engine(0)
+        try:
+            e.set_schur(T)
+            e.set_graphs(graphs)
+            e.set_trsm_ctas(ctas)
+            out.append(e.pstrirecy(rec, ctl, X0=X0))
+        finally:
+            e.close()
+    (s0, st0), (s1, st1), (s2, st2) = out
+    assert np.array_equal(s0, s1) and np.array_equal(s0, s2)
+    assert np.array_equal(st0.refine_it, st1.refine_it) and np.array_equal(st0.p_count, st1.p_count)
+    assert int(np.max(st0.refine_it)) >= 2      # some refine reached the replayed iterations
