@@ -3,19 +3,19 @@
 //   X = P · L⁻ᴴ · L⁻¹ · Pᴴ · B,  i.e. temp = B[p, :]; X = L \ temp; temp = Lᴴ \ X; X = temp[invp, :],
 // with L sparse lower triangular (the IC factor, CSC, as LowerTriangular(L) sees it).
 //
-// Schedule: block rows of 32 consecutive rows, one warp per block row and one lane per row,
-// taken by ticket in dependency order (ascending for L, descending for Lᴴ), so a block row
-// only waits on block rows whose warps started before it: every wait ends even when not
-// all warps are resident, and a block row starts as soon as the block rows it reads are
-// published (dataflow; the level-set parallelism of a level schedule without a barrier
-// per level).  The plan lists, per block row, the block rows it reads in the order they
-// finish, and per row where its terms from each of them end: the warp waits on each in
-// turn (one lane polls the block row's flag, alone on its 128-byte line, with a capped
-// exponential back-off), then every lane streams its terms from that block row four at a
-// time with independent loads.  The warp then solves the 32 × 32 diagonal block in 32
-// shuffle steps, multipliers in shared memory.  For the banded IC factors of psPrecRecy,
-// whose row i almost always reads row i − 1, the critical path is n/32 block hand-offs,
-// each carrying only the terms of the block row just finished.
+// Schedule: block rows of 32 consecutive rows, one CTA of eight warps per block row (lane =
+// row), taken by ticket in dependency order (ascending for L, descending for Lᴴ), so a block
+// row only waits on block rows whose CTAs started before it: every wait ends even when not all
+// CTAs are resident, and a block row starts as soon as the block rows it reads are published
+// (dataflow; the level-set parallelism of a level schedule without a barrier per level).  The
+// plan lists, per block row, the block rows it reads in the order they finish, and per row
+// where its terms from each of them end: the warps wait on each in turn (lane 0 of each warp
+// polls the block row's flag, alone on its 128-byte line, with a capped exponential back-off),
+// then stream strided shares of every row's terms from that block row four at a time with
+// independent loads.  Warp 0 then solves the 32 × 32 diagonal block in 32 shuffle steps,
+// multipliers in shared memory.  For the banded IC factors of psPrecRecy, whose row i almost
+// always reads row i − 1, the critical path is n/32 block hand-offs, each carrying only the
+// terms of the block row just finished.
 //
 // Flags carry an epoch (st.release / ld.acquire at gpu scope; the polling lane's acquire
 // reaches the other lanes through __syncwarp); every wait is bounded by RLS_SPIN_LIMIT
@@ -26,7 +26,6 @@
 
 constexpr int SPT_ROWS = 32;          // rows per block row (one warp)
 constexpr int SPT_FLAG_STRIDE = 32;   // ints between two block rows' flags (128 bytes)
-constexpr int SPT_WARPS = 2;          // warps per CTA
 
 // One triangular operator in block-row form (rows of L, or rows of Lᴴ).
 struct TriBlocks {
@@ -53,110 +52,6 @@ __device__ __forceinline__ void spt_st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// out[:, 0:K] = A⁻¹ · rhs[gather, 0:K]  (gather = nullptr: identity).  BACK: block rows and the
-// in-block sweep run from the last row to the first (the operator is upper triangular).
-// SPT_WARPS warps per CTA, any grid.  out must not alias rhs.  flags: one per block row,
-// SPT_FLAG_STRIDE ints apart.
-template <int K, bool BACK>
-__global__ void __launch_bounds__(32 * SPT_WARPS) k_sptrsv_blocks(TriBlocks A, const cplx* __restrict__ rhs,
-                                                                  int64_t ldr, const int64_t* __restrict__ gather,
-                                                                  cplx* out, int64_t ldo, int* ticket, int* flags,
-                                                                  int epoch, int* err) {
-  __shared__ cplx sm_m[SPT_WARPS][SPT_ROWS * SPT_ROWS];   // each lane's own row of multipliers
-  const int lane = threadIdx.x & 31;
-  cplx* mw = sm_m[threadIdx.x >> 5];
-  for (;;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(ticket, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= A.nblk) break;                           // uniform over the warp
-    const int64_t b = BACK ? (A.nblk - 1 - t) : t;
-    const int64_t i = b * SPT_ROWS + lane;
-    const bool live = i < A.n;
-    const cplx* mb = A.blk + b * (SPT_ROWS * SPT_ROWS);
-#pragma unroll 8
-    for (int s = 0; s < SPT_ROWS; ++s) mw[s * SPT_ROWS + lane] = mb[s * SPT_ROWS + lane];
-    cplx acc[K], r[K];
-    cplx d = czero();
-#pragma unroll
-    for (int c = 0; c < K; ++c) { acc[c] = czero(); r[c] = czero(); }
-    int64_t e = 0;
-    if (live) {
-      d = A.dinv[i];
-      const int64_t src = gather ? gather[i] : i;
-#pragma unroll
-      for (int c = 0; c < K; ++c) r[c] = rhs[(int64_t)c * ldr + src];
-      e = A.rowptr[i];
-    }
-    const int64_t k1 = A.depptr[b + 1];
-    for (int64_t k = A.depptr[b]; k < k1; ++k) {
-      if (lane == 0) {
-        const int* f = &flags[(int64_t)A.deps[k] * SPT_FLAG_STRIDE];
-        int spins = 0;
-        unsigned ns = 32;
-        while (spt_ld_acquire(f) != epoch) {
-          if (++spins > RLS_SPIN_LIMIT) { atomicOr(err, DEVERR_SPIN_TIMEOUT); break; }
-          if (spins > 16) {
-            __nanosleep(ns);
-            if (ns < 256) ns <<= 1;
-          }
-        }
-      }
-      __syncwarp();
-      const int64_t eend = live ? A.segend[k * SPT_ROWS + lane] : 0;
-      for (; e + 4 <= eend; e += 4) {
-        int64_t j[4];
-        cplx v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          j[u] = A.col[e + u];
-          v[u] = A.val[e + u];
-        }
-        cplx xv[4][K];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int c = 0; c < K; ++c) xv[u][c] = __ldcg(&out[(int64_t)c * ldo + j[u]]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int c = 0; c < K; ++c) acc[c] = cfma(v[u], xv[u][c], acc[c]);
-      }
-      for (; e < eend; ++e) {
-        const int64_t j = A.col[e];
-        const cplx v = A.val[e];
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[c] = cfma(v, __ldcg(&out[(int64_t)c * ldo + j]), acc[c]);
-      }
-    }
-    // in-block sweep: at step s, lane s's row is final; every row subtracts its multiple of it
-    cplx x[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) x[c] = czero();
-#pragma unroll 4
-    for (int q = 0; q < SPT_ROWS; ++q) {
-      const int s = BACK ? (SPT_ROWS - 1 - q) : q;
-      const cplx ms = mw[s * SPT_ROWS + lane];
-#pragma unroll
-      for (int c = 0; c < K; ++c) {
-        const cplx mine = cmul(csub(r[c], acc[c]), d);
-        cplx xs;
-        xs.x = __shfl_sync(0xffffffffu, mine.x, s);
-        xs.y = __shfl_sync(0xffffffffu, mine.y, s);
-        if (lane == s) x[c] = xs;
-        acc[c] = cfma(ms, xs, acc[c]);
-      }
-    }
-    if (live) {
-#pragma unroll
-      for (int c = 0; c < K; ++c) out[(int64_t)c * ldo + i] = x[c];
-    }
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) spt_st_release(&flags[b * SPT_FLAG_STRIDE], epoch);
-  }
-}
-
 // X[i, 0:K] = W[src[i], 0:K] (W column-major with ld n): the final X = temp[invp, :].
 template <int K>
 __global__ void __launch_bounds__(256) k_gather_rows(int64_t n, const int64_t* __restrict__ src,
@@ -169,13 +64,16 @@ __global__ void __launch_bounds__(256) k_gather_rows(int64_t n, const int64_t* _
   for (int c = 0; c < K; ++c) X[(int64_t)c * ldx + i] = W[(int64_t)c * ldw + s];
 }
 
-// The same solve with a CTA of SPW_WARPS warps per block row: every warp takes a strided share
+// out[:, 0:K] = A⁻¹ · rhs[gather, 0:K]  (gather = nullptr: identity).  BACK: block rows and the
+// in-block sweep run from the last row to the first (the operator is upper triangular).  out
+// must not alias rhs; flags: one per block row, SPT_FLAG_STRIDE ints apart; any grid.
+// A CTA of SPW_WARPS warps per block row: every warp takes a strided share
 // (offset w, stride SPW_WARPS) of each row's terms from each dependency, waiting for that
 // dependency's flag first, so a block row's terms from block rows finished long ago stream
 // while the block row finished last is still being solved; after its flag only about
 // (terms from it) / SPW_WARPS loads per lane remain on the critical path.  The warps' partial
 // sums meet in shared memory in a fixed order (deterministic), and warp 0 does the in-block
-// sweep and publishes the block row.  Same plan, flags and ticket order as k_sptrsv_blocks.
+// sweep and publishes the block row.
 constexpr int SPW_WARPS = 8;
 
 template <int K, bool BACK>
