@@ -497,7 +497,8 @@ def run_ours(args):
         ms = max(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
         timed = np.concatenate([np.arange(o + args.warmup * s, o + need) for o in offs[:-1]])
         res = {"ms": max_over_ranks(ms, world, "cuda"), "launches": int(l1 - l0), "sig": sig, "timed": timed,
-               "refines": int(np.sum(st.refine_it[timed] > 0)), "clk": clk, "offs": offs}
+               "refines": int(np.sum(st.refine_it[timed] > 0)), "clk": clk, "offs": offs,
+               "refine_it_hist": np.bincount(st.refine_it[timed][st.refine_it[timed] > 0]).tolist()}
         if profile:
             res["prof"] = {k: ls.profile(k) for k in range(4)}
             res["waits"] = ls.profile(4)
@@ -572,6 +573,7 @@ def run_ours(args):
     out["config"]["parallelism"] = (f"grid columns: {world} rank(s) x {lanes} concurrent lane(s) per GPU "
                                     "(independent traversals from column starts)")
     out["config"]["refine_fraction_timed"] = refines / (lanes * args.steps * s)
+    out["config"]["refine_iterations_hist"] = main["refine_it_hist"]   # refines by LOBPCG iteration count
     out["preprocess_s"] = pre_s
     out["gpu_launches"] = main["launches"]
     out["profiled_run"] = {"value": world * lanes * args.steps * s / (profd["ms"] / 1e3), "unit": "pts/s",
