@@ -1,4 +1,5 @@
-"""psTriRecy over several GPUs: one rank per GPU, each on a column-aligned share of the grid.
+"""psTriRecy and psPrecRecy over several GPUs: one rank per GPU, each on a column-aligned share
+of the grid.
 
 No reference counterpart (the reference walks the whole traversal in one process).  The
 zigzag traversal (recuGrid.jl:157-176) is cut into `world` near-equal contiguous runs of whole
@@ -92,4 +93,50 @@ def psTriRecy_ranks(C_, rec: Recursion, control=None, X0=None, group=None, lanes
         scal = t.cpu().numpy()
     st.n_it, st.n_pts = int(scal[0]), int(scal[1])
     st.preprocess_time_ns = st_l.preprocess_time_ns
+    return sigma, st
+
+
+_PREC_ARRAYS = ("p_count", "pred_p_count", "r_recy", "main_M_vec_apps", "main_M_vec_apps_no_recycle",
+                "main_L_vec_apps", "pred_M_vec_apps", "pred_L_vec_apps", "main_refine_it", "pred_refine_it")
+_PREC_SCALARS = ("main_recycle_time_ns", "main_refine_time_ns", "main_update_time_ns", "pred_recycle_time_ns",
+                 "pred_refine_time_ns", "pred_update_time_ns", "precond_time_ns", "n_it", "n_pred_it", "n_pts",
+                 "n_pred_pts", "n_precond_rebuild_pts")
+
+
+def psPrecRecy_ranks(C_, rec: Recursion, control=None, group=None, lanes: int = 1, device: int = None, solve=None,
+                     **kw):
+    """psPrecRecy on this rank's column-aligned share of rec.Z (its own preconditioner, built at
+    the share's first point, and its own recycled spaces), then the gather of σ and the per-point
+    statistics as psTriRecy_ranks gathers them.  The point lists (pts, pred_pts,
+    precond_rebuild_pts) stay per rank; the scalar counters and times are summed over ranks.
+    `solve(C_, sub_rec, control)` replaces the per-rank solver (default: rls_b200.psPrecRecy on
+    `device` with `lanes` lanes and the keyword arguments kw)."""
+    import torch.distributed as dist
+    from .solvers import PsPrecRecyControl, PsPrecRecyStats, psPrecRecy
+    control = control or PsPrecRecyControl()
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    offs = column_shares(len(rec.Z), rec.k, world)
+    sub = Recursion(rec.x_st, rec.x_ed, rec.y_st, rec.y_ed, rec.n_x, rec.n_y, rec.k)
+    sub.Z = np.ascontiguousarray(rec.Z[offs[rank]:offs[rank + 1]])
+    if solve is None:
+        dev = rank if device is None else device
+        sig_l, st_l = psPrecRecy(C_, sub, control, verbose=0, device=dev, lanes=lanes, **kw)
+    else:
+        sig_l, st_l = solve(C_, sub, control)
+    sigma, arrays = gather_shares(sig_l, {nm: getattr(st_l, nm) for nm in _PREC_ARRAYS}, offs, group)
+    st = PsPrecRecyStats(len(rec.Z))
+    for nm in _PREC_ARRAYS:
+        setattr(st, nm, arrays[nm])
+    for nm in ("pts", "pred_pts", "precond_rebuild_pts"):
+        setattr(st, nm, getattr(st_l, nm))
+    scal = np.array([getattr(st_l, nm) for nm in _PREC_SCALARS], dtype=np.float64)
+    if world > 1:
+        import torch
+        dev_t = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+        t = torch.as_tensor(scal, device=dev_t)
+        dist.all_reduce(t, group=group)
+        scal = t.cpu().numpy()
+    for nm, v in zip(_PREC_SCALARS, scal):
+        setattr(st, nm, int(v))
     return sigma, st

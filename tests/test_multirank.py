@@ -128,3 +128,53 @@ def test_library_gather_of_rank_shares(tmp_path):
         assert np.array_equal(d["p_count"], local)
         assert int(d["n_pts"]) == len(rec.Z)
     assert offs[1] % rec.k == 0 and 0 < offs[1] < len(rec.Z)
+
+
+def _fake_prec_solve(C_, sub, control):
+    """Stands in for the per-rank psPrecRecy: σ = |z| + 2 and per-point counters from z."""
+    from rls_b200.solvers import PsPrecRecyStats
+    st = PsPrecRecyStats(len(sub.Z))
+    st.main_refine_it[:] = (np.round(sub.Z.imag * 1000).astype(np.int64) % 5)
+    st.p_count[:] = np.arange(len(sub.Z))
+    st.n_pts = int(np.sum(st.main_refine_it > 0))
+    st.n_precond_rebuild_pts = 1
+    return np.abs(sub.Z) + 2.0, st
+
+
+def _prec_ranks_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from datetime import timedelta
+    from rls_b200.grid import recursion_grid
+    from rls_b200.distributed import psPrecRecy_ranks
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        rec = recursion_grid(-1.6, 0.8, -1.55, 1.55, 24, 12, 4)
+        sig, st = psPrecRecy_ranks(None, rec, solve=_fake_prec_solve)
+        np.savez(os.path.join(out_dir, f"prec{rank}.npz"), sig=sig, it=st.main_refine_it, p_count=st.p_count,
+                 n_pts=st.n_pts, builds=st.n_precond_rebuild_pts)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_library_gather_of_psprecrecy_shares(tmp_path):
+    """rls_b200.distributed.psPrecRecy_ranks on two gloo ranks: σ and the per-point counters of
+    both shares on every rank in rec.Z order; scalar counters summed (one preconditioner build
+    per rank)."""
+    import torch.multiprocessing as mp
+    from rls_b200.grid import recursion_grid
+    from rls_b200.distributed import column_shares
+    world = 2
+    mp.start_processes(_prec_ranks_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    rec = recursion_grid(-1.6, 0.8, -1.55, 1.55, 24, 12, 4)
+    offs = column_shares(len(rec.Z), rec.k, world)
+    it_ref = np.round(rec.Z.imag * 1000).astype(np.int64) % 5
+    for r in range(world):
+        d = np.load(tmp_path / f"prec{r}.npz")
+        assert np.array_equal(d["sig"], np.abs(rec.Z) + 2.0)
+        assert np.array_equal(d["it"], it_ref)
+        local = np.concatenate([np.arange(offs[q + 1] - offs[q]) for q in range(world)])
+        assert np.array_equal(d["p_count"], local)
+        assert int(d["n_pts"]) == int(np.sum(it_ref > 0))
+        assert int(d["builds"]) == world
