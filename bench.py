@@ -95,6 +95,7 @@ def parse():
     ap.add_argument("--lanes", type=int, default=20, help="concurrent grid lanes per GPU")
     ap.add_argument("--trsm-backoff", type=int, default=32, help="longest ns between TRSM flag polls")
     ap.add_argument("--no-graphs", action="store_true", help="refine iterations as direct launches")
+    ap.add_argument("--batch", type=int, default=0, help="largest speculative recycle batch (0: the library's 16)")
     ap.add_argument("--trsm-ctas", type=int, default=0,
                     help="CTAs per triangular solve in every lane (0: one per half block row)")
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
@@ -458,6 +459,8 @@ def run_ours(args):
         ls.set_trsm_backoff(args.trsm_backoff)
         if args.no_graphs:
             ls.set_graphs(False)
+        if args.batch:
+            ls.set_batch(args.batch)
         offs = ls.offsets(sub)
         if need > int(np.min(np.diff(offs))):
             raise SystemExit(f"--chunk × (warmup + steps) = {need} exceeds a lane of {int(np.min(np.diff(offs)))} points")
