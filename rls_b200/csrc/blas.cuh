@@ -497,7 +497,7 @@ __device__ __forceinline__ void half_product(const cplx* sA, const cplx* sX, cpl
 }
 
 template <int K>
-__global__ void __launch_bounds__(256) k_trsm_half(int nb, int bw, const cplx* __restrict__ G,
+__global__ void __launch_bounds__(256, 2) k_trsm_half(int nb, int bw, const cplx* __restrict__ G,
                                                    const cplx* __restrict__ Dinv,
                                                    const cplx* __restrict__ B, cplx* __restrict__ X, cplx* U,
                                                    int64_t ldx, int adj, int* __restrict__ ticket, int* flags,
