@@ -205,51 +205,62 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
       d[k] = A[k * lda + k].x;
     }
   };
-  __shared__ cplx yvp[16];
+  // y = τ·A·v in two barriers without a reduction per row: the m = n − m0 trailing rows
+  // form R = ⌈m/32⌉ groups of 32 (a lane per row) and the trailing columns nch = nw/R
+  // chunks (one when R > nw/2).  B: warp (g, c) sums its chunk for its rows, into ypart
+  // (nch > 1, then R·nch ≤ nw) or straight into w (nch = 1, warps loop over the groups).
+  // C: warp g < R adds the partials of its rows (warps loop over the groups beyond nw),
+  // stores y and one warp sum of its share of yᴴv.
+  __shared__ cplx ypart[HEEV_THREADS];
+  __shared__ cplx yvp[HEEV_THREADS / 32];
   if (n > 1 && warp == 0) make_reflector(0);
   __syncthreads();
   for (int k = 0; k < n - 1; ++k) {
-    const int m0 = k + 1;
+    const int m0 = k + 1, m = n - m0;
     const cplx t = tau[k];
     const cplx* vk = (k & 1) ? v1 : v;
     const bool active = (t.x != 0.0 || t.y != 0.0);
-    if (active) {   // B: rows m0 + warp + 16t, two at a time
-      cplx yvw = czero();
-      for (int i = m0 + warp; i < n; i += 32) {
-        const int i2 = i + 16;
-        const bool two = i2 < n;
-        cplx s0 = czero(), s1 = czero();
-        for (int j = m0 + lane; j < n; j += 32) {
-          const cplx vj = vk[j];
-          s0 = cfmac(A[i * lda + j], vj, s0);            // conj(A(j,i)) v_j = A(i,j) v_j
-          if (two) s1 = cfmac(A[i2 * lda + j], vj, s1);
+    const int R = (m + 31) >> 5, nch = max(1, nw / R), cl = (m + nch - 1) / nch;
+    if (active) {   // B: partial sums of (A v)_i over one column chunk
+      for (int u = warp; u < R * nch; u += nw) {
+        const int g = u % R, c = u / R;
+        const int i = m0 + g * 32 + lane;
+        cplx s = czero();
+        if (i < n) {
+          const int j1 = min(n, m0 + (c + 1) * cl);
+          for (int j = m0 + c * cl; j < j1; ++j) s = cfma(A[j * lda + i], vk[j], s);   // A(i,j) v_j
         }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        if (lane == 0) {
-          const cplx y0 = cmul(t, s0);
-          w[i] = y0;
-          yvw = cfmac(y0, vk[i], yvw);                   // Σ conj(y_i) v_i
-          if (two) {
-            const cplx y1 = cmul(t, s1);
-            w[i2] = y1;
-            yvw = cfmac(y1, vk[i2], yvw);
-          }
+        if (nch > 1) ypart[(c * R + g) * 32 + lane] = s;
+        else if (i < n) w[i] = s;
+      }
+    }
+    __syncthreads();
+    if (active && warp < R) {   // C: y_i = τ (A v)_i, and Σ conj(y_i) v_i over this warp's rows
+      cplx yvw = czero();
+      for (int g = warp; g < R; g += nw) {
+        const int i = m0 + g * 32 + lane;
+        cplx s;
+        if (nch > 1) {
+          s = ypart[g * 32 + lane];
+          for (int c = 1; c < nch; ++c) s = cadd(s, ypart[(c * R + g) * 32 + lane]);
+        } else {
+          s = (i < n) ? w[i] : czero();
+        }
+        if (i < n) {
+          const cplx y = cmul(t, s);
+          w[i] = y;
+          yvw = cfmac(y, vk[i], yvw);
         }
       }
+      yvw = warp_sum(yvw);
       if (lane == 0) yvp[warp] = yvw;
     }
     __syncthreads();
     cplx a2 = czero();
-    if (active) {   // α₂ from the 16 warp partials: a fixed butterfly, lane 0's value broadcast
-      cplx yv = yvp[lane & 15];
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        yv.x += __shfl_xor_sync(0xffffffffu, yv.x, o);
-        yv.y += __shfl_xor_sync(0xffffffffu, yv.y, o);
-      }
-      yv.x = __shfl_sync(0xffffffffu, yv.x, 0);
-      yv.y = __shfl_sync(0xffffffffu, yv.y, 0);
+    if (active) {   // α₂ = −½ τ yᴴv from the per-warp sums, in warp order
+      const int ns = min(R, nw);
+      cplx yv = yvp[0];
+      for (int g = 1; g < ns; ++g) yv = cadd(yv, yvp[g]);
       a2 = cscale(cmul(t, yv), -0.5);
     }
     if (warp == 0) {   // D, column m0 (all trailing rows), then the next reflector
