@@ -129,16 +129,15 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   const int b = blockIdx.x;
   const int n = pr;
   const int nlu = plan.nlu;
-  // shared layout: [A (n × lda cplx)] v v1 w tau (n cplx) d e e2 lam (n doubles)
+  // shared layout: [A (n × lda cplx)] v v1 tau (n cplx) yp (4n cplx) d e e2 lam (n doubles)
   // LU (nlu·6n doubles) S (gs_cap·n cplx)
   cplx* base = reinterpret_cast<cplx*>(dsm);
   const int lda = plan.lda > 0 ? plan.lda : n;
   cplx* A = plan.lda > 0 ? base : work.A + (int64_t)b * prmax * prmax;
   cplx* v = base + (plan.lda > 0 ? (size_t)n * lda : 0);
   cplx* v1 = v + n;
-  cplx* w = v1 + n;
-  cplx* tau = w + n;
-  double* d = reinterpret_cast<double*>(tau + n);
+  cplx* tau = v1 + n;
+  double* d = reinterpret_cast<double*>(tau + 5 * n);   // yp: tau + n .. tau + 5n
   double* e = d + n;
   double* e2 = e + n;
   double* lam = e2 + n;
@@ -165,13 +164,9 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
   __syncthreads();
 
   // 2. Householder tridiagonalisation: for column k reduce A[k+1:, k].  Both triangles of
-  //    the trailing block are kept, so row i of A is column i conjugated and y = τ·A·v is
-  //    a contiguous sweep per row.  Two barriers per column:
-  //      B  warp w forms y_i for the rows i ≡ w (mod 16) of the trailing block (lanes
-  //         over the columns, one warp sum per row) and its partial of yᴴv;
-  //      D  α₂ = −½ τ yᴴv; A −= v wᴴ + w vᴴ on the trailing block, w = y + α₂·v, columns
-  //         of warps 1..15; warp 0 updates column k+1 and forms the next reflector.
-  //    Reflectors alternate between two buffers.
+  //    the trailing block are kept, so every access to A reads a column with a lane per row
+  //    (conflict-free).  Two barriers per column (B and D below); reflectors alternate
+  //    between two buffers.
   auto make_reflector = [&](int k) {   // warp 0; column k (rows ≥ k+1) is final
     const int m0 = k + 1;
     cplx* vk = (k & 1) ? v1 : v;
@@ -205,91 +200,95 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
       d[k] = A[k * lda + k].x;
     }
   };
-  // y = τ·A·v in two barriers without a reduction per row: the m = n − m0 trailing rows
-  // form R = ⌈m/32⌉ groups of 32 (a lane per row) and the trailing columns nch = nw/R
-  // chunks (one when R > nw/2).  B: warp (g, c) sums its chunk for its rows, into ypart
-  // (nch > 1, then R·nch ≤ nw) or straight into w (nch = 1, warps loop over the groups).
-  // C: warp g < R adds the partials of its rows (warps loop over the groups beyond nw),
-  // stores y and one warp sum of its share of yᴴv.
-  __shared__ cplx ypart[HEEV_THREADS];
-  __shared__ cplx yvp[HEEV_THREADS / 32];
+  // B and D of column k (m0 = k + 1, trailing block rows and columns m0..n−1):
+  //   B  partial products P_c(i) = Σ_{j ≡ m0+c (mod 4)} A(i,j) v_j: warp w takes the row
+  //      groups g ≡ w (mod 4) (32 rows each, a lane per row) and column residue c = w/4, four
+  //      independent sums per thread, into yp[c·n + i]; each warp also forms its share of
+  //      Σ conj(P_c(i)) v_i (one warp sum per warp), so yᴴv = conj(τ)·Σ_w yvp[w] with y = τ Σ_c P_c.
+  //   D  α₂ = −½ τ yᴴv = −½|τ|² Σ_w yvp[w]; w_i = τ Σ_c P_c(i) + α₂ v_i is rebuilt from the
+  //      partials wherever it is needed; A −= v wᴴ + w vᴴ: columns m0+1.. by warps 1..15,
+  //      column m0 by warp 0, which then forms the next reflector.
+  constexpr int NWH = HEEV_THREADS / 32, RGS = 4, CCH = NWH / RGS;
+  static_assert(CCH == 4, "four column residues");
+  cplx* yp = tau + n;                 // CCH × n partial products
+  __shared__ cplx yvp[NWH];
   if (n > 1 && warp == 0) make_reflector(0);
   __syncthreads();
   for (int k = 0; k < n - 1; ++k) {
-    const int m0 = k + 1, m = n - m0;
+    const int m0 = k + 1;
     const cplx t = tau[k];
     const cplx* vk = (k & 1) ? v1 : v;
     const bool active = (t.x != 0.0 || t.y != 0.0);
-    const int R = (m + 31) >> 5, nch = max(1, nw / R), cl = (m + nch - 1) / nch;
-    if (active) {   // B: partial sums of (A v)_i over one column chunk
-      for (int u = warp; u < R * nch; u += nw) {
-        const int g = u % R, c = u / R;
+    if (active) {   // B
+      const int c = warp / RGS;
+      cplx yv = czero();
+      for (int g = warp % RGS; m0 + g * 32 < n; g += RGS) {
         const int i = m0 + g * 32 + lane;
-        cplx s = czero();
         if (i < n) {
-          const int j1 = min(n, m0 + (c + 1) * cl);
-          for (int j = m0 + c * cl; j < j1; ++j) s = cfma(A[j * lda + i], vk[j], s);   // A(i,j) v_j
-        }
-        if (nch > 1) ypart[(c * R + g) * 32 + lane] = s;
-        else if (i < n) w[i] = s;
-      }
-    }
-    __syncthreads();
-    if (active && warp < R) {   // C: y_i = τ (A v)_i, and Σ conj(y_i) v_i over this warp's rows
-      cplx yvw = czero();
-      for (int g = warp; g < R; g += nw) {
-        const int i = m0 + g * 32 + lane;
-        cplx s;
-        if (nch > 1) {
-          s = ypart[g * 32 + lane];
-          for (int c = 1; c < nch; ++c) s = cadd(s, ypart[(c * R + g) * 32 + lane]);
-        } else {
-          s = (i < n) ? w[i] : czero();
-        }
-        if (i < n) {
-          const cplx y = cmul(t, s);
-          w[i] = y;
-          yvw = cfmac(y, vk[i], yvw);
+          cplx s0 = czero(), s1 = czero(), s2 = czero(), s3 = czero();
+          int j = m0 + c;
+          for (; j + 3 * CCH < n; j += 4 * CCH) {
+            s0 = cfma(A[j * lda + i], vk[j], s0);                       // A(i,j) v_j
+            s1 = cfma(A[(j + CCH) * lda + i], vk[j + CCH], s1);
+            s2 = cfma(A[(j + 2 * CCH) * lda + i], vk[j + 2 * CCH], s2);
+            s3 = cfma(A[(j + 3 * CCH) * lda + i], vk[j + 3 * CCH], s3);
+          }
+          for (; j < n; j += CCH) s0 = cfma(A[j * lda + i], vk[j], s0);
+          const cplx s = cadd(cadd(s0, s1), cadd(s2, s3));
+          yp[c * n + i] = s;
+          yv = cfmac(s, vk[i], yv);                                     // conj(P_c(i)) v_i
         }
       }
-      yvw = warp_sum(yvw);
-      if (lane == 0) yvp[warp] = yvw;
+      yv = warp_sum(yv);
+      if (lane == 0) yvp[warp] = yv;
     }
     __syncthreads();
-    cplx a2 = czero();
-    if (active) {   // α₂ = −½ τ yᴴv from the per-warp sums, in warp order
-      const int ns = min(R, nw);
-      cplx yv = yvp[0];
-      for (int g = 1; g < ns; ++g) yv = cadd(yv, yvp[g]);
-      a2 = cscale(cmul(t, yv), -0.5);
-    }
-    if (warp == 0) {   // D, column m0 (all trailing rows), then the next reflector
-      if (active) {
-        const cplx vj = vk[m0], wj = cfma(a2, vj, w[m0]);
+    if (active) {   // D
+      cplx ys = yvp[0];
+#pragma unroll
+      for (int q = 1; q < NWH; ++q) ys = cadd(ys, yvp[q]);
+      const cplx a2 = cscale(ys, -0.5 * (t.x * t.x + t.y * t.y));
+      auto wrow = [&](int i) {
+        const cplx s = cadd(cadd(cadd(yp[i], yp[n + i]), yp[2 * n + i]), yp[3 * n + i]);
+        return cfma(a2, vk[i], cmul(t, s));
+      };
+      if (warp == 0) {   // column m0, all trailing rows
+        const cplx vj = vk[m0], wj = wrow(m0);
         for (int i = m0 + lane; i < n; i += 32) {
-          const cplx vi = vk[i], wi = cfma(a2, vi, w[i]);
+          const cplx vi = vk[i], wi = wrow(i);
           cplx aij = A[m0 * lda + i];
           aij = csub(aij, cmulc(wj, vi));    // v_i conj(w_j)
           aij = csub(aij, cmulc(vj, wi));    // w_i conj(v_j)
           A[m0 * lda + i] = aij;
         }
         __syncwarp();
-      }
-      if (k + 1 < n - 1) make_reflector(k + 1);
-    } else if (active) {   // D, columns m0+1 .. n-1 (all trailing rows)
-      for (int i0 = m0; i0 < n; i0 += 32) {
-        const int i = i0 + lane;
-        if (i >= n) continue;
-        const cplx vi = vk[i], wi = cfma(a2, vi, w[i]);
-        for (int j = m0 + warp; j < n; j += nw - 1) {
-          const cplx vj = vk[j], wj = cfma(a2, vj, w[j]);
-          cplx aij = A[j * lda + i];
-          aij = csub(aij, cmulc(wj, vi));
-          aij = csub(aij, cmulc(vj, wi));
-          A[j * lda + i] = aij;
+      } else {           // columns m0+warp, m0+warp+15, ..., rows in blocks of four groups
+        for (int g0 = 0; m0 + g0 * 32 < n; g0 += 4) {
+          cplx vi[4], wi[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = m0 + (g0 + q) * 32 + lane;
+            vi[q] = (i < n) ? vk[i] : czero();
+            wi[q] = (i < n) ? wrow(i) : czero();
+          }
+          for (int j = m0 + warp; j < n; j += NWH - 1) {
+            const cplx vj = vk[j], wj = wrow(j);
+            cplx a[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int i = m0 + (g0 + q) * 32 + lane;
+              a[q] = (i < n) ? A[j * lda + i] : czero();
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int i = m0 + (g0 + q) * 32 + lane;
+              if (i < n) A[j * lda + i] = csub(csub(a[q], cmulc(wj, vi[q])), cmulc(vj, wi[q]));
+            }
+          }
         }
       }
     }
+    if (warp == 0 && k + 1 < n - 1) make_reflector(k + 1);
     __syncthreads();
   }
   if (threadIdx.x == 0) d[n - 1] = A[(n - 1) * lda + (n - 1)].x;
@@ -491,7 +490,7 @@ __global__ void __launch_bounds__(HEEV_THREADS) k_heev_rr(int pr, int r, const c
 // as fit.
 inline HeevPlan heev_plan(int pr, size_t avail) {
   HeevPlan p{};
-  const size_t vec = (size_t)4 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
+  const size_t vec = (size_t)7 * pr * sizeof(cplx) + (size_t)4 * pr * sizeof(double);
   int lda = pr + ((4 - pr % 8) + 8) % 8;                    // ≡ 4 (mod 8)
   size_t need = vec + (size_t)pr * lda * sizeof(cplx);
   const size_t lu1 = (size_t)6 * pr * sizeof(double);
