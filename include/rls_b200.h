@@ -240,6 +240,23 @@ int rls_reorder_to_natural(const rls_grid* g, const rls_c64* Z, int64_t nZ,
 int rls_reorder_to_natural_grid(const rls_grid* g, const rls_c64* Z, int64_t nZ,
                                 const double* v, double* out);
 
+/* ---- MatrixMarket input (loaddata, src/utils/loadmtx.jl:1-28) -------------------------
+ * The reference reads `data/<name>.mtx` with MatrixMarket.jl's mmread and converts it to
+ * ComplexF64; these read a MatrixMarket file at `path` the same way (host only, no context).
+ * Symmetric, hermitian and skew-symmetric storage is expanded, coordinate duplicates add up,
+ * explicit zeros stay stored, pattern entries are 1.  A file that cannot be opened or parsed
+ * returns RLS_ERR_ARG with the file, line and reason in rls_last_error(NULL).
+ * rls_mtx_info: m × n, an upper bound of the stored entries after expansion (m·n for the
+ * array format) and dense = 1 for the array format.  Any output may be NULL. */
+int rls_mtx_info(const char* path, int64_t* m, int64_t* n, int64_t* nnz_max, int* dense);
+/* The coordinate format as CSC with 0- or 1-based indices (base): colptr has n + 1 entries,
+ * rowval and nzval room for cap entries (cap = nnz_max suffices); rows ascend within each
+ * column; *nnz gets the number of stored entries (RLS_ERR_DIM when it exceeds cap). */
+int rls_mtx_read_csc(const char* path, int base, int64_t cap, int64_t* colptr, int64_t* rowval,
+                     rls_c64* nzval, int64_t* nnz);
+/* The array format, column-major into A with leading dimension lda >= m. */
+int rls_mtx_read_dense(const char* path, rls_c64* A, int64_t lda);
+
 /* ---- operator upload ---------------------------------------------------------- */
 
 /* Uploads the upper-triangular complex Schur factor T of C (C = Q T Qᴴ), i.e.

@@ -21,6 +21,7 @@ from .solvers import (PsTriRecyControl, PsTriRecyStats, LobpcgSvdControl, Engine
 from ._lib import RLSError, ArgumentError, DimensionMismatch, SingularException
 from .operators import MulChainMat, NormalMat, IdentityMat, PermMat, InvMat, FilledMat, mul_coupled
 from .distributed import psTriRecy_ranks, psPrecRecy_ranks, column_shares
+from .mtx import loaddata, load_mtx, save_run
 
 __all__ = [
     "Recursion", "recursion_grid", "recursion_grid_zigzag", "recursion_grid_linear", "recursion_grid_spiral",
@@ -30,4 +31,5 @@ __all__ = [
     "psTriRecy", "ic_factor", "get_hsl_LLTP", "SparseLLTP_AD", "mul_coupled", "MulChainMat", "NormalMat", "IdentityMat", "PermMat", "InvMat",
     "FilledMat", "RLSError", "ArgumentError", "DimensionMismatch", "SingularException", "PsPrecRecyControl",
     "PsPrecRecyStats", "PrecRecyRun", "PrecRecyLanes", "psPrecRecy", "psTriRecy_ranks", "psPrecRecy_ranks", "column_shares",
+    "loaddata", "load_mtx", "save_run",
 ]

@@ -91,6 +91,9 @@ SIGNATURES = {
     "rls_natural_perm": (C.c_int, [C.POINTER(rls_grid), P, C.c_int64, P]),
     "rls_reorder_to_natural": (C.c_int, [C.POINTER(rls_grid), P, C.c_int64, P, P]),
     "rls_reorder_to_natural_grid": (C.c_int, [C.POINTER(rls_grid), P, C.c_int64, P, P]),
+    "rls_mtx_info": (C.c_int, [C.c_char_p, P, P, P, P]),
+    "rls_mtx_read_csc": (C.c_int, [C.c_char_p, C.c_int, C.c_int64, P, P, P, P]),
+    "rls_mtx_read_dense": (C.c_int, [C.c_char_p, P, C.c_int64]),
     "rls_set_schur": (C.c_int, [P, C.c_int64, P, C.c_int64]),
     "rls_set_schur_copy": (C.c_int, [P, P]),
     "rls_set_sparse_tri": (C.c_int, [P, C.c_int64, P, P, P, C.c_int, P]),

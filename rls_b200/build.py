@@ -2,8 +2,8 @@
 
     python -m rls_b200.build [--force]
 
-The grid code and the IC factorisation are compiled by g++ with -ffp-contract=off
-(bit-exact coordinates and factors);
+The grid code, the IC factorisation and the MatrixMarket reader are compiled by g++ with
+-ffp-contract=off (bit-exact coordinates and factors);
 the CUDA translation unit by nvcc for sm_100a only.
 """
 from __future__ import annotations
@@ -49,7 +49,8 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     grid_o = os.path.join(BUILD, "grid.o")
     eng_o = os.path.join(BUILD, "engine.o")
     ic_o = os.path.join(BUILD, "icfact.o")
-    for src, obj in (("grid.cpp", grid_o), ("icfact.cpp", ic_o)):
+    mtx_o = os.path.join(BUILD, "mtxio.o")
+    for src, obj in (("grid.cpp", grid_o), ("icfact.cpp", ic_o), ("mtxio.cpp", mtx_o)):
         _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-c",
               os.path.join(CSRC, src), "-o", obj])
     cmd = [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-c",
@@ -58,7 +59,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         cmd[1:1] = ["-Xptxas", "-v"]
     _run(cmd)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, ic_o, "-lcudart", "-lpthread"])
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, eng_o, grid_o, ic_o, mtx_o, "-lcudart", "-lpthread"])
     os.replace(tmp, LIB)
     return LIB
 
