@@ -33,6 +33,11 @@
 namespace {
 
 using cd = std::complex<double>;
+// a·b as Julia's `*` on Complex{Float64} forms it, (ac − bd) + i(ad + bc): the same bits as
+// std::complex's operator* whenever that is not NaN, without its Annex G recovery call.
+inline cd mulc(cd a, cd b) {
+  return cd(a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real());
+}
 
 constexpr double kSmall = 1e-20;
 constexpr double kLowAlpha = 1e-3;
@@ -102,7 +107,7 @@ Csc normal_lower(int64_t n, const Csc& C, cd z) {
         const cd b = cz.val[(size_t)qb];
         for (int64_t qa = h.ptr[(size_t)k]; qa < h.ptr[(size_t)k + 1]; ++qa) {
           const int64_t i = h.row[(size_t)qa];
-          const cd t2 = h.val[(size_t)qa] * b;
+          const cd t2 = mulc(h.val[(size_t)qa], b);
           if (seen[(size_t)i] != j) {
             seen[(size_t)i] = j;
             x[(size_t)i] = t2;
@@ -271,10 +276,10 @@ int64_t ic_attempt(int64_t n, const Csc& A, const std::vector<double>& scale, st
         nextl[(size_t)c] = headl[(size_t)r];
         headl[(size_t)r] = c;
       }
-      for (int64_t q = i0; q < i1; ++q) add(F.lr[(size_t)q], -(F.lv[(size_t)q] * ljc));
+      for (int64_t q = i0; q < i1; ++q) add(F.lr[(size_t)q], -mulc(F.lv[(size_t)q], ljc));
       for (int64_t q = posr[(size_t)c]; q < F.rp[(size_t)c + 1]; ++q) {
         const int64_t k = F.rr[(size_t)q];
-        if (k > j) add(k, -(F.rv[(size_t)q] * ljc));
+        if (k > j) add(k, -mulc(F.rv[(size_t)q], ljc));
       }
       c = cn;
     }
@@ -292,7 +297,7 @@ int64_t ic_attempt(int64_t n, const Csc& A, const std::vector<double>& scale, st
       }
       for (int64_t q = posl[(size_t)c]; q < F.lp[(size_t)c + 1]; ++q) {
         const int64_t k = F.lr[(size_t)q];
-        if (k > j) add(k, -(F.lv[(size_t)q] * rjc));
+        if (k > j) add(k, -mulc(F.lv[(size_t)q], rjc));
       }
       c = cn;
     }
