@@ -101,6 +101,9 @@ def parse():
     ap.add_argument("--ref-chunk", type=int, default=3, help="grid points per step of the CPU arm")
     ap.add_argument("--pp-chunk", type=int, default=100, help="grid points per step of the af23560 (psPrecRecy) leg")
     ap.add_argument("--pp-lanes", type=int, default=8, help="concurrent lanes of the af23560 (psPrecRecy) leg")
+    ap.add_argument("--mtx", default=None,
+                    help="af23560 workload: read C from this MatrixMarket file (e.g. the reference's "
+                         "data/af23560.mtx) instead of the synthetic af23560-shaped matrix")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--n", type=int, default=None, help="matrix order (default: the workload's)")
     ap.add_argument("--factor-only", type=int, default=0,
@@ -711,10 +714,21 @@ def af_controls(mod, normC):
         hsl_cntl_2=1e-6, gamma_tol=1e-3, lambda_n_tol=1e-3)
 
 
-def af_inputs(n):
+def af_inputs(n, mtx=None):
+    """C (the synthetic af23560-shaped matrix, or the MatrixMarket file `mtx` read as loaddata
+    reads it), the driver's main_normC and the column order."""
     from rls_b200.examples import af23560_shaped, AF23560_NORMC
     from scipy.sparse.csgraph import reverse_cuthill_mckee
-    C = af23560_shaped(n)
+    if mtx:
+        import scipy.sparse as sp
+        from rls_b200.mtx import load_mtx
+        C = load_mtx(mtx)
+        if not sp.issparse(C) or C.shape[0] != C.shape[1]:
+            raise SystemExit(f"--mtx {mtx}: psPrecRecy needs a square coordinate-format matrix")
+        C = C.tocsc()
+        C.sort_indices()
+    else:
+        C = af23560_shaped(n)
     # psPrecRecy orders by SPQR's column pivoting (qr(C).cpiv, psPrecRecy.jl:625), which needs
     # SuiteSparse; reverse Cuthill-McKee of |C| + |Cᵀ| stands in for that fill-reducing order
     p = np.ascontiguousarray(reverse_cuthill_mckee((abs(C) + abs(C.T)).tocsr(), symmetric_mode=True),
@@ -761,16 +775,25 @@ def run_precrecy(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    C, normC, p = af_inputs(n)
+    C, normC, p = af_inputs(n, args.mtx)
+    n = C.shape[0]
     s = args.pp_chunk
     nst = args.warmup + args.steps
-    out = {"metric": "σ_min grid pts/s (psPrecRecy, af23560-shaped N=23560, 200×200 grid, k=20, tol 1e-4)",
+    if args.mtx:
+        data = f"MatrixMarket file {os.path.basename(args.mtx)} (read by rls_mtx_read_csc as loaddata reads it)"
+        shape = f"{os.path.basename(args.mtx)} N={n} ({C.nnz} nnz, main_normC=645.74)"
+    else:
+        data = "synthetic af23560-shaped matrix (rls_b200.examples.af23560_shaped, NumPy PCG64 seed 20260318)"
+        shape = f"af23560-shaped N={n} (~20 nnz/row, band ±300, ‖C‖₂=645.74)"
+    metric = ("σ_min grid pts/s (psPrecRecy, af23560-shaped N=23560, 200×200 grid, k=20, tol 1e-4)" if not args.mtx
+              else f"σ_min grid pts/s (psPrecRecy, {os.path.basename(args.mtx)} N={n}, 200×200 grid, k=20, tol 1e-4)")
+    out = {"metric": metric,
            "unit": "pts/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
-           "data": "synthetic af23560-shaped matrix (rls_b200.examples.af23560_shaped, NumPy PCG64 seed 20260318)",
-           "config": {"workload": "psPrecRecy af23560-shaped N=%d (~20 nnz/row, band ±300, ‖C‖₂=645.74), 200x200 "
+           "data": data,
+           "config": {"workload": "psPrecRecy %s, 200x200 "
                                   "grid [-1.6,0.8]x[-1.55,1.55], k=20, tol=1e-4, r_main=6, p_main=60, r_pred=40, "
-                                  "p_pred=20, IC lsize=200 rsize=500, RCM column order" % n,
+                                  "p_pred=20, IC lsize=200 rsize=500, RCM column order" % shape,
                       "n": n, "nnz": int(C.nnz), "grid": list(AF_GRID), "points_per_step": s,
                       "span": f"traversal points {args.warmup * s}..{nst * s - 1} after {args.warmup * s} "
                               f"warm-up points (the run's first preconditioner build is in the warm-up)"}}

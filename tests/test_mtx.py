@@ -211,3 +211,23 @@ def test_save_run_writes_the_driver_fields(tmp_path):
     np.testing.assert_array_equal(z["sigma_min_grid"], reorder_to_natural_grid(rec, sig))
     assert float(z["elapsed"]) == 1.25 and int(z["stats_n_it"]) == 7
     assert z["stats_p_count"].shape == (len(rec.Z),)
+
+
+def test_bench_reads_the_af23560_matrix_from_a_file(tmp_path):
+    """bench.py --workload af23560 --mtx PATH: C comes from the file as loaddata reads it, with the
+    driver's main_normC and a permutation for the column order."""
+    import bench
+    rng = np.random.default_rng(11)
+    n = 40
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j in (i - 2, i, i + 3):
+            if 0 <= j < n:
+                rows.append(i); cols.append(j); vals.append(complex(rng.standard_normal(), 0))
+    path = tmp_path / "af.mtx"
+    write_coo(path, n, n, rows, cols, vals)
+    C, normC, p = bench.af_inputs(0, mtx=str(path))
+    np.testing.assert_array_equal(C.toarray(), scipy_dense(path))
+    assert sp.isspmatrix_csc(C) and C.has_sorted_indices
+    assert normC == 645.74
+    assert sorted(p.tolist()) == list(range(n))
