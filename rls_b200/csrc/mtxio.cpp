@@ -24,6 +24,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <new>
+#include <stdexcept>
 #include <vector>
 
 #include "../../include/rls_b200.h"
@@ -120,6 +122,8 @@ struct MtxFile {
         return fail("bad size line '" + s + "'");
     }
     if (a < 0 || b < 0 || c < 0) return fail("negative size");
+    if (a > 0 && b > INT64_MAX / a) return fail("m × n does not fit in 64 bits");
+    if (c > INT64_MAX / 2) return fail("too many entries");
     m = a;
     n = b;
     if (symm != S_GENERAL && m != n) return fail("a " + sym + " matrix must be square");
@@ -173,7 +177,7 @@ rls_c64 mirror(int symm, rls_c64 a) {
 
 }  // namespace
 
-extern "C" int rls_mtx_info(const char* path, int64_t* m, int64_t* n, int64_t* nnz_max, int* dense) {
+static int mtx_info_impl(const char* path, int64_t* m, int64_t* n, int64_t* nnz_max, int* dense) {
   MtxFile mf;
   const int rc = mf.open_header(path);
   if (rc != RLS_OK) return rc;
@@ -184,8 +188,8 @@ extern "C" int rls_mtx_info(const char* path, int64_t* m, int64_t* n, int64_t* n
   return RLS_OK;
 }
 
-extern "C" int rls_mtx_read_csc(const char* path, int base, int64_t cap, int64_t* colptr, int64_t* rowval,
-                                rls_c64* nzval, int64_t* nnz) {
+static int mtx_read_csc_impl(const char* path, int base, int64_t cap, int64_t* colptr, int64_t* rowval,
+                             rls_c64* nzval, int64_t* nnz) {
   if ((base != 0 && base != 1) || !colptr || !nnz || cap < 0 || (cap > 0 && (!rowval || !nzval))) {
     rls_host_error("rls_mtx_read_csc: invalid arguments");
     return RLS_ERR_ARG;
@@ -199,7 +203,9 @@ extern "C" int rls_mtx_read_csc(const char* path, int base, int64_t cap, int64_t
     rls_c64 v;
   };
   std::vector<Entry> ent;
-  ent.reserve(static_cast<size_t>(mf.symm == S_GENERAL ? mf.entries : 2 * mf.entries));
+  // the size line is not trusted for the allocation: reserve at most 2^24 entries up front
+  ent.reserve(static_cast<size_t>(std::min<int64_t>(mf.symm == S_GENERAL ? mf.entries : 2 * mf.entries,
+                                                    int64_t(1) << 24)));
   const int nv = mf.values_per_entry();
   int64_t seq = 0;
   for (int64_t q = 0; q < mf.entries; ++q) {
@@ -249,7 +255,7 @@ extern "C" int rls_mtx_read_csc(const char* path, int base, int64_t cap, int64_t
   return RLS_OK;
 }
 
-extern "C" int rls_mtx_read_dense(const char* path, rls_c64* A, int64_t lda) {
+static int mtx_read_dense_impl(const char* path, rls_c64* A, int64_t lda) {
   MtxFile mf;
   int rc = mf.open_header(path);
   if (rc != RLS_OK) return rc;
@@ -274,4 +280,32 @@ extern "C" int rls_mtx_read_dense(const char* path, rls_c64* A, int64_t lda) {
     }
   }
   return RLS_OK;
+}
+
+// The C entry points: no exception crosses the ABI (an allocation that fails, e.g. for a size
+// line far beyond the memory, returns RLS_ERR_NOMEM).
+template <class F>
+static int guarded(const char* what, F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    rls_host_error(std::string(what) + ": out of host memory");
+    return RLS_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    rls_host_error(std::string(what) + ": " + e.what());
+    return RLS_ERR_ARG;
+  }
+}
+
+extern "C" int rls_mtx_info(const char* path, int64_t* m, int64_t* n, int64_t* nnz_max, int* dense) {
+  return guarded("rls_mtx_info", [&] { return mtx_info_impl(path, m, n, nnz_max, dense); });
+}
+
+extern "C" int rls_mtx_read_csc(const char* path, int base, int64_t cap, int64_t* colptr, int64_t* rowval,
+                                rls_c64* nzval, int64_t* nnz) {
+  return guarded("rls_mtx_read_csc", [&] { return mtx_read_csc_impl(path, base, cap, colptr, rowval, nzval, nnz); });
+}
+
+extern "C" int rls_mtx_read_dense(const char* path, rls_c64* A, int64_t lda) {
+  return guarded("rls_mtx_read_dense", [&] { return mtx_read_dense_impl(path, A, lda); });
 }

@@ -42,10 +42,19 @@ def load_mtx(path):
         check(lib().rls_mtx_read_dense(_path(path), ptr(A), max(m, 1)))
         return A
     colptr = np.zeros(n + 1, dtype=np.int64)
-    rowval = np.zeros(max(nz, 1), dtype=np.int64)
-    nzval = np.zeros(max(nz, 1), dtype=np.complex128)
     nnz = C.c_int64(0)
-    check(lib().rls_mtx_read_csc(_path(path), 0, nz, ptr(colptr), ptr(rowval), ptr(nzval), C.byref(nnz)))
+    # the size line is not trusted for the allocation: a first pass with room for at most 2^24
+    # entries, then exactly the count the reader reports (RLS_ERR_DIM carries it)
+    cap = max(1, min(nz, 1 << 24))
+    while True:
+        rowval = np.zeros(cap, dtype=np.int64)
+        nzval = np.zeros(cap, dtype=np.complex128)
+        st = lib().rls_mtx_read_csc(_path(path), 0, cap, ptr(colptr), ptr(rowval), ptr(nzval), C.byref(nnz))
+        if st == -2 and nnz.value > cap:
+            cap = nnz.value
+            continue
+        check(st)
+        break
     k = nnz.value
     return sp.csc_matrix((nzval[:k].copy(), rowval[:k].copy(), colptr), shape=(m, n))
 

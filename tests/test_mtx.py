@@ -182,6 +182,8 @@ def test_empty_and_capacity(tmp_path):
     ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 1 x\n", "bad value"),
     ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 1 1.0 2.0\n", "trailing"),
     ("%%MatrixMarket matrix coordinate real general\n2 x 1\n", "size line"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1000000000000\n1 1 1.0\n", "ends after 1 of"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 9000000000000000000\n", "too many entries"),
 ])
 def test_malformed_files_raise(tmp_path, text, needle):
     path = tmp_path / "bad.mtx"
