@@ -99,3 +99,38 @@ def test_sparse_lu_operator_gives_the_qr_operators_results():
     s_lu, st_lu = OP.ps_tri_recy_sparse(C, p, rec, ctl, X0=X0, factor="lu")
     assert np.max(np.abs(s_qr - s_lu) / s_qr) <= 1e-8
     assert np.array_equal(st_qr.refine_it > 0, st_lu.refine_it > 0)
+
+
+@pytest.mark.parametrize("case", ["n1", "diagonal", "empty_columns", "two_blocks", "upper_only"])
+def test_band_order_edge_patterns(case):
+    """Degenerate patterns: the order is still a permutation, the stated bandwidths are those of
+    PᵀCP, and it is never wider than the natural order."""
+    rng = np.random.default_rng(3)
+    if case == "n1":
+        C = sp.csc_matrix(np.array([[2.0 + 1j]]))
+    elif case == "diagonal":
+        C = sp.diags(rng.standard_normal(50) + 3).tocsc().astype(np.complex128)
+    elif case == "empty_columns":
+        A = sp.random(40, 40, density=0.05, random_state=4, format="lil")
+        A[:, 7] = 0
+        A[:, 21] = 0
+        C = (A + sp.eye(40)).tocsc().astype(np.complex128)
+        C[7, 7] = 0                                   # stored zero on the diagonal
+        C.eliminate_zeros()
+    elif case == "two_blocks":
+        B1 = sp.random(30, 30, density=0.1, random_state=5) + sp.eye(30)
+        B2 = sp.random(25, 25, density=0.1, random_state=6) + sp.eye(25)
+        C = sp.block_diag([B1, B2]).tocsc().astype(np.complex128)
+        q = rng.permutation(55)
+        C = C[q][:, q].tocsc()
+    else:
+        C = sp.triu(sp.random(60, 60, density=0.08, random_state=7) + sp.eye(60)).tocsc().astype(np.complex128)
+    C.sort_indices()
+    n = C.shape[0]
+    p, l, u = R.band_order(C)
+    assert np.array_equal(np.sort(p), np.arange(n))
+    assert (l, u) == _bandwidths(C, p)
+    l0, u0 = _bandwidths(C, np.arange(n))
+    assert l * (l + u + 1) + l + u <= l0 * (l0 + u0 + 1) + l0 + u0
+    if case in ("n1", "diagonal"):
+        assert (l, u) == (0, 0)
