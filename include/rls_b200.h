@@ -11,8 +11,8 @@
  *   - calls are synchronous (rls_tsqr_r_noalloc and rls_spmm_shifted_dev only
  *     enqueue; see there); no exceptions cross the ABI; a negative return is an
  *     rls_status and rls_last_error() gives the message (rls_last_error(NULL)
- *     for rls_lane_offsets and rls_ic_factor, which take no context; the grid
- *     calls return the status alone);
+ *     for the calls that take no context: rls_lane_offsets, rls_ic_factor,
+ *     rls_band_order and rls_mtx_*; the grid calls return the status alone);
  *   - the library never frees or retains caller memory.
  */
 #ifndef RLS_B200_H
@@ -341,7 +341,10 @@ int rls_ctx_set_graphs(rls_ctx* ctx, int on);
  * forced-add gap budget, psTriRecy.jl:388-393) come from rls_grid_*.  X0 is
  * the n × r initial block the reference draws with rand!(X)
  * (psTriRecy.jl:607); NULL draws it on the device.  sigma_min receives nZ
- * values in Z order. */
+ * values in Z order.  Controls: r in 1..8, lobpcg_side 'L', implict_recycle true and
+ * implict_update false (RLS_ERR_ARG otherwise); the projected eigensolve keeps its work vectors
+ * (144 bytes per row) in shared memory, so p·r is limited to about 1600 on a B200 (a launch
+ * error beyond; the reference's drivers use p·r = 360). */
 int rls_pstrirecy_schur(rls_ctx* ctx, const rls_c64* Z, int64_t nZ, const rls_grid* g,
                         const rls_pstrirecy_control* control, const rls_c64* X0,
                         double* sigma_min, rls_pstrirecy_stats* stats);
